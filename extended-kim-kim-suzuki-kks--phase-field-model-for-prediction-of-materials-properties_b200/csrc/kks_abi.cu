@@ -1,0 +1,658 @@
+// kks_abi.cu - host runtime of one KKS cell behind the C ABI of include/kks.h.
+//
+// Execution model. An attempt is a fixed sequence of kernels and cuFFT
+// executions with no host decision inside it: the prologue reads the loop
+// state from device memory, the decide kernel writes it back (including the
+// reject / accept / enlarge outcome, pf_kks/solver.py:330-351), and a
+// rejection is handled on the device by restoring the step's input into the
+// candidate buffer. Consecutive attempts therefore alternate between the two
+// state buffers unconditionally, and the attempt for each parity is captured
+// once as a CUDA graph. kks_run launches as many attempt graphs as there are
+// steps left, synchronises once, reads the step counter, and launches again
+// for the steps that rejections consumed: one host synchronisation per batch
+// of steps, none per attempt.
+
+#include <cuda_runtime.h>
+#include <cufft.h>
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "kks_internal.cuh"
+
+static thread_local std::string g_last_error;
+
+static int set_error(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+#define CK(expr)                                                                                          \
+  do {                                                                                                    \
+    cudaError_t _e = (expr);                                                                              \
+    if (_e != cudaSuccess)                                                                                \
+      return set_error(KKS_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(_e));                \
+  } while (0)
+
+#define CKF(expr)                                                                                        \
+  do {                                                                                                   \
+    cufftResult _r = (expr);                                                                             \
+    if (_r != CUFFT_SUCCESS) return set_error(KKS_ERR_CUFFT, std::string(#expr) + ": cufft error " +      \
+                                              std::to_string((int)_r));                                  \
+  } while (0)
+
+struct kks_handle {
+  int device = 0, precision = 0, rsize = 8;
+  cudaStream_t stream = nullptr;
+  KksConst hc{};
+  KksConst* dc = nullptr;
+  KksCtl* d_ctl = nullptr;
+  KksPar* d_par = nullptr;
+  KksCtl* h_ctl = nullptr;  // pinned mirror
+  int32_t* h_target = nullptr;
+  uint8_t* d_flags = nullptr;
+  kks_record* d_ring = nullptr;
+  long long ring_cap = 0;
+  kks_step_row* d_rows = nullptr;
+  long long row_cap = 0;
+  double* d_kx = nullptr;
+  double* d_ky = nullptr;
+  double* d_xfer = nullptr;
+  void* arena = nullptr;
+  KksFieldPtrs f{};
+  int nblocks = 0;
+  cufftHandle plan_r2c3 = 0, plan_c2r5 = 0, plan_c2r2 = 0;
+  bool plans_made = false;
+  void* fft_work = nullptr;
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  int parity = 0;
+  bool uploaded = false;
+  double x_mean = 0.0;
+  long long rec_read = 0, row_read = 0;
+  std::vector<kks_record> recs;
+  std::vector<kks_step_row> rows;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  double device_ms = 0.0;
+  long long timed_attempts = 0;
+  long long attempts_launched = 0;
+};
+
+static size_t round_up(size_t v, size_t m) { return (v + m - 1) / m * m; }
+
+// Angular wave numbers of pf_kks/grid.py:6-20 (Nyquist entry of an even axis
+// left at 0), same arithmetic as the reference: j * 2 * pi / (n * 1).
+static void frequencies(int n, std::vector<double>& out, int count) {
+  out.assign(count, 0.0);
+  std::vector<double> lin(n, 0.0);
+  if (n % 2 == 1) {
+    int half = (int)((n - 1) / 2.0 + 1);
+    for (int j = 0; j < half; ++j) lin[j] = (double)j * 2 * M_PI / (n * 1.0);
+    int start = (int)(-(n + 1) / 2.0 + 1);
+    for (int j = half, v = start; j < n; ++j, ++v) lin[j] = (double)v * 2 * M_PI / (n * 1.0);
+  } else {
+    for (int j = 0; j < n / 2; ++j) lin[j] = (double)j * 2 * M_PI / (n * 1.0);
+    for (int j = n / 2 + 1, v = -n / 2 + 1; j < n; ++j, ++v) lin[j] = (double)v * 2 * M_PI / (n * 1.0);
+  }
+  for (int j = 0; j < count; ++j) out[j] = lin[j];
+}
+
+// np.interp at a scalar, host side (the stiffness is frozen at T(t = 0)).
+static double interp_host(double x, const double* xp, const double* fp, int n) {
+  if (n == 1 || x <= xp[0]) return fp[0];
+  if (x >= xp[n - 1]) return fp[n - 1];
+  int lo = 0, hi = n - 1;
+  while (hi - lo > 1) {
+    int mid = (lo + hi) / 2;
+    if (x >= xp[mid]) lo = mid; else hi = mid;
+  }
+  if (xp[lo] == x) return fp[lo];
+  double slope = (fp[lo + 1] - fp[lo]) / (xp[lo + 1] - xp[lo]);
+  return slope * (x - xp[lo]) + fp[lo];
+}
+
+template <typename R>
+static int enqueue_attempt(kks_handle* h, int p) {
+  cudaStream_t s = h->stream;
+  KksFieldPtrs& f = h->f;
+  const size_t NCp = h->hc.NCp;
+  kks_launch_prologue(h->dc, h->d_ctl, h->d_par, h->d_flags, h->d_ring, h->ring_cap, s);
+  kks_launch_square<R>(&h->hc, h->d_par, (R*)f.state[p], h->nblocks, s);
+  if (sizeof(R) == 8) {
+    CKF(cufftExecD2Z(h->plan_r2c3, (double*)f.state[p], (cufftDoubleComplex*)f.spec_a));
+  } else {
+    CKF(cufftExecR2C(h->plan_r2c3, (float*)f.state[p], (cufftComplex*)f.spec_a));
+  }
+  kks_launch_spectral_mid<R>(&h->hc, h->dc, h->d_par, f, s);
+  if (sizeof(R) == 8) {
+    CKF(cufftExecZ2D(h->plan_c2r5, (cufftDoubleComplex*)f.spec_bcd, (double*)f.real_b));
+  } else {
+    CKF(cufftExecC2R(h->plan_c2r5, (cufftComplex*)f.spec_bcd, (float*)f.real_b));
+  }
+  kks_launch_pre_pointwise<R>(&h->hc, h->dc, h->d_par, f, p, h->nblocks, s);
+  if (sizeof(R) == 8) {
+    CKF(cufftExecD2Z(h->plan_r2c3, (double*)f.real_c, (cufftDoubleComplex*)f.spec_bcd));
+  } else {
+    CKF(cufftExecR2C(h->plan_r2c3, (float*)f.real_c, (cufftComplex*)f.spec_bcd));
+  }
+  kks_launch_spectral_update<R>(&h->hc, h->dc, h->d_par, f, s);
+  if (sizeof(R) == 8) {
+    CKF(cufftExecZ2D(h->plan_c2r2, (cufftDoubleComplex*)f.spec_bcd + 3 * NCp, (double*)f.state[1 - p]));
+  } else {
+    CKF(cufftExecC2R(h->plan_c2r2, (cufftComplex*)f.spec_bcd + 3 * NCp, (float*)f.state[1 - p]));
+  }
+  kks_launch_post_pointwise<R>(&h->hc, h->dc, h->d_par, f, p, h->nblocks, s);
+  kks_launch_decide(h->dc, h->d_ctl, h->d_par, f.partials3, f.partials5, h->nblocks, h->d_ring, h->ring_cap,
+                    h->d_rows, h->row_cap, s);
+  kks_launch_restore<R>(&h->hc, h->dc, h->d_ctl, f, p, h->nblocks, s);
+  CK(cudaGetLastError());
+  return KKS_OK;
+}
+
+static int enqueue(kks_handle* h, int p) {
+  return h->precision == KKS_PRECISION_FP64 ? enqueue_attempt<double>(h, p) : enqueue_attempt<float>(h, p);
+}
+
+static int make_plans(kks_handle* h) {
+  const int nx = h->hc.nx, ny = h->hc.ny, nyh = h->hc.nyh;
+  int n[2] = {nx, ny};
+  int rembed[2] = {nx, ny};
+  int cembed[2] = {nx, nyh};
+  const bool d = h->precision == KKS_PRECISION_FP64;
+  size_t ws[3] = {0, 0, 0};
+  CKF(cufftCreate(&h->plan_r2c3));
+  CKF(cufftCreate(&h->plan_c2r5));
+  CKF(cufftCreate(&h->plan_c2r2));
+  h->plans_made = true;
+  for (cufftHandle p : {h->plan_r2c3, h->plan_c2r5, h->plan_c2r2}) CKF(cufftSetAutoAllocation(p, 0));
+  CKF(cufftMakePlanMany(h->plan_r2c3, 2, n, rembed, 1, h->hc.Np, cembed, 1, h->hc.NCp, d ? CUFFT_D2Z : CUFFT_R2C, 3,
+                        &ws[0]));
+  CKF(cufftMakePlanMany(h->plan_c2r5, 2, n, cembed, 1, h->hc.NCp, rembed, 1, h->hc.Np, d ? CUFFT_Z2D : CUFFT_C2R, 5,
+                        &ws[1]));
+  CKF(cufftMakePlanMany(h->plan_c2r2, 2, n, cembed, 1, h->hc.NCp, rembed, 1, h->hc.Np, d ? CUFFT_Z2D : CUFFT_C2R, 2,
+                        &ws[2]));
+  size_t w = std::max(ws[0], std::max(ws[1], ws[2]));
+  if (w > 0) CK(cudaMalloc(&h->fft_work, w));
+  for (cufftHandle p : {h->plan_r2c3, h->plan_c2r5, h->plan_c2r2}) {
+    CKF(cufftSetWorkArea(p, h->fft_work));
+    CKF(cufftSetStream(p, h->stream));
+  }
+  return KKS_OK;
+}
+
+static int capture_graphs(kks_handle* h) {
+  for (int p = 0; p < 2; ++p) {
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = enqueue(h, p);
+    cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+    if (rc != KKS_OK) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    if (e != cudaSuccess) return set_error(KKS_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&h->graph[p], g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return set_error(KKS_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+  }
+  return KKS_OK;
+}
+
+static void free_handle(kks_handle* h) {
+  if (!h) return;
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  for (int p = 0; p < 2; ++p)
+    if (h->graph[p]) cudaGraphExecDestroy(h->graph[p]);
+  if (h->plans_made) {
+    cufftDestroy(h->plan_r2c3);
+    cufftDestroy(h->plan_c2r5);
+    cufftDestroy(h->plan_c2r2);
+  }
+  cudaFree(h->fft_work);
+  cudaFree(h->arena);
+  cudaFree(h->dc);
+  cudaFree(h->d_ctl);
+  cudaFree(h->d_par);
+  cudaFree(h->d_flags);
+  cudaFree(h->d_ring);
+  cudaFree(h->d_rows);
+  cudaFree(h->d_kx);
+  cudaFree(h->d_ky);
+  cudaFree(h->d_xfer);
+  if (h->h_ctl) cudaFreeHost(h->h_ctl);
+  if (h->h_target) cudaFreeHost(h->h_target);
+  if (h->ev0) cudaEventDestroy(h->ev0);
+  if (h->ev1) cudaEventDestroy(h->ev1);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+}
+
+static int create_impl(kks_handle* h, const kks_params* prm, int32_t n_steps, const uint8_t* step_flags) {
+  CK(cudaSetDevice(h->device));
+  CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  CK(cudaEventCreate(&h->ev0));
+  CK(cudaEventCreate(&h->ev1));
+  KksConst& c = h->hc;
+  c.p = *prm;
+  c.nx = prm->nx;
+  c.ny = prm->ny;
+  c.nyh = prm->ny / 2 + 1;
+  c.N = prm->nx * prm->ny;
+  c.NC = prm->nx * c.nyh;
+  c.Np = (int)round_up((size_t)c.N, 64);
+  c.NCp = (int)round_up((size_t)c.NC, 32);
+  c.n_steps = n_steps;
+  c.dtime_s_min = prm->dtime_s / prm->dtime_min_divisor;
+  c.inv_N = 1.0 / (double)c.N;
+  const double T0 = interp_host(0.0, prm->sched_time, prm->sched_temp, prm->n_sched);
+  c.C11_0 = interp_host(T0, prm->table_T, prm->table[KKS_TAB_C11], prm->n_table);
+  c.C12_0 = interp_host(T0, prm->table_T, prm->table[KKS_TAB_C12], prm->n_table);
+  c.C44_0 = interp_host(T0, prm->table_T, prm->table[KKS_TAB_C44], prm->n_table);
+  c.c11 = c.C11_0 / c.C44_0;
+  c.c12 = c.C12_0 / c.C44_0;
+  c.c3 = (c.C11_0 + 2 * c.C12_0) / c.C44_0;
+  c.zero_dc = h->precision == KKS_PRECISION_MIXED;
+  h->rsize = h->precision == KKS_PRECISION_FP64 ? 8 : 4;
+
+  int nsm = 148;
+  CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device));
+  h->nblocks = kks_field_blocks(c.N, nsm);
+
+  // arena
+  const size_t R = h->rsize, Np = c.Np, NCp = c.NCp;
+  const size_t sz_state = 5 * Np * R, sz_spec_a = 3 * NCp * 2 * R, sz_real_b = 5 * Np * R, sz_real_c = 3 * Np * R,
+               sz_spec_bcd = 5 * NCp * 2 * R, sz_one = Np * R;
+  const size_t sz_part = round_up((size_t)h->nblocks * KKS_NPART * sizeof(double), 256);
+  size_t total = 2 * sz_state + sz_spec_a + sz_real_b + sz_real_c + sz_spec_bcd + 6 * sz_one + 2 * sz_part;
+  CK(cudaMalloc(&h->arena, total));
+  CK(cudaMemset(h->arena, 0, total));
+  char* a = (char*)h->arena;
+  h->f.state[0] = a; a += sz_state;
+  h->f.state[1] = a; a += sz_state;
+  h->f.spec_a = a; a += sz_spec_a;
+  h->f.real_b = a; a += sz_real_b;
+  h->f.real_c = a; a += sz_real_c;
+  h->f.spec_bcd = a; a += sz_spec_bcd;
+  h->f.eta_m = a; a += sz_one;
+  h->f.X_m = a; a += sz_one;
+  h->f.mu = a; a += sz_one;
+  for (int k = 0; k < 3; ++k) { h->f.g[k] = a; a += sz_one; }
+  h->f.partials3 = (double*)a; a += sz_part;
+  h->f.partials5 = (double*)a; a += sz_part;
+
+  std::vector<double> kx, ky;
+  frequencies(c.nx, kx, c.nx);
+  frequencies(c.ny, ky, c.nyh);
+  CK(cudaMalloc(&h->d_kx, c.nx * sizeof(double)));
+  CK(cudaMalloc(&h->d_ky, c.nyh * sizeof(double)));
+  CK(cudaMemcpy(h->d_kx, kx.data(), c.nx * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h->d_ky, ky.data(), c.nyh * sizeof(double), cudaMemcpyHostToDevice));
+  h->f.kx = h->d_kx;
+  h->f.ky = h->d_ky;
+
+  CK(cudaMalloc(&h->dc, sizeof(KksConst)));
+  CK(cudaMemcpy(h->dc, &c, sizeof(KksConst), cudaMemcpyHostToDevice));
+  CK(cudaMalloc(&h->d_ctl, sizeof(KksCtl)));
+  CK(cudaMemset(h->d_ctl, 0, sizeof(KksCtl)));
+  CK(cudaMalloc(&h->d_par, sizeof(KksPar)));
+  CK(cudaMemset(h->d_par, 0, sizeof(KksPar)));
+  CK(cudaMallocHost(&h->h_ctl, sizeof(KksCtl)));
+  memset(h->h_ctl, 0, sizeof(KksCtl));
+  CK(cudaMallocHost(&h->h_target, sizeof(int32_t)));
+  CK(cudaMalloc(&h->d_flags, std::max(n_steps, 1)));
+  CK(cudaMemset(h->d_flags, 0, std::max(n_steps, 1)));
+  if (n_steps > 0) CK(cudaMemcpy(h->d_flags, step_flags, n_steps, cudaMemcpyHostToDevice));
+  CK(cudaMalloc(&h->d_ring, h->ring_cap * sizeof(kks_record)));
+  CK(cudaMalloc(&h->d_rows, h->row_cap * sizeof(kks_step_row)));
+  CK(cudaMalloc(&h->d_xfer, (size_t)c.N * sizeof(double)));
+
+  int rc = make_plans(h);
+  if (rc != KKS_OK) return rc;
+  rc = capture_graphs(h);
+  if (rc != KKS_OK) return rc;
+  CK(cudaStreamSynchronize(h->stream));
+  return KKS_OK;
+}
+
+extern "C" {
+
+const char* kks_last_error(void) { return g_last_error.c_str(); }
+
+const char* kks_version(void) { return "kks_b200 1.0 (sm_100a, cuFFT)"; }
+
+int kks_create(const kks_params* params, int precision, int device, int32_t n_steps, const uint8_t* step_flags,
+               int64_t record_capacity, kks_handle** out) {
+  if (!params || !out) return set_error(KKS_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (params->nx < 2 || params->ny < 2) return set_error(KKS_ERR_ARG, "nx and ny must be >= 2 (np.gradient)");
+  if ((long long)params->nx * params->ny > (1LL << 30)) return set_error(KKS_ERR_ARG, "grid too large");
+  if (precision != KKS_PRECISION_FP64 && precision != KKS_PRECISION_MIXED)
+    return set_error(KKS_ERR_ARG, "precision must be KKS_PRECISION_FP64 or KKS_PRECISION_MIXED");
+  if (params->n_sched < 1 || params->n_sched > KKS_MAX_SCHED)
+    return set_error(KKS_ERR_ARG, "schedule length out of range");
+  if (params->n_table < 1 || params->n_table > KKS_MAX_TABLE)
+    return set_error(KKS_ERR_ARG, "table length out of range");
+  if (n_steps < 0 || (n_steps > 0 && !step_flags)) return set_error(KKS_ERR_ARG, "bad step schedule");
+  kks_handle* h = new (std::nothrow) kks_handle();
+  if (!h) return set_error(KKS_ERR_ARG, "out of host memory");
+  h->device = device;
+  h->precision = precision;
+  h->ring_cap = record_capacity > 64 ? record_capacity : 64;
+  h->row_cap = 4096;
+  int rc = create_impl(h, params, n_steps, step_flags);
+  if (rc != KKS_OK) {
+    std::string msg = g_last_error;
+    free_handle(h);
+    g_last_error = msg;
+    return rc;
+  }
+  *out = h;
+  return KKS_OK;
+}
+
+int kks_upload(kks_handle* h, const double* eta, const double* X, const double* X_al, const double* X_th) {
+  if (!h || !eta || !X || !X_al || !X_th) return set_error(KKS_ERR_ARG, "null argument");
+  CK(cudaSetDevice(h->device));
+  const int N = h->hc.N;
+  const size_t Np = h->hc.Np;
+  // mixed path: X is stored as a fluctuation around its FP64 mean
+  double x_mean = 0.0;
+  if (h->precision == KKS_PRECISION_MIXED) {
+    long double s = 0;
+    for (int i = 0; i < N; ++i) s += X[i];
+    x_mean = (double)(s / N);
+  }
+  h->x_mean = x_mean;
+  const double* src[4] = {eta, X, X_al, X_th};
+  const int slot[4] = {0, 1, 3, 4};
+  for (int k = 0; k < 4; ++k) {
+    if (h->precision == KKS_PRECISION_FP64) {
+      CK(cudaMemcpyAsync((double*)h->f.state[0] + slot[k] * Np, src[k], N * sizeof(double), cudaMemcpyHostToDevice,
+                         h->stream));
+    } else {
+      CK(cudaMemcpyAsync(h->d_xfer, src[k], N * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+      kks_launch_to_real<float>(h->d_xfer, (float*)h->f.state[0] + slot[k] * Np, N, k == 1 ? x_mean : 0.0,
+                                h->stream);
+      CK(cudaGetLastError());
+    }
+  }
+  // initial loop state (pf_kks/solver.py:118-175)
+  KksCtl* c = h->h_ctl;
+  memset(c, 0, sizeof(KksCtl));
+  c->iteration = 1;
+  c->minus_is_state = 1;
+  c->gm = 0; c->gs = 1; c->gb = 2;
+  c->Xv = h->hc.p.Xv0;
+  c->dtime_s = h->hc.p.dtime_s;
+  CK(cudaMemcpyAsync(h->d_ctl, c, sizeof(KksCtl), cudaMemcpyHostToDevice, h->stream));
+  KksPar par;
+  memset(&par, 0, sizeof(par));
+  par.x_mean = x_mean;
+  CK(cudaMemcpyAsync(h->d_par, &par, sizeof(KksPar), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  h->parity = 0;
+  h->rec_read = h->row_read = 0;
+  h->recs.clear();
+  h->rows.clear();
+  h->uploaded = true;
+  return KKS_OK;
+}
+
+static int drain_device(kks_handle* h) {
+  const KksCtl* c = h->h_ctl;
+  while (h->rec_read < c->n_rec) {
+    long long start = h->rec_read % h->ring_cap;
+    long long n = std::min(c->n_rec - h->rec_read, h->ring_cap - start);
+    size_t old = h->recs.size();
+    h->recs.resize(old + n);
+    CK(cudaMemcpy(h->recs.data() + old, h->d_ring + start, n * sizeof(kks_record), cudaMemcpyDeviceToHost));
+    h->rec_read += n;
+  }
+  while (h->row_read < c->n_row) {
+    long long start = h->row_read % h->row_cap;
+    long long n = std::min(c->n_row - h->row_read, h->row_cap - start);
+    size_t old = h->rows.size();
+    h->rows.resize(old + n);
+    CK(cudaMemcpy(h->rows.data() + old, h->d_rows + start, n * sizeof(kks_step_row), cudaMemcpyDeviceToHost));
+    h->row_read += n;
+  }
+  return KKS_OK;
+}
+
+int kks_run(kks_handle* h, int32_t n_steps, int32_t* status) {
+  if (!h || n_steps < 0) return set_error(KKS_ERR_ARG, "bad argument");
+  if (!h->uploaded) return set_error(KKS_ERR_STATE, "kks_run before kks_upload");
+  CK(cudaSetDevice(h->device));
+  KksCtl* c = h->h_ctl;
+  if (c->status != KKS_STATUS_OK) {
+    if (status) *status = c->status;
+    return KKS_OK;
+  }
+  const long long target = (long long)c->istep + n_steps;
+  if (target > h->hc.n_steps) return set_error(KKS_ERR_ARG, "run beyond the scheduled number of steps");
+  *h->h_target = (int32_t)target;
+  CK(cudaMemcpyAsync(&h->d_ctl->target_step, h->h_target, sizeof(int32_t), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaEventRecord(h->ev0, h->stream));
+  const long long max_batch = std::max(1LL, std::min(h->ring_cap / 2 - 1, h->row_cap - 1));
+  long long launched = 0;
+  while (c->istep < target && c->status == KKS_STATUS_OK) {
+    long long todo = std::min(target - c->istep, max_batch);
+    for (long long a = 0; a < todo; ++a) {
+      CK(cudaGraphLaunch(h->graph[h->parity], h->stream));
+      h->parity ^= 1;
+    }
+    launched += todo;
+    CK(cudaMemcpyAsync(c, h->d_ctl, sizeof(KksCtl), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    int rc = drain_device(h);
+    if (rc != KKS_OK) return rc;
+  }
+  CK(cudaEventRecord(h->ev1, h->stream));
+  CK(cudaEventSynchronize(h->ev1));
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+  h->device_ms += ms;
+  h->timed_attempts += launched;
+  h->attempts_launched += launched;
+  if (status) *status = c->status;
+  return KKS_OK;
+}
+
+int kks_drain(kks_handle* h, kks_record* records, int64_t record_cap, int64_t* n_records, kks_step_row* rows,
+              int64_t row_cap, int64_t* n_rows) {
+  if (!h) return set_error(KKS_ERR_ARG, "null handle");
+  if (n_records) {
+    if (!records && record_cap > 0) return set_error(KKS_ERR_ARG, "null record buffer");
+    int64_t n = std::min<int64_t>(record_cap, (int64_t)h->recs.size());
+    if (n > 0) memcpy(records, h->recs.data(), n * sizeof(kks_record));
+    h->recs.erase(h->recs.begin(), h->recs.begin() + n);
+    *n_records = n;
+  }
+  if (n_rows) {
+    if (!rows && row_cap > 0) return set_error(KKS_ERR_ARG, "null row buffer");
+    int64_t n = std::min<int64_t>(row_cap, (int64_t)h->rows.size());
+    if (n > 0) memcpy(rows, h->rows.data(), n * sizeof(kks_step_row));
+    h->rows.erase(h->rows.begin(), h->rows.begin() + n);
+    *n_rows = n;
+  }
+  return KKS_OK;
+}
+
+int kks_get_state(kks_handle* h, kks_run_state* s) {
+  if (!h || !s) return set_error(KKS_ERR_ARG, "null argument");
+  const KksCtl* c = h->h_ctl;
+  s->istep = c->istep;
+  s->iteration = c->iteration;
+  s->flag = c->flag;
+  s->good_step = c->good_step;
+  s->status = c->status;
+  s->parity = h->parity;
+  s->attempts = c->attempts;
+  s->n_records = (int64_t)h->recs.size();
+  s->n_rows = (int64_t)h->rows.size();
+  s->t = c->t;
+  s->t_s = c->t_s;
+  s->t_b = c->t_b;
+  s->ttime = c->ttime;
+  s->Xv = c->Xv;
+  s->dtime_s = c->dtime_s;
+  s->D_0 = c->D_0;
+  s->Meta_0 = c->Meta_0;
+  s->surf = c->surf;
+  s->surf_b = c->surf_b;
+  s->T_b = c->T_b;
+  s->error_istep = c->error_istep;
+  s->error_iteration = c->error_iteration;
+  s->error_dtime_s = c->error_dtime_s;
+  return KKS_OK;
+}
+
+int kks_download(kks_handle* h, double* eta, double* X, double* X_al, double* X_th) {
+  if (!h) return set_error(KKS_ERR_ARG, "null handle");
+  if (!h->uploaded) return set_error(KKS_ERR_STATE, "kks_download before kks_upload");
+  CK(cudaSetDevice(h->device));
+  const int N = h->hc.N;
+  const size_t Np = h->hc.Np;
+  double* dst[4] = {eta, X, X_al, X_th};
+  const int slot[4] = {0, 1, 3, 4};
+  for (int k = 0; k < 4; ++k) {
+    if (!dst[k]) continue;
+    if (h->precision == KKS_PRECISION_FP64) {
+      CK(cudaMemcpyAsync(dst[k], (double*)h->f.state[h->parity] + slot[k] * Np, N * sizeof(double),
+                         cudaMemcpyDeviceToHost, h->stream));
+    } else {
+      kks_launch_to_double<float>((float*)h->f.state[h->parity] + slot[k] * Np, h->d_xfer, N,
+                                  k == 1 ? h->x_mean : 0.0, h->stream);
+      CK(cudaGetLastError());
+      CK(cudaMemcpyAsync(dst[k], h->d_xfer, N * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    }
+    CK(cudaStreamSynchronize(h->stream));
+  }
+  return KKS_OK;
+}
+
+int kks_elastic_fields(kks_handle* h, double* sig4, double* eps4) {
+  if (!h || !sig4 || !eps4) return set_error(KKS_ERR_ARG, "null argument");
+  if (!h->uploaded || h->attempts_launched == 0) return set_error(KKS_ERR_STATE, "no attempt has run yet");
+  CK(cudaSetDevice(h->device));
+  const int p = h->parity ^ 1;  // the last attempt read its input from the other buffer
+  const int N = h->hc.N;
+  double* d_out = nullptr;
+  CK(cudaMalloc(&d_out, 8 * (size_t)N * sizeof(double)));
+  int one = 1;
+  cudaMemcpyAsync(&h->d_par->active, &one, sizeof(int), cudaMemcpyHostToDevice, h->stream);
+  KksFieldPtrs& f = h->f;
+  int rc = KKS_OK;
+  if (h->precision == KKS_PRECISION_FP64) {
+    kks_launch_square<double>(&h->hc, h->d_par, (double*)f.state[p], h->nblocks, h->stream);
+    if (cufftExecD2Z(h->plan_r2c3, (double*)f.state[p], (cufftDoubleComplex*)f.spec_a) != CUFFT_SUCCESS)
+      rc = set_error(KKS_ERR_CUFFT, "elastic R2C");
+    kks_launch_spectral_mid<double>(&h->hc, h->dc, h->d_par, f, h->stream);
+    if (cufftExecZ2D(h->plan_c2r5, (cufftDoubleComplex*)f.spec_bcd, (double*)f.real_b) != CUFFT_SUCCESS)
+      rc = set_error(KKS_ERR_CUFFT, "elastic C2R");
+    kks_launch_elastic_out<double>(&h->hc, h->dc, h->d_par, (double*)f.state[p], (double*)f.real_b, d_out,
+                                   d_out + 4 * (size_t)N, h->nblocks, h->stream);
+  } else {
+    kks_launch_square<float>(&h->hc, h->d_par, (float*)f.state[p], h->nblocks, h->stream);
+    if (cufftExecR2C(h->plan_r2c3, (float*)f.state[p], (cufftComplex*)f.spec_a) != CUFFT_SUCCESS)
+      rc = set_error(KKS_ERR_CUFFT, "elastic R2C");
+    kks_launch_spectral_mid<float>(&h->hc, h->dc, h->d_par, f, h->stream);
+    if (cufftExecC2R(h->plan_c2r5, (cufftComplex*)f.spec_bcd, (float*)f.real_b) != CUFFT_SUCCESS)
+      rc = set_error(KKS_ERR_CUFFT, "elastic C2R");
+    kks_launch_elastic_out<float>(&h->hc, h->dc, h->d_par, (float*)f.state[p], (float*)f.real_b, d_out,
+                                  d_out + 4 * (size_t)N, h->nblocks, h->stream);
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(sig4, d_out, 4 * (size_t)N * sizeof(double), cudaMemcpyDeviceToHost,
+                                            h->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(eps4, d_out + 4 * (size_t)N, 4 * (size_t)N * sizeof(double),
+                                            cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  cudaFree(d_out);
+  if (e != cudaSuccess) return set_error(KKS_ERR_CUDA, std::string("elastic fields: ") + cudaGetErrorString(e));
+  return rc;
+}
+
+// checkpoint blob: header | KksCtl | x_mean | parity | state[0..1] | eta_m | X_m | mu | g[0..2]
+struct CkptHeader {
+  char magic[8];
+  int32_t nx, ny, precision, parity;
+  double x_mean;
+  uint64_t bytes;
+};
+
+static size_t ckpt_field_bytes(kks_handle* h) { return (size_t)h->hc.Np * h->rsize; }
+
+int kks_checkpoint(kks_handle* h, void* buf, size_t cap, size_t* size) {
+  if (!h || !size) return set_error(KKS_ERR_ARG, "null argument");
+  const size_t fb = ckpt_field_bytes(h);
+  const size_t need = sizeof(CkptHeader) + sizeof(KksCtl) + 10 * fb + 6 * fb;
+  *size = need;
+  if (!buf) return KKS_OK;
+  if (cap < need) return set_error(KKS_ERR_CAPACITY, "checkpoint buffer too small");
+  if (!h->uploaded) return set_error(KKS_ERR_STATE, "nothing to checkpoint");
+  CK(cudaSetDevice(h->device));
+  char* o = (char*)buf;
+  CkptHeader hd;
+  memcpy(hd.magic, "KKSCKPT1", 8);
+  hd.nx = h->hc.nx; hd.ny = h->hc.ny; hd.precision = h->precision; hd.parity = h->parity;
+  hd.x_mean = h->x_mean;
+  hd.bytes = need;
+  memcpy(o, &hd, sizeof(hd)); o += sizeof(hd);
+  CK(cudaMemcpy(o, h->d_ctl, sizeof(KksCtl), cudaMemcpyDeviceToHost)); o += sizeof(KksCtl);
+  for (int p = 0; p < 2; ++p) { CK(cudaMemcpy(o, h->f.state[p], 5 * fb, cudaMemcpyDeviceToHost)); o += 5 * fb; }
+  void* rest[6] = {h->f.eta_m, h->f.X_m, h->f.mu, h->f.g[0], h->f.g[1], h->f.g[2]};
+  for (void* r : rest) { CK(cudaMemcpy(o, r, fb, cudaMemcpyDeviceToHost)); o += fb; }
+  return KKS_OK;
+}
+
+int kks_restore(kks_handle* h, const void* buf, size_t size) {
+  if (!h || !buf) return set_error(KKS_ERR_ARG, "null argument");
+  const size_t fb = ckpt_field_bytes(h);
+  const size_t need = sizeof(CkptHeader) + sizeof(KksCtl) + 10 * fb + 6 * fb;
+  if (size < need) return set_error(KKS_ERR_CAPACITY, "checkpoint blob too small");
+  const char* o = (const char*)buf;
+  CkptHeader hd;
+  memcpy(&hd, o, sizeof(hd)); o += sizeof(hd);
+  if (memcmp(hd.magic, "KKSCKPT1", 8) != 0 || hd.nx != h->hc.nx || hd.ny != h->hc.ny ||
+      hd.precision != h->precision)
+    return set_error(KKS_ERR_ARG, "checkpoint does not match this cell");
+  CK(cudaSetDevice(h->device));
+  CK(cudaStreamSynchronize(h->stream));
+  memcpy(h->h_ctl, o, sizeof(KksCtl)); o += sizeof(KksCtl);
+  h->h_ctl->target_step = h->h_ctl->istep;
+  CK(cudaMemcpy(h->d_ctl, h->h_ctl, sizeof(KksCtl), cudaMemcpyHostToDevice));
+  for (int p = 0; p < 2; ++p) { CK(cudaMemcpy(h->f.state[p], o, 5 * fb, cudaMemcpyHostToDevice)); o += 5 * fb; }
+  void* rest[6] = {h->f.eta_m, h->f.X_m, h->f.mu, h->f.g[0], h->f.g[1], h->f.g[2]};
+  for (void* r : rest) { CK(cudaMemcpy(r, o, fb, cudaMemcpyHostToDevice)); o += fb; }
+  h->parity = hd.parity;
+  h->x_mean = hd.x_mean;
+  KksPar par;
+  memset(&par, 0, sizeof(par));
+  par.x_mean = hd.x_mean;
+  CK(cudaMemcpy(h->d_par, &par, sizeof(KksPar), cudaMemcpyHostToDevice));
+  h->rec_read = h->h_ctl->n_rec;
+  h->row_read = h->h_ctl->n_row;
+  h->recs.clear();
+  h->rows.clear();
+  h->uploaded = true;
+  return KKS_OK;
+}
+
+int kks_timing(kks_handle* h, double* device_ms, int64_t* attempts) {
+  if (!h) return set_error(KKS_ERR_ARG, "null handle");
+  if (device_ms) *device_ms = h->device_ms;
+  if (attempts) *attempts = h->timed_attempts;
+  return KKS_OK;
+}
+
+int kks_destroy(kks_handle* h) {
+  free_handle(h);
+  return KKS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,157 @@
+// kks_internal.cuh - device-side state shared by the scalar kernels
+// (kks_scalar.cu), the field kernels (kks_fields.cu) and the host runtime
+// (kks_abi.cu).
+//
+// Layout in HBM of one cell (R = double for FP64, float for the mixed path;
+// Np = nx*ny rounded up to 64 elements, NCp = nx*(ny/2+1) rounded up to 32):
+//
+//   state[p], p = 0, 1 : R[5*Np]   eta | X | eta^2 | X_al | X_th
+//       (eta, X, eta^2 are the batch-3 R2C input; eta, X of the other parity
+//        are the batch-2 C2R output, so the attempt writes its candidate
+//        state straight into state[1-p])
+//   spec_a             : C[3*NCp]  FT(eta) | FT(X) | FT(eta^2)
+//   real_b             : R[5*Np]   eps_xx | eps_yy | eps_xy | d_x eta | d_y eta
+//   real_c             : R[3*Np]   drive | flux_x | flux_y
+//   spec_bcd           : C[5*NCp]  slots 0-4: B spectra (C2R input);
+//                                  slots 0-2: C spectra (R2C output, after B is consumed);
+//                                  slots 3-4: D spectra eta_b^, X_b^ (C2R input)
+//   eta_m, X_m, mu     : R[Np]     residual pair "minus" entry (pf_kks/solver.py:172-173)
+//   g[3]               : R[Np]     free-energy buffers rotated by index (minus, pre-update, new)
+//   partials           : double[nblocks * KKS_NPART] block sums of the reductions
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "kks.h"
+
+#define KKS_NPART 24
+// slots of the partial sums
+enum {
+  // written by the pre-update pointwise kernel (old state)
+  P3_G = 0,      // sum G_s
+  P3_GEL,        // sum (G_s + el_s)
+  P3_ETA,        // sum eta
+  P3_XLO,        // sum X[eta < 0.05]
+  P3_NLO,        // count eta < 0.05
+  P3_XHI,        // sum X[eta > 0.95]
+  P3_NHI,        // count eta > 0.95
+  P3_IFACE,      // interface cells of eta (surface steps)
+  // written by the post-update pointwise kernel (new state)
+  P5_GRAD2,      // sum (d_x eta_b)^2 + (d_y eta_b)^2 (np.gradient stencil)
+  P5_XLO,        // sum X_b[eta_b < 0.05]
+  P5_NLO,
+  P5_XHI,        // sum X_b[eta_b > 0.95]
+  P5_NHI,
+  P5_ETA,        // sum eta_b
+  P5_IFACE,      // interface cells of eta_b (surface steps)
+  P5_DIFF,       // sum dX/dt * mu_mean
+  P5_AC,         // sum (1/L) (deta/dt)^2
+  P5_TEMP,       // sum (G+ - G-)/dt
+  P5_COMB,       // sum (-diff + ac - temp)
+  P_COUNT
+};
+
+// Loop state of the cell (the scalar variables of pf_kks/solver.py:118-175),
+// read and written only by the single-thread prologue and decide kernels.
+struct KksCtl {
+  int32_t istep, iteration, flag, good_step, status, target_step;
+  int32_t minus_is_state, gm, gs, gb, restore, surf_valid, surf_b_valid, T_b_valid;
+  int32_t error_istep, error_iteration;
+  long long attempts, n_rec, n_row;
+  double t, t_s, t_b, ttime, Xv, dtime_s, D_0, Meta_0;
+  double surf, surf_b, T_b;
+  double E_prev, ts_prev, ed_sum, ed_comp;
+  int32_t ed_n, pad0;
+  double error_dtime_s;
+  // residual terms of the last attempt of the current step (history row)
+  double res[5];
+  int32_t res_valid, pad1;
+};
+
+// Per-attempt coefficients, written by the prologue, read by every field kernel.
+struct KksPar {
+  int32_t active, istep, iteration, surface;
+  int32_t armed_write, armed_residual, minus_is_state, gm, gs, gb;
+  double T, D, Meta, L, Vm;
+  double dt, L_s, kappa2_s, D_s, w_s;
+  double A_alp_s, B_alp_s, C_alp_s, A_thet_s, B_thet_s, C_thet_s;
+  double A_alp, B_alp, A_thet, B_thet;
+  double C44, epsX;
+  // derived
+  double inv_C44;
+  double pc_shift;   // (B_alp - B_thet) / (2 A_thet)
+  double pc_ratio;   // A_alp / A_thet
+  double ac_mul;     // -dtime_s * L_s
+  double ac_den;     // dtime_s * L_s * kappa2_s
+  double ch_mul;     // dtime_s * D_s
+  double inv_dt, inv_Ls;
+  // vertex forms of the two parabolas, for the FP32 path: f = A (c - v)^2 + f0
+  double va, fa0, vt, ft0;
+  double x_mean;     // mean of X carried in FP64 (mixed path; 0 for FP64)
+};
+
+// Run constants in device memory.
+struct KksConst {
+  kks_params p;
+  int32_t nx, ny, nyh, N, NC, Np, NCp, n_steps;
+  double dtime_s_min;
+  double inv_N;
+  // frozen stiffness at T0, normalised by C44(T0) (pf_kks/solver.py:152-154)
+  double c11, c12, c3;   // C11/C44_0, C12/C44_0, (C11 + 2 C12)/C44_0
+  double C11_0, C12_0, C44_0;
+  int32_t zero_dc;       // mixed path: project the mean mode of X out of the fluctuation field
+  int32_t pad;
+};
+
+// ---------------------------------------------------------------------------
+// launchers (kks_scalar.cu)
+void kks_launch_prologue(const KksConst* c, KksCtl* ctl, KksPar* par, const uint8_t* step_flags, kks_record* ring,
+                         long long ring_cap, cudaStream_t s);
+void kks_launch_decide(const KksConst* c, KksCtl* ctl, const KksPar* par, const double* partials3,
+                       const double* partials5, int nblocks, kks_record* ring, long long ring_cap,
+                       kks_step_row* rows, long long row_cap, cudaStream_t s);
+
+// launchers (kks_fields.cu); R = double or float
+struct KksFieldPtrs {
+  void* state[2];
+  void* spec_a;
+  void* real_b;
+  void* real_c;
+  void* spec_bcd;
+  void* eta_m;
+  void* X_m;
+  void* mu;
+  void* g[3];
+  double* partials3;
+  double* partials5;
+  const double* kx;
+  const double* ky;
+};
+
+int kks_field_blocks(int N, int num_sms);
+
+template <typename R>
+void kks_launch_square(const KksConst* hc, const KksPar* par, R* state, int nblocks, cudaStream_t s);
+template <typename R>
+void kks_launch_spectral_mid(const KksConst* hc, const KksConst* dc, const KksPar* par, const KksFieldPtrs& f,
+                             cudaStream_t s);
+template <typename R>
+void kks_launch_pre_pointwise(const KksConst* hc, const KksConst* dc, const KksPar* par, const KksFieldPtrs& f,
+                              int parity, int nblocks, cudaStream_t s);
+template <typename R>
+void kks_launch_spectral_update(const KksConst* hc, const KksConst* dc, const KksPar* par, const KksFieldPtrs& f,
+                                cudaStream_t s);
+template <typename R>
+void kks_launch_post_pointwise(const KksConst* hc, const KksConst* dc, const KksPar* par, const KksFieldPtrs& f,
+                               int parity, int nblocks, cudaStream_t s);
+template <typename R>
+void kks_launch_restore(const KksConst* hc, const KksConst* dc, const KksCtl* ctl, const KksFieldPtrs& f, int parity,
+                        int nblocks, cudaStream_t s);
+template <typename R>
+void kks_launch_elastic_out(const KksConst* hc, const KksConst* dc, const KksPar* par, const R* eta, const R* real_b,
+                            double* sig4, double* eps4, int nblocks, cudaStream_t s);
+template <typename R>
+void kks_launch_to_real(const double* src, R* dst, int n, double shift, cudaStream_t s);
+template <typename R>
+void kks_launch_to_double(const R* src, double* dst, int n, double shift, cudaStream_t s);

@@ -1,0 +1,404 @@
+// kks_scalar.cu - the scalar part of an attempt, on the device.
+//
+// Two single-thread stages bracket the field kernels of every attempt:
+//
+//  * kks_prologue: temperature from the heat-treatment schedule, vacancy
+//    model, Si diffusivity, interface mobility, Allen-Cahn coefficient, table
+//    interpolation and the dimensionless parameter set
+//    (pf_kks/solver.py:179-240, pf_kks/kinetics.py:9-107, pf_kks/materials.py:57-59);
+//  * kks_decide: finishes the block reductions, forms the total energy and the
+//    energy residual, and takes the reject / accept / enlarge decision and the
+//    end-of-step bookkeeping (pf_kks/solver.py:270-404, pf_kks/residual.py:26-66).
+//
+// This file is compiled with -fmad=false: every scalar expression is evaluated
+// with the same operation order and roundings as the reference's float64
+// Python, so the scalars (and the log lines printed from them) follow the
+// reference; only the libm-level exp may differ by an ulp.
+
+#include <math.h>
+
+#include "kks_internal.cuh"
+
+namespace {
+
+// Constants of pf_kks/constants.py:6-21.
+__device__ const double kR = 8.314472;
+__device__ const double kHF1VA = 63680;
+__device__ const double kSF1VA = 2.49;
+__device__ const double kHB = 10613;
+__device__ const double kSB_KB = 42453;
+__device__ const double kZ = 12;
+__device__ const double kD0_AL = 1.7e-4;
+__device__ const double kQ_AL = 142e3;
+__device__ const double kD0_SI = 3.66e-6;
+__device__ const double kQ_SI = 110958;
+
+// np.interp for a scalar abscissa (numpy's arr_interp: binary search, slope
+// times offset plus left value, end values outside the table).
+__device__ double interp(double x, const double* xp, const double* fp, int n) {
+  if (n == 1) return fp[0];
+  if (x < xp[0]) return fp[0];
+  if (x > xp[n - 1]) return fp[n - 1];
+  if (x == xp[n - 1]) return fp[n - 1];
+  int lo = 0, hi = n - 1;  // xp[lo] <= x < xp[hi]
+  while (hi - lo > 1) {
+    int mid = (lo + hi) >> 1;
+    if (x >= xp[mid]) lo = mid; else hi = mid;
+  }
+  if (xp[lo] == x) return fp[lo];
+  double slope = (fp[lo + 1] - fp[lo]) / (xp[lo + 1] - xp[lo]);
+  double r = slope * (x - xp[lo]) + fp[lo];
+  if (isnan(r)) {
+    r = slope * (x - xp[lo + 1]) + fp[lo + 1];
+    if (isnan(r) && fp[lo] == fp[lo + 1]) r = fp[lo];
+  }
+  return r;
+}
+
+__device__ double tab(const kks_params& p, int k, double T) {
+  return interp(T, p.table_T, p.table[k], p.n_table);
+}
+
+// pf_kks/kinetics.py:9-14
+__device__ double equilibrium_vacancy_fraction(double T) {
+  return exp(-(kHF1VA - T * kSF1VA) / (kR * T)) *
+         (1 - kZ * 0.01 + kZ * 0.01 * exp((kHB - T * kSB_KB) / (kR * T)));
+}
+
+// pf_kks/kinetics.py:24-38
+__device__ double si_diffusivity(double T, double Xv, double Xve, double D0, double QD, double cap) {
+  double factor = fabs(1 + (Xv - Xve) / Xve);
+  double D;
+  if (factor > cap) D = cap * D0 * exp(-QD / (kR * T));
+  else D = factor * D0 * exp(-QD / (kR * T));
+  if (factor < 1) D = D0 * exp(-QD / (kR * T));
+  return D;
+}
+
+// pf_kks/kinetics.py:41-45
+__device__ double effective_vacancy_diffusivity(double T, double Xv, double Xve) {
+  double D_Al = kD0_AL * exp(-kQ_AL / (kR * T));
+  double D_Si = kD0_SI * exp(-kQ_SI / (kR * T));
+  return fabs(1 + (Xv - Xve) / Xve) * (0.03 * D_Si + 0.97 * D_Al);
+}
+
+__device__ void push_record(KksCtl* ctl, kks_record* ring, long long cap, const kks_record& r) {
+  ring[ctl->n_rec % cap] = r;
+  ctl->n_rec += 1;
+}
+
+__global__ void kks_prologue(const KksConst* __restrict__ c, KksCtl* ctl, KksPar* par,
+                             const uint8_t* __restrict__ step_flags, kks_record* ring, long long ring_cap) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const kks_params& p = c->p;
+  if (ctl->status != KKS_STATUS_OK || ctl->istep >= ctl->target_step) {
+    par->active = 0;
+    return;
+  }
+  const int istep = ctl->istep;
+  const double T = interp(ctl->t, p.sched_time, p.sched_temp, p.n_sched);
+  const int surface = step_flags[istep] & 1;
+
+  double Xv = ctl->Xv;
+  const double Xve = equilibrium_vacancy_fraction(T);
+  const double D = si_diffusivity(T, Xv, Xve, p.D0, p.QD, p.diffusion_enhancement_cap);
+  const double Meta = p.Meta0 * exp(-p.QMeta / (kR * T));
+  const double Deff = effective_vacancy_diffusivity(T, Xv, Xve);
+  if (istep == 0) {
+    ctl->D_0 = D;
+    ctl->Meta_0 = Meta;
+    ctl->dtime_s = p.dtime_s;
+  }
+  double dtime_s = ctl->dtime_s;
+  if (dtime_s > p.dtime_max) dtime_s = p.dtime_max;
+  if (dtime_s < c->dtime_s_min) dtime_s = c->dtime_s_min;
+  ctl->dtime_s = dtime_s;
+  const double D_0 = ctl->D_0;
+  const double Meta_0 = ctl->Meta_0;
+  const double dx2 = p.dx * p.dx;
+  const double dtime = (dx2 / D_0) * p.dtime_s;  // ttime and Xv use the initial step (quirk of the reference)
+  ctl->ttime = ctl->ttime + dtime;
+  {
+    double dXv = (1 - exp(-dtime * (Deff / p.Lv2))) * (Xve - Xv);
+    ctl->Xv = Xv + dXv;
+  }
+
+  const double A_alp = tab(p, KKS_TAB_A_ALP, T);
+  const double B_alp = tab(p, KKS_TAB_B_ALP, T);
+  const double C_alp = tab(p, KKS_TAB_C_ALP, T);
+  const double C44 = tab(p, KKS_TAB_C44, T);
+  const double A_thet = tab(p, KKS_TAB_A_THET, T);
+  const double B_thet = tab(p, KKS_TAB_B_THET, T);
+  const double C_thet = tab(p, KKS_TAB_C_THET, T);
+  const double sigma = tab(p, KKS_TAB_GAMMA, T);
+  const double Omega0 = tab(p, KKS_TAB_VM, T);
+  const double epsX = tab(p, KKS_TAB_EPSX, T);
+  const double X_Si_fcc = tab(p, KKS_TAB_X_SI_FCC, T);
+
+  // pf_kks/kinetics.py:60-80
+  const double kappa2 = 2 * p.lambd * sigma * 3 / p.alpha;
+  const double w = (sigma * 3 * p.alpha) / p.lambd;
+  const double kappa = sqrt(kappa2);
+  const double xi = (19.0 / 30.0) * (1 / Omega0) * 2 * A_alp * ((X_Si_fcc - 0.9999) * (X_Si_fcc - 0.9999));
+  const double L = (sigma / (kappa * kappa)) * (1 / (1 / Meta + kappa * xi / (D * sqrt(2 * w)))) * 0.01;
+
+  if (istep % 100 == 0) {
+    kks_record r;
+    r.kind = KKS_REC_STATE;
+    r.istep = istep;
+    r.iteration = ctl->iteration;
+    r.good_step = ctl->flag ? ctl->good_step : -1;
+    r.T = T; r.D = D; r.L = L; r.Meta = Meta; r.Vm = Omega0; r.dtime_s = dtime_s;
+    r.res_total = r.res_energy_derivative = r.res_diffusion = r.res_allen_cahn = r.res_temperature = 0;
+    r.energy_s = 0;
+    push_record(ctl, ring, ring_cap, r);
+  }
+
+  // pf_kks/kinetics.py:83-107 (normalize)
+  KksPar q;
+  q.active = 1;
+  q.istep = istep;
+  q.iteration = ctl->iteration;
+  q.surface = surface;
+  q.armed_write = ctl->flag == 1;
+  q.armed_residual = (ctl->flag == 1) && (istep >= ctl->good_step + 2);
+  q.minus_is_state = ctl->minus_is_state;
+  q.gm = ctl->gm;
+  q.gs = ctl->gs;
+  q.gb = ctl->gb;
+  q.T = T; q.D = D; q.Meta = Meta; q.L = L; q.Vm = Omega0;
+  q.dt = dtime_s;
+  q.L_s = (L * C44 * dx2) / D_0;
+  const double kappa2_norm = 2 * p.lambd * sigma * 3 / p.alpha;
+  const double w_norm = (sigma * 3 * p.alpha) / p.lambd;
+  q.kappa2_s = kappa2_norm / (C44 * dx2);
+  q.D_s = D / D_0;
+  q.w_s = w_norm / (C44);
+  q.A_thet_s = A_thet / (C44 * Omega0);
+  q.B_thet_s = B_thet / (C44 * Omega0);
+  q.C_thet_s = C_thet / (C44 * Omega0);
+  q.A_alp_s = A_alp / (C44 * Omega0);
+  q.B_alp_s = B_alp / (C44 * Omega0);
+  q.C_alp_s = C_alp / (C44 * Omega0);
+  (void)Meta_0;
+  q.A_alp = A_alp; q.B_alp = B_alp; q.A_thet = A_thet; q.B_thet = B_thet;
+  q.C44 = C44;
+  q.epsX = epsX;
+  q.inv_C44 = 1.0 / C44;
+  q.pc_shift = (B_alp - B_thet) / (2 * A_thet);
+  q.pc_ratio = A_alp / A_thet;
+  q.ac_mul = -dtime_s * q.L_s;
+  q.ac_den = dtime_s * q.L_s * q.kappa2_s;
+  q.ch_mul = dtime_s * q.D_s;
+  q.inv_dt = 1.0 / dtime_s;
+  q.inv_Ls = 1 / q.L_s;
+  q.va = -q.B_alp_s / (2 * q.A_alp_s);
+  q.fa0 = q.C_alp_s - q.B_alp_s * q.B_alp_s / (4 * q.A_alp_s);
+  q.vt = -q.B_thet_s / (2 * q.A_thet_s);
+  q.ft0 = q.C_thet_s - q.B_thet_s * q.B_thet_s / (4 * q.A_thet_s);
+  q.x_mean = par->x_mean;
+  *par = q;
+  ctl->attempts += 1;
+}
+
+// Finish a sum over the partials of all blocks (fixed order, deterministic).
+__device__ double block_sum(double v) {
+  __shared__ double sh[32];
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) sh[wid] = v;
+  __syncthreads();
+  v = 0;
+  if (wid == 0) {
+    const int nw = (blockDim.x + 31) >> 5;
+    v = lane < nw ? sh[lane] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  }
+  return v;  // valid in thread 0
+}
+
+__global__ void kks_decide(const KksConst* __restrict__ c, KksCtl* ctl, const KksPar* __restrict__ par,
+                           const double* __restrict__ partials3, const double* __restrict__ partials5, int nblocks,
+                           kks_record* ring, long long ring_cap, kks_step_row* rows, long long row_cap) {
+  __shared__ double S[P_COUNT];
+  if (!par->active) return;
+  for (int k = 0; k < P_COUNT; ++k) {
+    const double* src = k < P5_GRAD2 ? partials3 : partials5;
+    double v = 0;
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) v += src[(size_t)b * KKS_NPART + k];
+    v = block_sum(v);
+    if (threadIdx.x == 0) S[k] = v;
+  }
+  if (threadIdx.x != 0) return;
+
+  const kks_params& p = c->p;
+  const double Nd = (double)c->N;
+  const int istep = par->istep;
+  const int iteration = ctl->iteration;
+  double dtime_s = ctl->dtime_s;
+
+  // total_energy (pf_kks/free_energy.py:98-110): both gradient components carry G and el
+  const double energy_s = S[P3_GEL] * 2.0 + (0.5 * par->kappa2_s) * S[P5_GRAD2];
+  if (par->surface) {  // interface measure of the step's input state (pf_kks/solver.py:180-181)
+    ctl->surf = S[P3_IFACE] * p.surf_scale;
+    ctl->surf_valid = 1;
+  }
+
+  if (iteration == p.max_iterations) {  // pf_kks/solver.py:292-295
+    ctl->status = KKS_STATUS_MAX_ITER;
+    ctl->error_istep = istep;
+    ctl->error_iteration = iteration;
+    ctl->error_dtime_s = dtime_s;
+    return;
+  }
+
+  int outcome = 0;  // 0: no residual, 1: rejected, 2: accepted, 3: enlarged
+  if (par->armed_residual) {
+    // kks_residual (pf_kks/residual.py:26-66); energy derivative = running
+    // mean over the completed steps since good_step
+    const double ed = ctl->ed_sum / (double)ctl->ed_n;
+    const double total = ed + S[P5_COMB];
+    if (!isfinite(total)) {  // pf_kks/solver.py:312-313
+      ctl->status = KKS_STATUS_NONFINITE;
+      ctl->error_istep = istep;
+      ctl->error_iteration = iteration;
+      ctl->error_dtime_s = dtime_s;
+      return;
+    }
+    ctl->res[0] = total;
+    ctl->res[1] = ed;
+    ctl->res[2] = S[P5_DIFF];
+    ctl->res[3] = S[P5_AC];
+    ctl->res[4] = S[P5_TEMP];
+    ctl->res_valid = 1;
+    kks_record r;
+    r.istep = istep;
+    r.iteration = iteration;
+    r.good_step = ctl->good_step;
+    r.T = par->T; r.D = par->D; r.L = par->L; r.Meta = par->Meta; r.Vm = par->Vm;
+    r.res_total = total;
+    r.res_energy_derivative = ed;
+    r.res_diffusion = S[P5_DIFF];
+    r.res_allen_cahn = S[P5_AC];
+    r.res_temperature = S[P5_TEMP];
+    r.energy_s = energy_s;
+    if (fabs(total) > p.residual_max) {
+      dtime_s /= p.step_factor;
+      r.kind = KKS_REC_REJECTED;
+      outcome = 1;
+    } else if (fabs(total) > p.residual_min) {
+      r.kind = KKS_REC_ACCEPTED;
+      outcome = 2;
+    } else {
+      r.kind = KKS_REC_ENLARGED;
+      outcome = 3;
+    }
+    r.dtime_s = dtime_s;
+    push_record(ctl, ring, ring_cap, r);
+    if (outcome == 3) dtime_s *= p.step_factor;
+  }
+  ctl->dtime_s = dtime_s;
+
+  const int gm = par->gm, gs = par->gs, gb = par->gb;
+  if (outcome == 1) {
+    // The rejected attempt becomes the "minus" entry of the pair; the host
+    // graph then restores the step's input state into the candidate buffer.
+    ctl->iteration = iteration + 1;
+    ctl->restore = 1;
+    ctl->minus_is_state = 0;
+    ctl->gm = gb;
+    ctl->gs = gm;
+    ctl->gb = gs;
+    return;
+  }
+
+  // ---- end of step (pf_kks/solver.py:353-404)
+  ctl->restore = 0;
+  ctl->minus_is_state = 1;
+  ctl->gm = gs;  // post-loop overwrite: the pair keeps the pre-update free energy
+  ctl->gs = gm;
+  ctl->gb = gb;
+
+  const double dx2 = p.dx * p.dx;
+  const double t = ctl->t;
+  const double t_s = ctl->t_s + dtime_s;
+  const double dtime = (dx2 / ctl->D_0) * dtime_s;
+  const double t_b = ctl->t_b + (dx2 / ctl->D_0) * dtime_s;
+  ctl->t_s = t_s;
+  ctl->t_b = t_b;
+  if (par->surface) {
+    ctl->T_b = interp(t_b, p.sched_time, p.sched_temp, p.n_sched);
+    ctl->T_b_valid = 1;
+    ctl->surf_b = S[P5_IFACE] * p.surf_scale;
+    ctl->surf_b_valid = 1;
+  }
+
+  // running sum of the energy derivative terms (pf_kks/residual.py:48-60)
+  if (ctl->flag == 1 && istep >= ctl->good_step + 1) {
+    const double term = (energy_s - ctl->E_prev) / (t_s - ctl->ts_prev);
+    const double y = term - ctl->ed_comp;
+    const double tt = ctl->ed_sum + y;
+    ctl->ed_comp = (tt - ctl->ed_sum) - y;
+    ctl->ed_sum = tt;
+    ctl->ed_n += 1;
+  }
+  ctl->E_prev = energy_s;
+  ctl->ts_prev = t_s;
+
+  const double X_al_mean = S[P3_XLO] / S[P3_NLO];
+  const double X_th_mean = S[P3_XHI] / S[P3_NHI];
+  const int armed_before = ctl->flag;
+  if (X_al_mean <= p.x_equilibrium && ctl->flag == 0 && istep > 1) {  // pf_kks/solver.py:375-378
+    ctl->good_step = istep + p.good_step_offset;
+    ctl->flag = 1;
+  }
+  (void)armed_before;
+
+  kks_step_row row;
+  for (int k = 0; k < 32; ++k) row.v[k] = 0;
+  row.v[KKS_H_X_AL_MEAN] = X_al_mean;
+  row.v[KKS_H_X_TH_MEAN] = X_th_mean;
+  row.v[KKS_H_X_MEAN] = X_th_mean;  // mask (eta > 0.05) & (eta > 0.95) is eta > 0.95
+  row.v[KKS_H_DX_AL_MEAN] = S[P5_XLO] / S[P5_NLO] - S[P3_XLO] / S[P3_NLO];
+  row.v[KKS_H_DX_TH_MEAN] = S[P5_XHI] / S[P5_NHI] - S[P3_XHI] / S[P3_NHI];
+  row.v[KKS_H_DETA_MEAN] = S[P5_ETA] / Nd - S[P3_ETA] / Nd;
+  row.v[KKS_H_DT] = ctl->T_b - par->T;
+  row.v[KKS_H_ETA_MEAN] = S[P3_ETA] / Nd;
+  row.v[KKS_H_G_MEAN] = S[P3_G] / Nd;
+  row.v[KKS_H_SURF] = ctl->surf_b;
+  row.v[KKS_H_DSURF] = ctl->surf_b - ctl->surf;
+  row.v[KKS_H_T] = par->T;
+  row.v[KKS_H_DTIME] = dtime;
+  row.v[KKS_H_TIME] = t;
+  row.v[KKS_H_TIME_S] = t_s;
+  row.v[KKS_H_L] = par->L;
+  row.v[KKS_H_ENERGY_S] = energy_s;
+  row.v[KKS_H_DTIME_S] = dtime_s;
+  if (par->armed_residual) {
+    for (int k = 0; k < 5; ++k) row.v[KKS_H_RES_TOTAL + k] = ctl->res[k];
+  }
+  row.v[KKS_H_TTIME] = ctl->ttime;
+  row.v[KKS_H_ISTEP] = (double)istep;
+  row.v[KKS_H_SURF_VALID] = (double)(ctl->surf_b_valid + 2 * ctl->surf_valid);
+  rows[ctl->n_row % row_cap] = row;
+  ctl->n_row += 1;
+
+  ctl->t = t_b;
+  ctl->istep = istep + 1;
+  ctl->iteration = 1;
+  ctl->res_valid = 0;
+}
+
+}  // namespace
+
+void kks_launch_prologue(const KksConst* c, KksCtl* ctl, KksPar* par, const uint8_t* step_flags, kks_record* ring,
+                         long long ring_cap, cudaStream_t s) {
+  kks_prologue<<<1, 32, 0, s>>>(c, ctl, par, step_flags, ring, ring_cap);
+}
+
+void kks_launch_decide(const KksConst* c, KksCtl* ctl, const KksPar* par, const double* partials3,
+                       const double* partials5, int nblocks, kks_record* ring, long long ring_cap,
+                       kks_step_row* rows, long long row_cap, cudaStream_t s) {
+  kks_decide<<<1, 256, 0, s>>>(c, ctl, par, partials3, partials5, nblocks, ring, ring_cap, rows, row_cap);
+}

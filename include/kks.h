@@ -1,0 +1,172 @@
+/*
+ * kks.h - C ABI of the B200-native extended-KKS phase-field step.
+ *
+ * One handle owns one simulation cell on one GPU: its fields stay resident in
+ * device memory, every attempt of the semi-implicit step (KKS free energy,
+ * Khachaturyan elasticity, spectral Allen-Cahn / Cahn-Hilliard updates, phase
+ * compositions, energy residual and the accept / enlarge / reject decision)
+ * runs on the device, and the host only launches work, drains log records and
+ * moves fields at the boundary.
+ *
+ * The reference (pf_kks, pure Python) has no FFI; its one entry point for this
+ * path is `pf_kks.solver.run(cfg, eta, X, X_al, X_th, out_dir, base_dir,
+ * write_logs, verbose)` (pf_kks/solver.py:76-414). The functions below are the
+ * pieces that call decomposes into; each names the reference lines it replaces.
+ *
+ * Conventions: every function returns 0 (KKS_OK) or a negative error code;
+ * kks_last_error() gives a message. No exception crosses the ABI. A handle
+ * uses one CUDA stream and is not thread-safe. Field arrays are C-order
+ * (nx, ny) float64 on the host, y fastest, as the reference's (nx, ny, 1).
+ */
+#ifndef KKS_H
+#define KKS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define KKS_OK 0
+#define KKS_ERR_ARG (-1)      /* invalid argument (size, pointer, option) */
+#define KKS_ERR_CUDA (-2)     /* CUDA runtime error */
+#define KKS_ERR_CUFFT (-3)    /* cuFFT error */
+#define KKS_ERR_STATE (-4)    /* call out of order (e.g. run before upload) */
+#define KKS_ERR_CAPACITY (-5) /* host buffer too small */
+
+/* Run status of a cell, set on the device (pf_kks/solver.py:292-295, 312-313). */
+#define KKS_STATUS_OK 0
+#define KKS_STATUS_MAX_ITER 1   /* AdaptiveStepError: no admissible step after max_iterations attempts */
+#define KKS_STATUS_NONFINITE 2  /* AdaptiveStepError: non-finite energy residual */
+
+#define KKS_PRECISION_FP64 0  /* all-FP64 step */
+#define KKS_PRECISION_MIXED 1 /* FP32 fields / FFTs / pointwise; FP64 scalars, phase compositions, mean X mode, sums */
+
+#define KKS_MAX_SCHED 64
+#define KKS_MAX_TABLE 32
+#define KKS_NTAB 13
+/* Order of the material tables in kks_params.table (pf_kks/materials.py:17-31). */
+enum {
+  KKS_TAB_A_ALP = 0, KKS_TAB_B_ALP, KKS_TAB_C_ALP, KKS_TAB_A_THET, KKS_TAB_B_THET, KKS_TAB_C_THET,
+  KKS_TAB_C11, KKS_TAB_C12, KKS_TAB_C44, KKS_TAB_EPSX, KKS_TAB_VM, KKS_TAB_GAMMA, KKS_TAB_X_SI_FCC
+};
+
+/* Run constants: SimulationConfig (pf_kks/config.py:12-90) after the scaling
+ * that solver.run applies at its start (pf_kks/solver.py:101-116), plus the
+ * tables of final_export.npz (pf_kks/materials.py:33-55, already scaled by
+ * c_gamma / c_eps0). */
+typedef struct kks_params {
+  int32_t nx, ny;
+  int32_t max_iterations, good_step_offset;
+  double dx;          /* grid spacing [m] */
+  double lambd;       /* half interface width [m] = half_width_cells * dx */
+  double alpha;       /* interface-width constant */
+  double D0, QD;      /* Si diffusion prefactor (x c_D) [m^2/s], activation energy [J/mol] */
+  double Meta0, QMeta;/* interface mobility prefactor (x c_Meta), activation energy */
+  double Lv2;         /* vacancy_sink_distance^2 [m^2] */
+  double diffusion_enhancement_cap;
+  double Xv0;         /* initial vacancy site fraction = quenched_vacancy_fraction(T_quench) */
+  double dtime_s, dtime_max, dtime_min_divisor;
+  double residual_max, residual_min, step_factor;
+  double x_equilibrium;
+  double surf_scale;  /* dx^2 / (2 lambd) (pf_kks/microstructure.py:128) */
+  int32_t n_sched, n_table;
+  double sched_time[KKS_MAX_SCHED], sched_temp[KKS_MAX_SCHED];
+  double table_T[KKS_MAX_TABLE];
+  double table[KKS_NTAB][KKS_MAX_TABLE];
+} kks_params;
+
+/* One log record, emitted on the device in program order
+ * (pf_kks/runlog.py:32-140 formats them). */
+#define KKS_REC_STATE 1     /* RunLog.state: every attempt of a step multiple of 100 */
+#define KKS_REC_REJECTED 2  /* RunLog.rejected (dtime_s already divided) */
+#define KKS_REC_ACCEPTED 3  /* RunLog.accepted */
+#define KKS_REC_ENLARGED 4  /* RunLog.enlarged (dtime_s not yet multiplied) */
+typedef struct kks_record {
+  int32_t kind, istep, iteration, good_step;
+  double T, D, L, Meta, Vm, dtime_s;
+  double res_total, res_energy_derivative, res_diffusion, res_allen_cahn, res_temperature;
+  double energy_s;
+} kks_record;
+
+/* Per-step history row (pf_kks/solver.py:375-395 and the energy / dt /
+ * residual arrays of :166-170, 410-413). */
+enum {
+  KKS_H_X_AL_MEAN = 0, KKS_H_X_TH_MEAN, KKS_H_X_MEAN, KKS_H_DX_AL_MEAN, KKS_H_DX_TH_MEAN, KKS_H_DETA_MEAN,
+  KKS_H_DT, KKS_H_ETA_MEAN, KKS_H_G_MEAN, KKS_H_SURF, KKS_H_DSURF, KKS_H_T, KKS_H_DTIME, KKS_H_TIME,
+  KKS_H_TIME_S, KKS_H_L, KKS_H_ENERGY_S, KKS_H_DTIME_S, KKS_H_RES_TOTAL, KKS_H_RES_ENERGY_DERIVATIVE,
+  KKS_H_RES_DIFFUSION, KKS_H_RES_ALLEN_CAHN, KKS_H_RES_TEMPERATURE, KKS_H_TTIME, KKS_H_ISTEP,
+  KKS_H_SURF_VALID, KKS_H_COUNT
+};
+typedef struct kks_step_row {
+  double v[32];
+} kks_step_row;
+
+/* Scalar run state (the loop variables of pf_kks/solver.py:118-175). */
+typedef struct kks_run_state {
+  int32_t istep, iteration, flag, good_step, status, parity;
+  int64_t attempts, n_records, n_rows;
+  double t, t_s, t_b, ttime, Xv, dtime_s, D_0, Meta_0, surf, surf_b, T_b;
+  int32_t error_istep, error_iteration;
+  double error_dtime_s;
+} kks_run_state;
+
+typedef struct kks_handle kks_handle;
+
+/* Create a cell: allocate its device arena, plan the batched cuFFT R2C/C2R
+ * transforms and capture the attempt graphs. Replaces the set-up of
+ * pf_kks/solver.py:99-175 (tables, FFT plans, wave vectors, frozen-stiffness
+ * Green operator, initial scalars). precision: KKS_PRECISION_*.
+ * step_flags[i] bit 0: step i+1 is a surface-sampling step
+ * (Schedule.surface_steps, pf_kks/solver.py:46-53); n_steps entries. */
+int kks_create(const kks_params* params, int precision, int device, int32_t n_steps, const uint8_t* step_flags,
+               int64_t record_capacity, kks_handle** out);
+
+/* Upload the initial fields (host float64, nx*ny each). Replaces the arrays
+ * handed to pf_kks/solver.py:76. */
+int kks_upload(kks_handle* h, const double* eta, const double* X, const double* X_al, const double* X_th);
+
+/* Advance up to n_steps accepted steps (attempt loop of pf_kks/solver.py:176-404)
+ * without a host synchronisation per attempt; returns when the steps are done
+ * or the device status is not OK. *status receives KKS_STATUS_*. */
+int kks_run(kks_handle* h, int32_t n_steps, int32_t* status);
+
+/* Copy the log records and history rows produced since the last drain. */
+int kks_drain(kks_handle* h, kks_record* records, int64_t record_cap, int64_t* n_records, kks_step_row* rows,
+              int64_t row_cap, int64_t* n_rows);
+
+/* Scalar loop state. */
+int kks_get_state(kks_handle* h, kks_run_state* state);
+
+/* Download the current fields (host float64, nx*ny each); any pointer may be NULL. */
+int kks_download(kks_handle* h, double* eta, double* X, double* X_al, double* X_th);
+
+/* Elastic stress and strain of the last attempt (returned by solve_elasticity,
+ * pf_kks/elasticity.py:107-163; SimulationResult.sig_el / eps_el). Components
+ * xx, yy, zz, xy (xz = yz = 0 in 2-D), nx*ny each: sig4 and eps4 hold 4*nx*ny. */
+int kks_elastic_fields(kks_handle* h, double* sig4, double* eps4);
+
+/* Exact restart point: every device buffer and scalar that carries state from
+ * one attempt to the next (the reference has none: pf_kks/io.py:6-8). With
+ * buf == NULL, *size receives the size in bytes. */
+int kks_checkpoint(kks_handle* h, void* buf, size_t cap, size_t* size);
+int kks_restore(kks_handle* h, const void* buf, size_t size);
+
+/* Device milliseconds spent in kks_run since creation (CUDA events on the
+ * handle's stream) and the attempts they covered. */
+int kks_timing(kks_handle* h, double* device_ms, int64_t* attempts);
+
+int kks_destroy(kks_handle* h);
+
+/* Message of the last error of this thread. */
+const char* kks_last_error(void);
+
+/* Library version string. */
+const char* kks_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* KKS_H */
