@@ -1,0 +1,364 @@
+"""Benchmark: KKS steps/s of the semi-implicit step at 1420^2 on B200.
+
+Workload (the reference-metric configuration that fits one GPU): the 1420 x 1420
+cell (710 nm, 40 Voronoi cells, ~1200 particles of radius U(3,10), heated
+400 -> 719 K at 20 K/min, energy-residual adaptive dt), mixed FP32/FP64 step.
+One step = one attempt of the time loop over the whole cell; the inputs (4
+fields of 1420^2) are resident in HBM when the timed region starts, and the
+per-attempt working set (~300 MB) is larger than the 126 MB L2.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 (torchrun, one rank per GPU) every rank advances its own cell
+(seed = rank): the ensemble shards with no collective in the step, so the
+scaling is weak; the device time is the max over ranks.
+
+``--impl reference`` times the CPU oracle (a numpy restatement of the
+reference's ``pf_kks.solver.run`` step, run with every host core for its FFTs)
+on the same workload, rank 0 only.
+"""
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(REPO, "extended-kim-kim-suzuki-kks--phase-field-model-for-prediction-of-materials-properties_b200")
+for _p in (PKG, REPO):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "KKS steps/s @1420^2 (mixed FP32/FP64 step)"
+UNIT = "steps/s"
+# Algorithmic HBM traffic of one attempt in units of one N-element real field
+# (every array touched once; 2-D transforms counted as a single pass):
+# state 8 + forward spectra 12 + C2R outputs 10 + pre-inverse spectra 4 +
+# non-state R2C inputs 8 = 42; armed steps add the residual pair (7) = 49.
+UNITS_UNARMED = 42
+UNITS_ARMED = 49
+
+
+def env_rank():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def measured_peaks():
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device),
+                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        try:
+            for line in open(self.path):
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 7:
+                    continue
+                try:
+                    sm.append(float(parts[0]))
+                    mx.append(float(parts[1]))
+                except ValueError:
+                    continue
+                for name, v in zip(("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"),
+                                   parts[3:7]):
+                    if v.lower().startswith("active"):
+                        reasons.add(name)
+        except OSError:
+            pass
+        finally:
+            try:
+                os.unlink(self.path)
+            except OSError:
+                pass
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def bench_config(precision, armed=None, attempts=None):
+    cfg = {
+        "workload": "ramp1420: 1420x1420 KKS cell (710 nm), 40 Voronoi cells, ~1200 particles R~U(3,10), "
+                    "400->719 K at 20 K/min, adaptive dt; one cell per GPU",
+        "grid": [1420, 1420],
+        "precision": precision,
+        "l2": "per-attempt working set ~300 MB > 126 MB L2 (no flush needed)",
+    }
+    if armed is not None:
+        cfg["armed"] = armed
+    if attempts is not None:
+        cfg["attempts"] = int(attempts)
+    return cfg
+
+
+def make_workload(precision, seed):
+    from pf_kks_gpu import workloads
+
+    cfg, spec = workloads.ramp1420(n_steps=100000, precision=precision, seed=seed)
+    return cfg, spec, workloads.initial_state(cfg, spec)
+
+
+def run_reference(args):
+    """CPU arm: the oracle's step on the same workload, every host core for the FFTs."""
+    rank, world, _ = env_rank()
+    if rank != 0:
+        return 0
+    from oracle import kks_oracle
+
+    cores = os.cpu_count() or 1
+    cfg, spec, state = make_workload("fp64", 0)
+    budget_s = 150.0
+    warm = min(args.warmup, 1)
+    t0 = time.perf_counter()
+    if warm:
+        kks_oracle.run(cfg, *state, cfg.material_tables, write_logs=False, save_maps=False, max_steps=warm,
+                       fft_workers=cores)
+    per_step = (time.perf_counter() - t0) / max(warm, 1)
+    k = max(1, min(args.steps, int(budget_s / max(per_step, 1e-3))))
+    t0 = time.perf_counter()
+    kks_oracle.run(cfg, *state, cfg.material_tables, write_logs=False, save_maps=False, max_steps=k,
+                   fft_workers=cores)
+    dt = time.perf_counter() - t0
+    value = k / dt
+    sample = f"{k} steps of the 1420^2 workload from its initial state (FP64 numpy, scipy.fft with {cores} workers)"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": k,
+        "warmup": warm, "ms_per_step": 1000.0 * dt / k, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": bench_config(args.precision),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def cpu_baseline(state, cfg):
+    """Bounded CPU sample of the same workload for the GPU arm's line."""
+    from oracle import kks_oracle
+
+    cores = os.cpu_count() or 1
+    k = 3
+    t0 = time.perf_counter()
+    kks_oracle.run(cfg, *state, cfg.material_tables, write_logs=False, save_maps=False, max_steps=k,
+                   fft_workers=cores)
+    dt = time.perf_counter() - t0
+    return {"value": k / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"first {k} steps of the same 1420^2 cell, FP64 numpy oracle, scipy.fft with {cores} workers"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
+    ap.add_argument("--precision", default="mixed", choices=("mixed", "fp64"))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        return run_reference(args)
+
+    rank, world, local_rank = env_rank()
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    from pf_kks_gpu import solver
+    from pf_kks_gpu.materials import MaterialTables
+
+    cfg, spec, state = make_workload(args.precision, seed=rank)
+    tables = MaterialTables.from_npz(cfg.material_tables, cfg.c_gamma, cfg.c_eps0)
+    N = cfg.nx * cfg.ny
+    p = 4 if args.precision == "mixed" else 8
+
+    def barrier():
+        if dist is not None:
+            import torch
+
+            torch.cuda.synchronize()
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        import torch
+
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local_rank}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    cell = solver.Cell(cfg, tables, precision=args.precision, device=local_rank)
+    cell.upload(*state)
+    cell.run(args.warmup)
+    cell.drain()
+    s0 = cell.state()
+    barrier()
+    ms0, a0 = cell.timing()
+    with ClockSampler(local_rank) as clocks:
+        cell.run(args.steps)
+    ms1, a1 = cell.timing()
+    s1 = cell.state()
+    cell.drain()
+    barrier()
+    dev_ms = max_over_ranks(ms1 - ms0)
+    steps_done = s1.istep - s0.istep
+    attempts = s1.attempts - s0.attempts
+    armed = bool(s1.flag) and s1.istep >= s1.good_step + 2
+    value = world * steps_done / (dev_ms / 1000.0)
+    ms_per_attempt = (ms1 - ms0) / max(attempts, 1)
+    cell.close()
+
+    # FP64 step on the same cell, for the mixed-vs-FP64 ratio of the metric
+    fp64 = None
+    if args.precision == "mixed":
+        c64 = solver.Cell(cfg, tables, precision="fp64", device=local_rank)
+        c64.upload(*state)
+        c64.run(args.warmup)
+        m0, _ = c64.timing()
+        k64 = max(10, args.steps // 4)
+        c64.run(k64)
+        m1, _ = c64.timing()
+        c64.close()
+        fp64 = k64 / ((m1 - m0) / 1000.0)
+
+    # end to end through the C ABI: host fields in, K steps, fields and histories out
+    import ctypes
+
+    try:
+        import torch
+
+        pinned = [torch.empty(N, dtype=torch.float64).pin_memory().numpy() for _ in range(8)]
+    except Exception:
+        pinned = [np.empty(N) for _ in range(8)]
+    for k in range(4):
+        pinned[k][:] = state[k].ravel()
+    e2e_cell = solver.Cell(cfg, tables, precision=args.precision, device=local_rank)
+    e2e_cell.upload(*[pinned[k] for k in range(4)])
+    e2e_cell.run(args.warmup)
+    e2e_cell.drain()
+    barrier()
+    lib = e2e_cell.lib
+    t0 = time.perf_counter()
+    lib.kks_upload(e2e_cell.h, *[pinned[k].ctypes.data_as(ctypes.POINTER(ctypes.c_double)) for k in range(4)])
+    e2e_cell.run(args.steps)
+    recs, rows = e2e_cell.drain()
+    lib.kks_download(e2e_cell.h, *[pinned[4 + k].ctypes.data_as(ctypes.POINTER(ctypes.c_double)) for k in range(4)])
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    e2e_steps = e2e_cell.state().istep
+    e2e_cell.close()
+    e2e_value = world * e2e_steps / e2e_s
+
+    units = UNITS_ARMED if armed else UNITS_UNARMED
+    peak, peak_kind = measured_peaks()
+    alg_bytes = units * N * p
+    achieved = alg_bytes / (ms_per_attempt / 1000.0) / 1e9
+    traffic = None
+    tpath = os.path.join(REPO, "profiles", f"attempt_traffic_1420_{args.precision}.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            traffic = json.load(f).get("dram_bytes_per_attempt")
+
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return 0
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": dev_ms / max(steps_done, 1),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32+f64" if args.precision == "mixed" else "f64",
+        "data": "synthetic",
+        "config": bench_config(args.precision, armed, attempts),
+        "cell_updates_per_s": value * N,
+        "fp64_steps_per_s": fp64,
+        "mixed_over_fp64": (value / world / fp64) if fp64 else None,
+        "roofline": {
+            "bound": "hbm",
+            "achieved": achieved,
+            "peak": peak,
+            "unit": "GB/s",
+            "frac": achieved / peak,
+            "traffic": traffic,
+            "kernel": "one attempt (captured CUDA graph: 8 own kernels + cuFFT R2C/C2R)",
+            "algorithmic_bytes": alg_bytes,
+            "peak_kind": peak_kind,
+        },
+        "clocks": clocks.summary(),
+        "e2e": {
+            "value": e2e_value,
+            "unit": UNIT,
+            "h2d_bytes_per_step": 4 * N * 8 / max(e2e_steps, 1),
+            "d2h_bytes_per_step": (4 * N * 8 + len(rows) * 256 + len(recs) * 128) / max(e2e_steps, 1),
+            "note": "kks_upload (4 fields) + kks_run(K) + kks_drain + kks_download (4 fields) per call of K steps",
+        },
+        "gpu_launches": int(8 * attempts),
+    }
+    if not args.no_cpu_baseline and world == 1:
+        line["cpu_baseline"] = cpu_baseline(state, cfg)
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

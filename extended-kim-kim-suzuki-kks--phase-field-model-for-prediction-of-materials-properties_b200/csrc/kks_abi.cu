@@ -64,15 +64,15 @@ struct kks_handle {
   double* d_ky = nullptr;
   double* d_xfer = nullptr;
   void* arena = nullptr;
+  size_t arena_bytes = 0, state_bytes = 0;
   KksFieldPtrs f{};
   int nblocks = 0;
-  cufftHandle plan_r2c3 = 0, plan_c2r5 = 0, plan_c2r2 = 0;
+  cufftHandle plan_r2c3 = 0, plan_c2r3 = 0, plan_c2r2 = 0;
   bool plans_made = false;
   void* fft_work = nullptr;
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   int parity = 0;
   bool uploaded = false;
-  double x_mean = 0.0;
   long long rec_read = 0, row_read = 0;
   std::vector<kks_record> recs;
   std::vector<kks_step_row> rows;
@@ -115,46 +115,46 @@ static double interp_host(double x, const double* xp, const double* fp, int n) {
   return slope * (x - xp[lo]) + fp[lo];
 }
 
-template <typename R>
+template <bool MIXED>
 static int enqueue_attempt(kks_handle* h, int p) {
   cudaStream_t s = h->stream;
   KksFieldPtrs& f = h->f;
   const size_t NCp = h->hc.NCp;
+  const int nb = h->nblocks;
   kks_launch_prologue(h->dc, h->d_ctl, h->d_par, h->d_flags, h->d_ring, h->ring_cap, s);
-  kks_launch_square<R>(&h->hc, h->d_par, (R*)f.state[p], h->nblocks, s);
-  if (sizeof(R) == 8) {
-    CKF(cufftExecD2Z(h->plan_r2c3, (double*)f.state[p], (cufftDoubleComplex*)f.spec_a));
+  kks_launch_prep<MIXED>(&h->hc, h->d_par, f, p, nb, s);
+  if (!MIXED) {
+    CKF(cufftExecD2Z(h->plan_r2c3, (double*)f.fft_in[p], (cufftDoubleComplex*)f.spec_a));
   } else {
-    CKF(cufftExecR2C(h->plan_r2c3, (float*)f.state[p], (cufftComplex*)f.spec_a));
+    CKF(cufftExecR2C(h->plan_r2c3, (float*)f.fft_in[p], (cufftComplex*)f.spec_a));
   }
-  kks_launch_spectral_mid<R>(&h->hc, h->dc, h->d_par, f, s);
-  if (sizeof(R) == 8) {
-    CKF(cufftExecZ2D(h->plan_c2r5, (cufftDoubleComplex*)f.spec_bcd, (double*)f.real_b));
+  kks_launch_spectral_mid<MIXED>(&h->hc, h->dc, h->d_par, f, nb, s);
+  if (!MIXED) {
+    CKF(cufftExecZ2D(h->plan_c2r3, (cufftDoubleComplex*)f.spec_bcd, (double*)f.real_b));
   } else {
-    CKF(cufftExecC2R(h->plan_c2r5, (cufftComplex*)f.spec_bcd, (float*)f.real_b));
+    CKF(cufftExecC2R(h->plan_c2r3, (cufftComplex*)f.spec_bcd, (float*)f.real_b));
   }
-  kks_launch_pre_pointwise<R>(&h->hc, h->dc, h->d_par, f, p, h->nblocks, s);
-  if (sizeof(R) == 8) {
+  kks_launch_pre_pointwise<MIXED>(&h->hc, h->dc, h->d_par, f, p, nb, s);
+  if (!MIXED) {
     CKF(cufftExecD2Z(h->plan_r2c3, (double*)f.real_c, (cufftDoubleComplex*)f.spec_bcd));
   } else {
     CKF(cufftExecR2C(h->plan_r2c3, (float*)f.real_c, (cufftComplex*)f.spec_bcd));
   }
-  kks_launch_spectral_update<R>(&h->hc, h->dc, h->d_par, f, s);
-  if (sizeof(R) == 8) {
-    CKF(cufftExecZ2D(h->plan_c2r2, (cufftDoubleComplex*)f.spec_bcd + 3 * NCp, (double*)f.state[1 - p]));
+  kks_launch_spectral_update<MIXED>(&h->hc, h->dc, h->d_par, f, nb, s);
+  if (!MIXED) {
+    CKF(cufftExecZ2D(h->plan_c2r2, (cufftDoubleComplex*)f.spec_bcd + 3 * NCp, (double*)f.fft_out[p]));
   } else {
-    CKF(cufftExecC2R(h->plan_c2r2, (cufftComplex*)f.spec_bcd + 3 * NCp, (float*)f.state[1 - p]));
+    CKF(cufftExecC2R(h->plan_c2r2, (cufftComplex*)f.spec_bcd + 3 * NCp, (float*)f.fft_out[p]));
   }
-  kks_launch_post_pointwise<R>(&h->hc, h->dc, h->d_par, f, p, h->nblocks, s);
-  kks_launch_decide(h->dc, h->d_ctl, h->d_par, f.partials3, f.partials5, h->nblocks, h->d_ring, h->ring_cap,
-                    h->d_rows, h->row_cap, s);
-  kks_launch_restore<R>(&h->hc, h->dc, h->d_ctl, f, p, h->nblocks, s);
+  kks_launch_post_pointwise<MIXED>(&h->hc, h->dc, h->d_par, f, p, nb, s);
+  kks_launch_decide(h->dc, h->d_ctl, h->d_par, f.partials, nb, h->d_ring, h->ring_cap, h->d_rows, h->row_cap, s);
+  kks_launch_restore<MIXED>(&h->hc, h->dc, h->d_ctl, f, p, nb, s);
   CK(cudaGetLastError());
   return KKS_OK;
 }
 
 static int enqueue(kks_handle* h, int p) {
-  return h->precision == KKS_PRECISION_FP64 ? enqueue_attempt<double>(h, p) : enqueue_attempt<float>(h, p);
+  return h->precision == KKS_PRECISION_FP64 ? enqueue_attempt<false>(h, p) : enqueue_attempt<true>(h, p);
 }
 
 static int make_plans(kks_handle* h) {
@@ -165,19 +165,19 @@ static int make_plans(kks_handle* h) {
   const bool d = h->precision == KKS_PRECISION_FP64;
   size_t ws[3] = {0, 0, 0};
   CKF(cufftCreate(&h->plan_r2c3));
-  CKF(cufftCreate(&h->plan_c2r5));
+  CKF(cufftCreate(&h->plan_c2r3));
   CKF(cufftCreate(&h->plan_c2r2));
   h->plans_made = true;
-  for (cufftHandle p : {h->plan_r2c3, h->plan_c2r5, h->plan_c2r2}) CKF(cufftSetAutoAllocation(p, 0));
+  for (cufftHandle p : {h->plan_r2c3, h->plan_c2r3, h->plan_c2r2}) CKF(cufftSetAutoAllocation(p, 0));
   CKF(cufftMakePlanMany(h->plan_r2c3, 2, n, rembed, 1, h->hc.Np, cembed, 1, h->hc.NCp, d ? CUFFT_D2Z : CUFFT_R2C, 3,
                         &ws[0]));
-  CKF(cufftMakePlanMany(h->plan_c2r5, 2, n, cembed, 1, h->hc.NCp, rembed, 1, h->hc.Np, d ? CUFFT_Z2D : CUFFT_C2R, 5,
+  CKF(cufftMakePlanMany(h->plan_c2r3, 2, n, cembed, 1, h->hc.NCp, rembed, 1, h->hc.Np, d ? CUFFT_Z2D : CUFFT_C2R, 3,
                         &ws[1]));
   CKF(cufftMakePlanMany(h->plan_c2r2, 2, n, cembed, 1, h->hc.NCp, rembed, 1, h->hc.Np, d ? CUFFT_Z2D : CUFFT_C2R, 2,
                         &ws[2]));
   size_t w = std::max(ws[0], std::max(ws[1], ws[2]));
   if (w > 0) CK(cudaMalloc(&h->fft_work, w));
-  for (cufftHandle p : {h->plan_r2c3, h->plan_c2r5, h->plan_c2r2}) {
+  for (cufftHandle p : {h->plan_r2c3, h->plan_c2r3, h->plan_c2r2}) {
     CKF(cufftSetWorkArea(p, h->fft_work));
     CKF(cufftSetStream(p, h->stream));
   }
@@ -209,7 +209,7 @@ static void free_handle(kks_handle* h) {
     if (h->graph[p]) cudaGraphExecDestroy(h->graph[p]);
   if (h->plans_made) {
     cufftDestroy(h->plan_r2c3);
-    cufftDestroy(h->plan_c2r5);
+    cufftDestroy(h->plan_c2r3);
     cufftDestroy(h->plan_c2r2);
   }
   cudaFree(h->fft_work);
@@ -255,34 +255,56 @@ static int create_impl(kks_handle* h, const kks_params* prm, int32_t n_steps, co
   c.c11 = c.C11_0 / c.C44_0;
   c.c12 = c.C12_0 / c.C44_0;
   c.c3 = (c.C11_0 + 2 * c.C12_0) / c.C44_0;
-  c.zero_dc = h->precision == KKS_PRECISION_MIXED;
   h->rsize = h->precision == KKS_PRECISION_FP64 ? 8 : 4;
 
   int nsm = 148;
   CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device));
   h->nblocks = kks_field_blocks(c.N, nsm);
 
-  // arena
-  const size_t R = h->rsize, Np = c.Np, NCp = c.NCp;
-  const size_t sz_state = 5 * Np * R, sz_spec_a = 3 * NCp * 2 * R, sz_real_b = 5 * Np * R, sz_real_c = 3 * Np * R,
+  // arena (layout in kks_internal.cuh)
+  const bool mixed = h->precision == KKS_PRECISION_MIXED;
+  c.mixed = mixed;
+  const size_t R = h->rsize, Np = c.Np, NCp = c.NCp, D = sizeof(double);
+  const size_t sz_state = mixed ? 2 * Np * D + 2 * Np * R : 5 * Np * D;
+  const size_t sz_fin = mixed ? 3 * Np * R : 0;
+  const size_t sz_spec_a = 3 * NCp * 2 * R, sz_real_b = 3 * Np * R, sz_real_c = 3 * Np * R,
                sz_spec_bcd = 5 * NCp * 2 * R, sz_one = Np * R;
   const size_t sz_part = round_up((size_t)h->nblocks * KKS_NPART * sizeof(double), 256);
-  size_t total = 2 * sz_state + sz_spec_a + sz_real_b + sz_real_c + sz_spec_bcd + 6 * sz_one + 2 * sz_part;
+  size_t total = 2 * sz_state + sz_fin + sz_spec_a + sz_real_b + sz_real_c + sz_spec_bcd + 2 * Np * D + 4 * sz_one +
+                 sz_part;
   CK(cudaMalloc(&h->arena, total));
   CK(cudaMemset(h->arena, 0, total));
+  h->arena_bytes = total;
   char* a = (char*)h->arena;
-  h->f.state[0] = a; a += sz_state;
-  h->f.state[1] = a; a += sz_state;
+  char* state[2];
+  state[0] = a; a += sz_state;
+  state[1] = a; a += sz_state;
+  h->state_bytes = sz_state;
+  char* fin = a; a += sz_fin;
   h->f.spec_a = a; a += sz_spec_a;
   h->f.real_b = a; a += sz_real_b;
   h->f.real_c = a; a += sz_real_c;
   h->f.spec_bcd = a; a += sz_spec_bcd;
-  h->f.eta_m = a; a += sz_one;
-  h->f.X_m = a; a += sz_one;
+  h->f.eta_m = a; a += Np * D;
+  h->f.X_m = a; a += Np * D;
   h->f.mu = a; a += sz_one;
   for (int k = 0; k < 3; ++k) { h->f.g[k] = a; a += sz_one; }
-  h->f.partials3 = (double*)a; a += sz_part;
-  h->f.partials5 = (double*)a; a += sz_part;
+  h->f.partials = (double*)a; a += sz_part;
+  for (int p = 0; p < 2; ++p) {
+    h->f.eta[p] = state[p];
+    h->f.X[p] = state[p] + Np * D;
+    if (mixed) {
+      h->f.X_al[p] = state[p] + 2 * Np * D;
+      h->f.X_th[p] = state[p] + 2 * Np * D + Np * R;
+    } else {
+      h->f.X_al[p] = state[p] + 3 * Np * D;
+      h->f.X_th[p] = state[p] + 4 * Np * D;
+    }
+  }
+  for (int p = 0; p < 2; ++p) {
+    h->f.fft_in[p] = mixed ? fin : state[p];           // eta | X | eta^2
+    h->f.fft_out[p] = mixed ? h->f.real_c : state[1 - p];  // eta_b | X_b, or d_eta | d_X
+  }
 
   std::vector<double> kx, ky;
   frequencies(c.nx, kx, c.nx);
@@ -354,32 +376,42 @@ int kks_create(const kks_params* params, int precision, int device, int32_t n_st
   return KKS_OK;
 }
 
+// Host float64 field -> device field of type R (state fields eta and X are
+// float64 on both paths; X_al, X_th follow the path's precision).
+static int put_field(kks_handle* h, void* dst, bool is_double, const double* src) {
+  const int N = h->hc.N;
+  if (is_double) {
+    CK(cudaMemcpyAsync(dst, src, N * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  } else {
+    CK(cudaMemcpyAsync(h->d_xfer, src, N * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    kks_launch_to_real<float>(h->d_xfer, (float*)dst, N, h->stream);
+    CK(cudaGetLastError());
+  }
+  return KKS_OK;
+}
+
+static int get_field(kks_handle* h, double* dst, const void* src, bool is_double) {
+  const int N = h->hc.N;
+  if (is_double) {
+    CK(cudaMemcpyAsync(dst, src, N * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  } else {
+    kks_launch_to_double<float>((const float*)src, h->d_xfer, N, h->stream);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(dst, h->d_xfer, N * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  }
+  CK(cudaStreamSynchronize(h->stream));
+  return KKS_OK;
+}
+
 int kks_upload(kks_handle* h, const double* eta, const double* X, const double* X_al, const double* X_th) {
   if (!h || !eta || !X || !X_al || !X_th) return set_error(KKS_ERR_ARG, "null argument");
   CK(cudaSetDevice(h->device));
-  const int N = h->hc.N;
-  const size_t Np = h->hc.Np;
-  // mixed path: X is stored as a fluctuation around its FP64 mean
-  double x_mean = 0.0;
-  if (h->precision == KKS_PRECISION_MIXED) {
-    long double s = 0;
-    for (int i = 0; i < N; ++i) s += X[i];
-    x_mean = (double)(s / N);
-  }
-  h->x_mean = x_mean;
-  const double* src[4] = {eta, X, X_al, X_th};
-  const int slot[4] = {0, 1, 3, 4};
-  for (int k = 0; k < 4; ++k) {
-    if (h->precision == KKS_PRECISION_FP64) {
-      CK(cudaMemcpyAsync((double*)h->f.state[0] + slot[k] * Np, src[k], N * sizeof(double), cudaMemcpyHostToDevice,
-                         h->stream));
-    } else {
-      CK(cudaMemcpyAsync(h->d_xfer, src[k], N * sizeof(double), cudaMemcpyHostToDevice, h->stream));
-      kks_launch_to_real<float>(h->d_xfer, (float*)h->f.state[0] + slot[k] * Np, N, k == 1 ? x_mean : 0.0,
-                                h->stream);
-      CK(cudaGetLastError());
-    }
-  }
+  const bool d = h->precision == KKS_PRECISION_FP64;
+  int rc;
+  if ((rc = put_field(h, h->f.eta[0], true, eta)) != KKS_OK) return rc;
+  if ((rc = put_field(h, h->f.X[0], true, X)) != KKS_OK) return rc;
+  if ((rc = put_field(h, h->f.X_al[0], d, X_al)) != KKS_OK) return rc;
+  if ((rc = put_field(h, h->f.X_th[0], d, X_th)) != KKS_OK) return rc;
   // initial loop state (pf_kks/solver.py:118-175)
   KksCtl* c = h->h_ctl;
   memset(c, 0, sizeof(KksCtl));
@@ -389,16 +421,14 @@ int kks_upload(kks_handle* h, const double* eta, const double* X, const double* 
   c->Xv = h->hc.p.Xv0;
   c->dtime_s = h->hc.p.dtime_s;
   CK(cudaMemcpyAsync(h->d_ctl, c, sizeof(KksCtl), cudaMemcpyHostToDevice, h->stream));
-  KksPar par;
-  memset(&par, 0, sizeof(par));
-  par.x_mean = x_mean;
-  CK(cudaMemcpyAsync(h->d_par, &par, sizeof(KksPar), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemsetAsync(h->d_par, 0, sizeof(KksPar), h->stream));
   CK(cudaStreamSynchronize(h->stream));
   h->parity = 0;
   h->rec_read = h->row_read = 0;
   h->recs.clear();
   h->rows.clear();
   h->uploaded = true;
+  h->attempts_launched = 0;
   return KKS_OK;
 }
 
@@ -515,131 +545,138 @@ int kks_download(kks_handle* h, double* eta, double* X, double* X_al, double* X_
   if (!h) return set_error(KKS_ERR_ARG, "null handle");
   if (!h->uploaded) return set_error(KKS_ERR_STATE, "kks_download before kks_upload");
   CK(cudaSetDevice(h->device));
-  const int N = h->hc.N;
-  const size_t Np = h->hc.Np;
-  double* dst[4] = {eta, X, X_al, X_th};
-  const int slot[4] = {0, 1, 3, 4};
-  for (int k = 0; k < 4; ++k) {
-    if (!dst[k]) continue;
-    if (h->precision == KKS_PRECISION_FP64) {
-      CK(cudaMemcpyAsync(dst[k], (double*)h->f.state[h->parity] + slot[k] * Np, N * sizeof(double),
-                         cudaMemcpyDeviceToHost, h->stream));
-    } else {
-      kks_launch_to_double<float>((float*)h->f.state[h->parity] + slot[k] * Np, h->d_xfer, N,
-                                  k == 1 ? h->x_mean : 0.0, h->stream);
-      CK(cudaGetLastError());
-      CK(cudaMemcpyAsync(dst[k], h->d_xfer, N * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-    }
-    CK(cudaStreamSynchronize(h->stream));
-  }
+  const bool d = h->precision == KKS_PRECISION_FP64;
+  const int p = h->parity;
+  int rc;
+  if (eta && (rc = get_field(h, eta, h->f.eta[p], true)) != KKS_OK) return rc;
+  if (X && (rc = get_field(h, X, h->f.X[p], true)) != KKS_OK) return rc;
+  if (X_al && (rc = get_field(h, X_al, h->f.X_al[p], d)) != KKS_OK) return rc;
+  if (X_th && (rc = get_field(h, X_th, h->f.X_th[p], d)) != KKS_OK) return rc;
   return KKS_OK;
 }
+
+}  // extern "C"
+
+template <bool MIXED>
+static int elastic_impl(kks_handle* h, int p, double* d_out) {
+  KksFieldPtrs& f = h->f;
+  cudaStream_t s = h->stream;
+  kks_launch_prep<MIXED>(&h->hc, h->d_par, f, p, h->nblocks, s);
+  if (!MIXED) {
+    CKF(cufftExecD2Z(h->plan_r2c3, (double*)f.fft_in[p], (cufftDoubleComplex*)f.spec_a));
+  } else {
+    CKF(cufftExecR2C(h->plan_r2c3, (float*)f.fft_in[p], (cufftComplex*)f.spec_a));
+  }
+  kks_launch_strain_spectra<MIXED>(&h->hc, h->dc, h->d_par, f, h->nblocks, s);
+  if (!MIXED) {
+    CKF(cufftExecZ2D(h->plan_c2r3, (cufftDoubleComplex*)f.spec_bcd, (double*)f.real_b));
+  } else {
+    CKF(cufftExecC2R(h->plan_c2r3, (cufftComplex*)f.spec_bcd, (float*)f.real_b));
+  }
+  kks_launch_elastic_out<MIXED>(&h->hc, h->dc, h->d_par, f, p, d_out, d_out + 4 * (size_t)h->hc.N, h->nblocks, s);
+  CK(cudaGetLastError());
+  return KKS_OK;
+}
+
+extern "C" {
 
 int kks_elastic_fields(kks_handle* h, double* sig4, double* eps4) {
   if (!h || !sig4 || !eps4) return set_error(KKS_ERR_ARG, "null argument");
   if (!h->uploaded || h->attempts_launched == 0) return set_error(KKS_ERR_STATE, "no attempt has run yet");
   CK(cudaSetDevice(h->device));
   const int p = h->parity ^ 1;  // the last attempt read its input from the other buffer
-  const int N = h->hc.N;
+  const size_t N = h->hc.N;
   double* d_out = nullptr;
-  CK(cudaMalloc(&d_out, 8 * (size_t)N * sizeof(double)));
+  CK(cudaMalloc(&d_out, 8 * N * sizeof(double)));
   int one = 1;
-  cudaMemcpyAsync(&h->d_par->active, &one, sizeof(int), cudaMemcpyHostToDevice, h->stream);
-  KksFieldPtrs& f = h->f;
-  int rc = KKS_OK;
-  if (h->precision == KKS_PRECISION_FP64) {
-    kks_launch_square<double>(&h->hc, h->d_par, (double*)f.state[p], h->nblocks, h->stream);
-    if (cufftExecD2Z(h->plan_r2c3, (double*)f.state[p], (cufftDoubleComplex*)f.spec_a) != CUFFT_SUCCESS)
-      rc = set_error(KKS_ERR_CUFFT, "elastic R2C");
-    kks_launch_spectral_mid<double>(&h->hc, h->dc, h->d_par, f, h->stream);
-    if (cufftExecZ2D(h->plan_c2r5, (cufftDoubleComplex*)f.spec_bcd, (double*)f.real_b) != CUFFT_SUCCESS)
-      rc = set_error(KKS_ERR_CUFFT, "elastic C2R");
-    kks_launch_elastic_out<double>(&h->hc, h->dc, h->d_par, (double*)f.state[p], (double*)f.real_b, d_out,
-                                   d_out + 4 * (size_t)N, h->nblocks, h->stream);
-  } else {
-    kks_launch_square<float>(&h->hc, h->d_par, (float*)f.state[p], h->nblocks, h->stream);
-    if (cufftExecR2C(h->plan_r2c3, (float*)f.state[p], (cufftComplex*)f.spec_a) != CUFFT_SUCCESS)
-      rc = set_error(KKS_ERR_CUFFT, "elastic R2C");
-    kks_launch_spectral_mid<float>(&h->hc, h->dc, h->d_par, f, h->stream);
-    if (cufftExecC2R(h->plan_c2r5, (cufftComplex*)f.spec_bcd, (float*)f.real_b) != CUFFT_SUCCESS)
-      rc = set_error(KKS_ERR_CUFFT, "elastic C2R");
-    kks_launch_elastic_out<float>(&h->hc, h->dc, h->d_par, (float*)f.state[p], (float*)f.real_b, d_out,
-                                  d_out + 4 * (size_t)N, h->nblocks, h->stream);
+  cudaError_t e = cudaMemcpyAsync(&h->d_par->active, &one, sizeof(int), cudaMemcpyHostToDevice, h->stream);
+  int rc = e == cudaSuccess ? KKS_OK : set_error(KKS_ERR_CUDA, cudaGetErrorString(e));
+  if (rc == KKS_OK)
+    rc = h->precision == KKS_PRECISION_FP64 ? elastic_impl<false>(h, p, d_out) : elastic_impl<true>(h, p, d_out);
+  if (rc == KKS_OK) {
+    e = cudaMemcpyAsync(sig4, d_out, 4 * N * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(eps4, d_out + 4 * N, 4 * N * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) rc = set_error(KKS_ERR_CUDA, std::string("elastic fields: ") + cudaGetErrorString(e));
   }
-  cudaError_t e = cudaGetLastError();
-  if (e == cudaSuccess) e = cudaMemcpyAsync(sig4, d_out, 4 * (size_t)N * sizeof(double), cudaMemcpyDeviceToHost,
-                                            h->stream);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(eps4, d_out + 4 * (size_t)N, 4 * (size_t)N * sizeof(double),
-                                            cudaMemcpyDeviceToHost, h->stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  cudaStreamSynchronize(h->stream);
   cudaFree(d_out);
-  if (e != cudaSuccess) return set_error(KKS_ERR_CUDA, std::string("elastic fields: ") + cudaGetErrorString(e));
   return rc;
 }
 
-// checkpoint blob: header | KksCtl | x_mean | parity | state[0..1] | eta_m | X_m | mu | g[0..2]
+// checkpoint blob: header | KksCtl | state[0] | state[1] | eta_m | X_m | mu | g[0..2]
 struct CkptHeader {
   char magic[8];
   int32_t nx, ny, precision, parity;
-  double x_mean;
   uint64_t bytes;
 };
 
-static size_t ckpt_field_bytes(kks_handle* h) { return (size_t)h->hc.Np * h->rsize; }
+static size_t ckpt_bytes(kks_handle* h) {
+  const size_t Np = h->hc.Np;
+  return sizeof(CkptHeader) + sizeof(KksCtl) + 2 * h->state_bytes + 2 * Np * sizeof(double) + 4 * Np * h->rsize;
+}
+
+static void ckpt_regions(kks_handle* h, void** ptr, size_t* len) {
+  const size_t Np = h->hc.Np;
+  ptr[0] = h->f.eta[0]; len[0] = h->state_bytes;
+  ptr[1] = h->f.eta[1]; len[1] = h->state_bytes;
+  ptr[2] = h->f.eta_m; len[2] = Np * sizeof(double);
+  ptr[3] = h->f.X_m; len[3] = Np * sizeof(double);
+  ptr[4] = h->f.mu; len[4] = Np * h->rsize;
+  for (int k = 0; k < 3; ++k) { ptr[5 + k] = h->f.g[k]; len[5 + k] = Np * h->rsize; }
+}
 
 int kks_checkpoint(kks_handle* h, void* buf, size_t cap, size_t* size) {
   if (!h || !size) return set_error(KKS_ERR_ARG, "null argument");
-  const size_t fb = ckpt_field_bytes(h);
-  const size_t need = sizeof(CkptHeader) + sizeof(KksCtl) + 10 * fb + 6 * fb;
+  const size_t need = ckpt_bytes(h);
   *size = need;
   if (!buf) return KKS_OK;
   if (cap < need) return set_error(KKS_ERR_CAPACITY, "checkpoint buffer too small");
   if (!h->uploaded) return set_error(KKS_ERR_STATE, "nothing to checkpoint");
   CK(cudaSetDevice(h->device));
+  CK(cudaStreamSynchronize(h->stream));
   char* o = (char*)buf;
   CkptHeader hd;
-  memcpy(hd.magic, "KKSCKPT1", 8);
+  memcpy(hd.magic, "KKSCKPT2", 8);
   hd.nx = h->hc.nx; hd.ny = h->hc.ny; hd.precision = h->precision; hd.parity = h->parity;
-  hd.x_mean = h->x_mean;
   hd.bytes = need;
   memcpy(o, &hd, sizeof(hd)); o += sizeof(hd);
   CK(cudaMemcpy(o, h->d_ctl, sizeof(KksCtl), cudaMemcpyDeviceToHost)); o += sizeof(KksCtl);
-  for (int p = 0; p < 2; ++p) { CK(cudaMemcpy(o, h->f.state[p], 5 * fb, cudaMemcpyDeviceToHost)); o += 5 * fb; }
-  void* rest[6] = {h->f.eta_m, h->f.X_m, h->f.mu, h->f.g[0], h->f.g[1], h->f.g[2]};
-  for (void* r : rest) { CK(cudaMemcpy(o, r, fb, cudaMemcpyDeviceToHost)); o += fb; }
+  void* ptr[8];
+  size_t len[8];
+  ckpt_regions(h, ptr, len);
+  for (int k = 0; k < 8; ++k) { CK(cudaMemcpy(o, ptr[k], len[k], cudaMemcpyDeviceToHost)); o += len[k]; }
   return KKS_OK;
 }
 
 int kks_restore(kks_handle* h, const void* buf, size_t size) {
   if (!h || !buf) return set_error(KKS_ERR_ARG, "null argument");
-  const size_t fb = ckpt_field_bytes(h);
-  const size_t need = sizeof(CkptHeader) + sizeof(KksCtl) + 10 * fb + 6 * fb;
+  const size_t need = ckpt_bytes(h);
   if (size < need) return set_error(KKS_ERR_CAPACITY, "checkpoint blob too small");
   const char* o = (const char*)buf;
   CkptHeader hd;
   memcpy(&hd, o, sizeof(hd)); o += sizeof(hd);
-  if (memcmp(hd.magic, "KKSCKPT1", 8) != 0 || hd.nx != h->hc.nx || hd.ny != h->hc.ny ||
-      hd.precision != h->precision)
+  if (memcmp(hd.magic, "KKSCKPT2", 8) != 0 || hd.nx != h->hc.nx || hd.ny != h->hc.ny ||
+      hd.precision != h->precision || hd.bytes != need)
     return set_error(KKS_ERR_ARG, "checkpoint does not match this cell");
   CK(cudaSetDevice(h->device));
   CK(cudaStreamSynchronize(h->stream));
   memcpy(h->h_ctl, o, sizeof(KksCtl)); o += sizeof(KksCtl);
   h->h_ctl->target_step = h->h_ctl->istep;
   CK(cudaMemcpy(h->d_ctl, h->h_ctl, sizeof(KksCtl), cudaMemcpyHostToDevice));
-  for (int p = 0; p < 2; ++p) { CK(cudaMemcpy(h->f.state[p], o, 5 * fb, cudaMemcpyHostToDevice)); o += 5 * fb; }
-  void* rest[6] = {h->f.eta_m, h->f.X_m, h->f.mu, h->f.g[0], h->f.g[1], h->f.g[2]};
-  for (void* r : rest) { CK(cudaMemcpy(r, o, fb, cudaMemcpyHostToDevice)); o += fb; }
+  void* ptr[8];
+  size_t len[8];
+  ckpt_regions(h, ptr, len);
+  for (int k = 0; k < 8; ++k) { CK(cudaMemcpy(ptr[k], o, len[k], cudaMemcpyHostToDevice)); o += len[k]; }
+  CK(cudaMemset(h->d_par, 0, sizeof(KksPar)));
   h->parity = hd.parity;
-  h->x_mean = hd.x_mean;
-  KksPar par;
-  memset(&par, 0, sizeof(par));
-  par.x_mean = hd.x_mean;
-  CK(cudaMemcpy(h->d_par, &par, sizeof(KksPar), cudaMemcpyHostToDevice));
   h->rec_read = h->h_ctl->n_rec;
   h->row_read = h->h_ctl->n_row;
   h->recs.clear();
   h->rows.clear();
   h->uploaded = true;
+  h->attempts_launched = 0;
   return KKS_OK;
 }
 

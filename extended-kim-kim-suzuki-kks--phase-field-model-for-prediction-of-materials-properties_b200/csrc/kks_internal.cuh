@@ -2,21 +2,27 @@
 // (kks_scalar.cu), the field kernels (kks_fields.cu) and the host runtime
 // (kks_abi.cu).
 //
-// Layout in HBM of one cell (R = double for FP64, float for the mixed path;
-// Np = nx*ny rounded up to 64 elements, NCp = nx*(ny/2+1) rounded up to 32):
+// Layout in HBM of one cell (Np = nx*ny rounded up to 64 elements,
+// NCp = nx*(ny/2+1) rounded up to 32; R = double on the FP64 path, float on
+// the mixed path):
 //
-//   state[p], p = 0, 1 : R[5*Np]   eta | X | eta^2 | X_al | X_th
-//       (eta, X, eta^2 are the batch-3 R2C input; eta, X of the other parity
-//        are the batch-2 C2R output, so the attempt writes its candidate
-//        state straight into state[1-p])
+// FP64 path (the reference's formulation: new fields are inverse transforms of
+// the updated spectra)
+//   state[p], p = 0, 1 : double[5*Np]  eta | X | eta^2 | X_al | X_th
+//       (eta | X | eta^2 is the batch-3 R2C input; the batch-2 C2R writes the
+//        candidate eta_b | X_b straight into state[1-p])
+// mixed path (increment formulation: the FP32 transforms only carry the
+// step's increments, the state itself is kept in FP64)
+//   state[p]           : double eta[Np] | double X[Np] | float X_al[Np] | float X_th[Np]
+//   fft_in             : float[3*Np]   eta | X | eta^2 (batch-3 R2C input)
+//   the batch-2 C2R writes d_eta | d_X into real_c
+// both paths
 //   spec_a             : C[3*NCp]  FT(eta) | FT(X) | FT(eta^2)
-//   real_b             : R[5*Np]   eps_xx | eps_yy | eps_xy | d_x eta | d_y eta
-//   real_c             : R[3*Np]   drive | flux_x | flux_y
-//   spec_bcd           : C[5*NCp]  slots 0-4: B spectra (C2R input);
-//                                  slots 0-2: C spectra (R2C output, after B is consumed);
-//                                  slots 3-4: D spectra eta_b^, X_b^ (C2R input)
-//   eta_m, X_m, mu     : R[Np]     residual pair "minus" entry (pf_kks/solver.py:172-173)
-//   g[3]               : R[Np]     free-energy buffers rotated by index (minus, pre-update, new)
+//   real_b             : R[3*Np]   tr eps | d_x eta | d_y eta
+//   real_c             : R[3*Np]   drive | flux_x | flux_y   (mixed: then d_eta | d_X)
+//   spec_bcd           : C[5*NCp]  slots 0-2: B spectra, then C spectra; slots 3-4: D spectra
+//   eta_m, X_m         : S[Np]     residual pair "minus" entry (S = double on both paths)
+//   mu, g[3]           : R[Np]     diffusion potential, free-energy buffers rotated by index
 //   partials           : double[nblocks * KKS_NPART] block sums of the reductions
 #pragma once
 
@@ -25,19 +31,26 @@
 
 #include "kks.h"
 
-#define KKS_NPART 24
-// slots of the partial sums
+#define KKS_NPART 32
+// slots of the partial sums (every field kernel is launched with the same grid)
 enum {
-  // written by the pre-update pointwise kernel (old state)
-  P3_G = 0,      // sum G_s
-  P3_GEL,        // sum (G_s + el_s)
+  // spectral_mid: Parseval sums of the elastic energy, weight w = 1 or 2 per
+  // half-spectrum bin, p = w |FT(eta^2)|^2, O = strain multipliers
+  P2_OXX2 = 0,   // sum p Oxx^2
+  P2_OYY2,       // sum p Oyy^2
+  P2_OXXYY,      // sum p Oxx Oyy
+  P2_OXY2,       // sum p Oxy^2
+  P2_OTR,        // sum p (Oxx + Oyy)
+  P2_P,          // sum p
+  // pre_pointwise (old state)
+  P3_G,          // sum G_s
   P3_ETA,        // sum eta
   P3_XLO,        // sum X[eta < 0.05]
   P3_NLO,        // count eta < 0.05
   P3_XHI,        // sum X[eta > 0.95]
   P3_NHI,        // count eta > 0.95
   P3_IFACE,      // interface cells of eta (surface steps)
-  // written by the post-update pointwise kernel (new state)
+  // post_pointwise (new state)
   P5_GRAD2,      // sum (d_x eta_b)^2 + (d_y eta_b)^2 (np.gradient stencil)
   P5_XLO,        // sum X_b[eta_b < 0.05]
   P5_NLO,
@@ -51,6 +64,7 @@ enum {
   P5_COMB,       // sum (-diff + ac - temp)
   P_COUNT
 };
+static_assert(P_COUNT <= KKS_NPART, "partials slots");
 
 // Loop state of the cell (the scalar variables of pf_kks/solver.py:118-175),
 // read and written only by the single-thread prologue and decide kernels.
@@ -88,7 +102,6 @@ struct KksPar {
   double inv_dt, inv_Ls;
   // vertex forms of the two parabolas, for the FP32 path: f = A (c - v)^2 + f0
   double va, fa0, vt, ft0;
-  double x_mean;     // mean of X carried in FP64 (mixed path; 0 for FP64)
 };
 
 // Run constants in device memory.
@@ -97,10 +110,10 @@ struct KksConst {
   int32_t nx, ny, nyh, N, NC, Np, NCp, n_steps;
   double dtime_s_min;
   double inv_N;
-  // frozen stiffness at T0, normalised by C44(T0) (pf_kks/solver.py:152-154)
+  // frozen stiffness at T0 (pf_kks/solver.py:152-154), and normalised by C44(T0)
   double c11, c12, c3;   // C11/C44_0, C12/C44_0, (C11 + 2 C12)/C44_0
   double C11_0, C12_0, C44_0;
-  int32_t zero_dc;       // mixed path: project the mean mode of X out of the fluctuation field
+  int32_t mixed;
   int32_t pad;
 };
 
@@ -108,13 +121,17 @@ struct KksConst {
 // launchers (kks_scalar.cu)
 void kks_launch_prologue(const KksConst* c, KksCtl* ctl, KksPar* par, const uint8_t* step_flags, kks_record* ring,
                          long long ring_cap, cudaStream_t s);
-void kks_launch_decide(const KksConst* c, KksCtl* ctl, const KksPar* par, const double* partials3,
-                       const double* partials5, int nblocks, kks_record* ring, long long ring_cap,
-                       kks_step_row* rows, long long row_cap, cudaStream_t s);
+void kks_launch_decide(const KksConst* c, KksCtl* ctl, const KksPar* par, const double* partials, int nblocks,
+                       kks_record* ring, long long ring_cap, kks_step_row* rows, long long row_cap, cudaStream_t s);
 
-// launchers (kks_fields.cu); R = double or float
+// Device buffers of one cell (typed per path in kks_fields.cu).
 struct KksFieldPtrs {
-  void* state[2];
+  void* eta[2];
+  void* X[2];
+  void* X_al[2];
+  void* X_th[2];
+  void* fft_in[2];  // batch-3 R2C input (eta | X | eta^2) for an attempt of parity p
+  void* fft_out[2]; // batch-2 C2R output for an attempt of parity p
   void* spec_a;
   void* real_b;
   void* real_c;
@@ -123,35 +140,42 @@ struct KksFieldPtrs {
   void* X_m;
   void* mu;
   void* g[3];
-  double* partials3;
-  double* partials5;
+  double* partials;
   const double* kx;
   const double* ky;
 };
 
 int kks_field_blocks(int N, int num_sms);
 
-template <typename R>
-void kks_launch_square(const KksConst* hc, const KksPar* par, R* state, int nblocks, cudaStream_t s);
-template <typename R>
+// Field kernels of one attempt. MIXED selects the FP32 increment path.
+template <bool MIXED>
+void kks_launch_prep(const KksConst* hc, const KksPar* par, const KksFieldPtrs& f, int parity, int nblocks,
+                     cudaStream_t s);
+template <bool MIXED>
 void kks_launch_spectral_mid(const KksConst* hc, const KksConst* dc, const KksPar* par, const KksFieldPtrs& f,
-                             cudaStream_t s);
-template <typename R>
+                             int nblocks, cudaStream_t s);
+template <bool MIXED>
 void kks_launch_pre_pointwise(const KksConst* hc, const KksConst* dc, const KksPar* par, const KksFieldPtrs& f,
                               int parity, int nblocks, cudaStream_t s);
-template <typename R>
+template <bool MIXED>
 void kks_launch_spectral_update(const KksConst* hc, const KksConst* dc, const KksPar* par, const KksFieldPtrs& f,
-                                cudaStream_t s);
-template <typename R>
+                                int nblocks, cudaStream_t s);
+template <bool MIXED>
 void kks_launch_post_pointwise(const KksConst* hc, const KksConst* dc, const KksPar* par, const KksFieldPtrs& f,
                                int parity, int nblocks, cudaStream_t s);
+template <bool MIXED>
+void kks_launch_restore(const KksConst* hc, const KksConst* dc, const KksCtl* ctl, const KksFieldPtrs& f,
+                        int parity, int nblocks, cudaStream_t s);
+// elastic fields of the state of parity p (pf_kks/elasticity.py:107-163): the
+// three strain spectra into spec_bcd slots 0-2 (then C2R into real_b), and the
+// stress / elastic strain components xx, yy, zz, xy.
+template <bool MIXED>
+void kks_launch_strain_spectra(const KksConst* hc, const KksConst* dc, const KksPar* par, const KksFieldPtrs& f,
+                               int nblocks, cudaStream_t s);
+template <bool MIXED>
+void kks_launch_elastic_out(const KksConst* hc, const KksConst* dc, const KksPar* par, const KksFieldPtrs& f,
+                            int parity, double* sig4, double* eps4, int nblocks, cudaStream_t s);
 template <typename R>
-void kks_launch_restore(const KksConst* hc, const KksConst* dc, const KksCtl* ctl, const KksFieldPtrs& f, int parity,
-                        int nblocks, cudaStream_t s);
+void kks_launch_to_real(const double* src, R* dst, int n, cudaStream_t s);
 template <typename R>
-void kks_launch_elastic_out(const KksConst* hc, const KksConst* dc, const KksPar* par, const R* eta, const R* real_b,
-                            double* sig4, double* eps4, int nblocks, cudaStream_t s);
-template <typename R>
-void kks_launch_to_real(const double* src, R* dst, int n, double shift, cudaStream_t s);
-template <typename R>
-void kks_launch_to_double(const R* src, double* dst, int n, double shift, cudaStream_t s);
+void kks_launch_to_double(const R* src, double* dst, int n, cudaStream_t s);

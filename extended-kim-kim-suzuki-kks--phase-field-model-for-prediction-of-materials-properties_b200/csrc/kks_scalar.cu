@@ -196,7 +196,6 @@ __global__ void kks_prologue(const KksConst* __restrict__ c, KksCtl* ctl, KksPar
   q.fa0 = q.C_alp_s - q.B_alp_s * q.B_alp_s / (4 * q.A_alp_s);
   q.vt = -q.B_thet_s / (2 * q.A_thet_s);
   q.ft0 = q.C_thet_s - q.B_thet_s * q.B_thet_s / (4 * q.A_thet_s);
-  q.x_mean = par->x_mean;
   *par = q;
   ctl->attempts += 1;
 }
@@ -219,14 +218,13 @@ __device__ double block_sum(double v) {
 }
 
 __global__ void kks_decide(const KksConst* __restrict__ c, KksCtl* ctl, const KksPar* __restrict__ par,
-                           const double* __restrict__ partials3, const double* __restrict__ partials5, int nblocks,
-                           kks_record* ring, long long ring_cap, kks_step_row* rows, long long row_cap) {
+                           const double* __restrict__ partials, int nblocks, kks_record* ring, long long ring_cap,
+                           kks_step_row* rows, long long row_cap) {
   __shared__ double S[P_COUNT];
   if (!par->active) return;
   for (int k = 0; k < P_COUNT; ++k) {
-    const double* src = k < P5_GRAD2 ? partials3 : partials5;
     double v = 0;
-    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) v += src[(size_t)b * KKS_NPART + k];
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) v += partials[(size_t)b * KKS_NPART + k];
     v = block_sum(v);
     if (threadIdx.x == 0) S[k] = v;
   }
@@ -238,8 +236,19 @@ __global__ void kks_decide(const KksConst* __restrict__ c, KksCtl* ctl, const Kk
   const int iteration = ctl->iteration;
   double dtime_s = ctl->dtime_s;
 
+  // Elastic energy sum from Parseval's theorem: eps_ab^ = epsX c3 O_ab FT(eta^2)
+  // and a = epsX eta^2, so every sum of products of eps_xx, eps_yy, eps_xy and a
+  // is a weighted sum of |FT(eta^2)|^2 (sum_x f g = 1/N sum_k f^ conj(g^)).
+  const double eX = par->epsX;
+  const double A2 = (eX * c->c3) * (eX * c->c3) / Nd;
+  const double Sxx = A2 * S[P2_OXX2], Syy = A2 * S[P2_OYY2], Sxxyy = A2 * S[P2_OXXYY], Sxy2 = A2 * S[P2_OXY2];
+  const double Stra = eX * eX * c->c3 / Nd * S[P2_OTR];  // sum (eps_xx + eps_yy) a
+  const double Saa = eX * eX / Nd * S[P2_P];             // sum a^2
+  const double el_sum = 0.5 * (c->C11_0 * (Sxx + Syy - 2 * Stra + 3 * Saa) +
+                               2 * c->C12_0 * (Sxxyy - 2 * Stra + 3 * Saa) + 4 * c->C44_0 * Sxy2);
+
   // total_energy (pf_kks/free_energy.py:98-110): both gradient components carry G and el
-  const double energy_s = S[P3_GEL] * 2.0 + (0.5 * par->kappa2_s) * S[P5_GRAD2];
+  const double energy_s = (S[P3_G] + el_sum / par->C44) * 2.0 + (0.5 * par->kappa2_s) * S[P5_GRAD2];
   if (par->surface) {  // interface measure of the step's input state (pf_kks/solver.py:180-181)
     ctl->surf = S[P3_IFACE] * p.surf_scale;
     ctl->surf_valid = 1;
@@ -397,8 +406,7 @@ void kks_launch_prologue(const KksConst* c, KksCtl* ctl, KksPar* par, const uint
   kks_prologue<<<1, 32, 0, s>>>(c, ctl, par, step_flags, ring, ring_cap);
 }
 
-void kks_launch_decide(const KksConst* c, KksCtl* ctl, const KksPar* par, const double* partials3,
-                       const double* partials5, int nblocks, kks_record* ring, long long ring_cap,
-                       kks_step_row* rows, long long row_cap, cudaStream_t s) {
-  kks_decide<<<1, 256, 0, s>>>(c, ctl, par, partials3, partials5, nblocks, ring, ring_cap, rows, row_cap);
+void kks_launch_decide(const KksConst* c, KksCtl* ctl, const KksPar* par, const double* partials, int nblocks,
+                       kks_record* ring, long long ring_cap, kks_step_row* rows, long long row_cap, cudaStream_t s) {
+  kks_decide<<<1, 256, 0, s>>>(c, ctl, par, partials, nblocks, ring, ring_cap, rows, row_cap);
 }

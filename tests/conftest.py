@@ -60,10 +60,13 @@ def rel_l2(a, b):
 _NUM = re.compile(r"[-+]?\d+\.\d+(?:e[-+]\d+)?|[-+]?\d+")
 
 
-def assert_logs_equivalent(a, b):
+def assert_logs_equivalent(a, b, tiny=1e-8, tiny_rtol=0.05, zero=1e-15):
     """Logs with the same lines and decisions: the text around the numbers is
     identical, integers are equal, and reals agree within one unit of their
-    last printed digit (the log prints 3 significant digits)."""
+    last printed digit (the log prints 3 significant digits). Reals below
+    ``tiny`` in magnitude (residual terms at round-off level) may differ by
+    ``tiny_rtol`` relative, and reals below ``zero`` on both sides (sums of
+    differences of identical states: pure round-off) count as equal."""
     la, lb = a.splitlines(), b.splitlines()
     assert len(la) == len(lb), (len(la), len(lb))
     for x, y in zip(la, lb):
@@ -73,11 +76,16 @@ def assert_logs_equivalent(a, b):
                 assert u == v, (x, y)
                 continue
             fu, fv = float(u), float(v)
+            if max(abs(fu), abs(fv)) < zero:
+                continue
             if "e" in u:
                 ulp = 10.0 ** (int(u.split("e")[1]) - 2)
             else:
                 ulp = 10.0 ** -len(u.split(".")[1])
-            assert abs(fu - fv) <= 1.0001 * ulp, (x, y)
+            tol = 1.0001 * ulp
+            if abs(fv) < tiny:
+                tol = max(tol, tiny_rtol * abs(fv))
+            assert abs(fu - fv) <= tol, (x, y)
 
 
 @pytest.fixture(scope="session")
