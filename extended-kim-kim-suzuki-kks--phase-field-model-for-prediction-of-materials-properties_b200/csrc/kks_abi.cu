@@ -32,6 +32,8 @@ static int set_error(int code, const std::string& msg) {
   return code;
 }
 
+int kks_set_error(int code, const std::string& msg) { return set_error(code, msg); }
+
 #define CK(expr)                                                                                          \
   do {                                                                                                    \
     cudaError_t _e = (expr);                                                                              \

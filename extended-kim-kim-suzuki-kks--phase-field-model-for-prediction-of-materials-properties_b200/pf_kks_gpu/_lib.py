@@ -44,6 +44,7 @@ H = {
 EXPORTS = (
     "kks_create", "kks_upload", "kks_run", "kks_drain", "kks_get_state", "kks_download", "kks_elastic_fields",
     "kks_checkpoint", "kks_restore", "kks_timing", "kks_destroy", "kks_last_error", "kks_version",
+    "kks_state_sums_noalloc",
 )
 
 
@@ -123,6 +124,8 @@ def load(path=LIB_PATH):
     lib.kks_restore.argtypes = [vp, vp, ctypes.c_size_t]
     lib.kks_timing.argtypes = [vp, dp, P(ctypes.c_int64)]
     lib.kks_destroy.argtypes = [vp]
+    lib.kks_state_sums_noalloc.argtypes = [vp, vp, ctypes.c_int32, ctypes.c_int32, vp, vp]
+    lib.kks_state_sums_noalloc.restype = ctypes.c_int
     lib.kks_last_error.restype = ctypes.c_char_p
     lib.kks_version.restype = ctypes.c_char_p
     for name in ("kks_create", "kks_upload", "kks_run", "kks_drain", "kks_get_state", "kks_download",

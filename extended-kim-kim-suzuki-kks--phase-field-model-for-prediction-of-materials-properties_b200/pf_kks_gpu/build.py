@@ -29,6 +29,7 @@ SOURCES = {
     "kks_scalar.cu": ["-fmad=false"],
     "kks_fields.cu": [],
     "kks_abi.cu": [],
+    "kks_noalloc.cu": [],
 }
 
 

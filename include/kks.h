@@ -159,6 +159,26 @@ int kks_timing(kks_handle* h, double* device_ms, int64_t* attempts);
 
 int kks_destroy(kks_handle* h);
 
+/* No counterpart in the reference. For callers that cannot allocate device
+ * memory (a framework that owns all device memory through its own pool, or a
+ * latency-critical loop that must not call cudaMalloc / cudaFree because they
+ * may synchronise the device): the sums behind the old-state histories of one
+ * step (pf_kks/solver.py:380-395) and the interface cell count
+ * (pf_kks/microstructure.py:117-128) of a state already in device memory, with
+ * no allocation. eta, X: device float64, nx*ny each (C order); out: device
+ * float64[6] = { sum eta, sum X[eta < 0.05], count(eta < 0.05),
+ * sum X[eta > 0.95], count(eta > 0.95), cells with 4 corners in [0.1, 0.9] }.
+ * Runs asynchronously on `stream` (a cudaStream_t, NULL = default stream).
+ * Its scratch is a fixed device array of KKS_NOALLOC_MAX_BLOCKS x 6 doubles
+ * (48 KiB) held by every GPU that loads the library; nx*ny above
+ * KKS_NOALLOC_MAX_POINTS is rejected with KKS_ERR_CAPACITY. The first call on
+ * a device looks up that array's address (make it before any stream capture).
+ * Calls share the array: calls that overlap on the GPU race and must be
+ * serialised by the caller. */
+#define KKS_NOALLOC_MAX_BLOCKS 1024
+#define KKS_NOALLOC_MAX_POINTS (1 << 26)
+int kks_state_sums_noalloc(const double* eta, const double* X, int32_t nx, int32_t ny, double* out, void* stream);
+
 /* Message of the last error of this thread. */
 const char* kks_last_error(void);
 
