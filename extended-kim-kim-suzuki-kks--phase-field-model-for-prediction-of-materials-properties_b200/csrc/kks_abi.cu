@@ -23,6 +23,7 @@
 #include <string>
 #include <vector>
 
+#include "kks_fft.cuh"
 #include "kks_internal.cuh"
 
 static thread_local std::string g_last_error;
@@ -82,6 +83,13 @@ struct kks_handle {
   double device_ms = 0.0;
   long long timed_attempts = 0;
   long long attempts_launched = 0;
+  // shared-memory FFT pipeline of the mixed path (kks_fft.cu)
+  bool fused = false;
+  void* fft_arena = nullptr;
+  KksFftConst* d_fc = nullptr;
+  KksFftLaunch fl{};
+  double* partials_fused = nullptr;
+  int nb_fused = 0;
 };
 
 static size_t round_up(size_t v, size_t m) { return (v + m - 1) / m * m; }
@@ -155,8 +163,174 @@ static int enqueue_attempt(kks_handle* h, int p) {
   return KKS_OK;
 }
 
+static int enqueue_fused(kks_handle* h, int p) {
+  cudaStream_t s = h->stream;
+  kks_launch_prologue(h->dc, h->d_ctl, h->d_par, h->d_flags, h->d_ring, h->ring_cap, s);
+  kks_fft_launch_attempt(h->fl, p, s);
+  kks_launch_decide(h->dc, h->d_ctl, h->d_par, h->partials_fused, h->nb_fused, h->d_ring, h->ring_cap, h->d_rows,
+                    h->row_cap, s);
+  kks_launch_restore<true>(&h->hc, h->dc, h->d_ctl, h->f, p, h->nblocks, s);
+  CK(cudaGetLastError());
+  return KKS_OK;
+}
+
 static int enqueue(kks_handle* h, int p) {
+  if (h->fused) return enqueue_fused(h, p);
   return h->precision == KKS_PRECISION_FP64 ? enqueue_attempt<false>(h, p) : enqueue_attempt<true>(h, p);
+}
+
+// ---------------------------------------------------------------------------
+// Plans of the shared-memory FFT (kks_fft.cu): radices 4, 2, 3, 5, 7 and at
+// most one larger prime from KKS_FFT_PRIMES as the last DIF stage.
+struct AxisTables {
+  std::vector<float2> tw;
+  std::vector<float4> prow;
+  std::vector<int> slot;
+};
+
+static bool build_axis(int n, KksFftAxis& ax, AxisTables& t) {
+  std::vector<int> rad;
+  int m = n;
+  for (int r : {4, 2, 3, 5, 7})
+    while (m % r == 0) { rad.push_back(r); m /= r; }
+  int P = 0;
+  if (m > 1) {
+    bool ok = false;
+    for (int p : KKS_FFT_PRIMES) ok = ok || (m == p);
+    if (!ok) return false;
+    P = m;
+    rad.push_back(m);
+  }
+  if ((int)rad.size() > KKS_FFT_MAXST || rad.empty()) return false;
+  memset(&ax, 0, sizeof(ax));
+  ax.n = n;
+  ax.nst = (int)rad.size();
+  ax.P = P;
+  int L = n;
+  t.tw.clear();
+  for (int s = 0; s < ax.nst; ++s) {
+    const int r = rad[s], q = L / r;
+    ax.r[s] = r;
+    ax.L[s] = L;
+    ax.q[s] = q;
+    ax.tw_off[s] = (int)t.tw.size();
+    if (q > 1)
+      for (int j = 0; j < q; ++j)
+        for (int mm = 0; mm < r; ++mm) {
+          const double th = 2.0 * M_PI * (double)((long long)j * mm % L) / (double)L;
+          t.tw.push_back(make_float2((float)cos(th), (float)sin(th)));
+        }
+    L = q;
+  }
+  if (t.tw.empty()) t.tw.push_back(make_float2(1.f, 0.f));
+  t.prow.clear();
+  if (P) {
+    const int H = (P - 1) / 2, H2 = (H + 1) / 2;
+    for (int k = 1; k <= H; ++k)
+      for (int h = 0; h < H2; ++h) {
+        const int n0 = 2 * h + 1, n1 = 2 * h + 2;
+        const double a0 = 2.0 * M_PI * (double)((long long)n0 * k % P) / P;
+        const double a1 = 2.0 * M_PI * (double)((long long)n1 * k % P) / P;
+        float4 v;
+        v.x = (float)cos(a0);
+        v.y = (float)sin(a0);
+        v.z = n1 <= H ? (float)cos(a1) : 0.f;
+        v.w = n1 <= H ? (float)sin(a1) : 0.f;
+        t.prow.push_back(v);
+      }
+  } else {
+    t.prow.push_back(make_float4(0.f, 0.f, 0.f, 0.f));
+  }
+  // position of frequency k after the DIF: digits d_s of the position (weights q_s)
+  // are the digits of k read with weights r_0 r_1 ... r_{s-1}
+  t.slot.assign(n, 0);
+  for (int pos = 0; pos < n; ++pos) {
+    int rem = pos, k = 0, w = 1;
+    for (int s = 0; s < ax.nst; ++s) {
+      const int d = rem / ax.q[s];
+      rem = rem % ax.q[s];
+      k += d * w;
+      w *= ax.r[s];
+    }
+    t.slot[k] = pos;
+  }
+  return true;
+}
+
+template <typename T>
+static int upload_vec(const std::vector<T>& v, T** dst) {
+  CK(cudaMalloc(dst, v.size() * sizeof(T)));
+  CK(cudaMemcpy(*dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return KKS_OK;
+}
+
+static int setup_fused(kks_handle* h, const std::vector<double>& kx) {
+  KksConst& c = h->hc;
+  KksFftConst fc;
+  memset(&fc, 0, sizeof(fc));
+  AxisTables tx, ty;
+  if (!build_axis(c.nx, fc.ax, tx) || !build_axis(c.ny, fc.ay, ty)) return KKS_OK;  // not supported: cuFFT
+  int optin = 0;
+  CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device));
+  const size_t col_smem = 2 * (size_t)KKS_FFT_COLS * c.nx * sizeof(float2) + 4096;
+  const size_t row_smem = 3 * (size_t)c.ny * sizeof(float2) + 4096;
+  if (col_smem > (size_t)optin || row_smem > (size_t)optin) return KKS_OK;
+  std::vector<float> kx_slot(c.nx);
+  for (int k = 0; k < c.nx; ++k) kx_slot[tx.slot[k]] = (float)kx[k];
+  // device tables and buffers in one allocation
+  const size_t fs = (size_t)c.nx * c.nyh * sizeof(float2);
+  auto al = [](size_t b) { return (b + 255) / 256 * 256; };
+  const size_t b_twx = al(tx.tw.size() * sizeof(float2)), b_twy = al(ty.tw.size() * sizeof(float2));
+  const size_t b_prx = al(tx.prow.size() * sizeof(float4)), b_pry = al(ty.prow.size() * sizeof(float4));
+  const size_t b_slx = al(tx.slot.size() * sizeof(int)), b_sly = al(ty.slot.size() * sizeof(int));
+  const size_t b_kxs = al(kx_slot.size() * sizeof(float));
+  const size_t b_spec = al(3 * fs) * 2 + al(2 * fs);
+  const size_t total = b_twx + b_twy + b_prx + b_pry + b_slx + b_sly + b_kxs + b_spec;
+  CK(cudaMalloc(&h->fft_arena, total));
+  char* a = (char*)h->fft_arena;
+  auto put = [&](const void* src, size_t n, size_t b) -> char* {
+    char* p = a;
+    cudaMemcpy(p, src, n, cudaMemcpyHostToDevice);
+    a += b;
+    return p;
+  };
+  fc.ax.tw = (const float2*)put(tx.tw.data(), tx.tw.size() * sizeof(float2), b_twx);
+  fc.ay.tw = (const float2*)put(ty.tw.data(), ty.tw.size() * sizeof(float2), b_twy);
+  fc.ax.prow = (const float2*)put(tx.prow.data(), tx.prow.size() * sizeof(float4), b_prx);
+  fc.ay.prow = (const float2*)put(ty.prow.data(), ty.prow.size() * sizeof(float4), b_pry);
+  fc.ax.slot = (const int*)put(tx.slot.data(), tx.slot.size() * sizeof(int), b_slx);
+  fc.ay.slot = (const int*)put(ty.slot.data(), ty.slot.size() * sizeof(int), b_sly);
+  fc.kx_slot = (const float*)put(kx_slot.data(), kx_slot.size() * sizeof(float), b_kxs);
+  CK(cudaGetLastError());
+  void* RA = a; a += al(3 * fs);
+  void* RB = a; a += al(3 * fs);
+  void* SA = a; a += al(2 * fs);
+  CK(cudaMemset(RA, 0, b_spec));
+  CK(cudaMalloc(&h->d_fc, sizeof(KksFftConst)));
+  CK(cudaMemcpy(h->d_fc, &fc, sizeof(KksFftConst), cudaMemcpyHostToDevice));
+  KksFftLaunch& L = h->fl;
+  L.dc = h->dc;
+  L.par = h->d_par;
+  L.fc = h->d_fc;
+  L.f = &h->f;
+  L.RA = RA;
+  L.RB = RB;
+  L.SA = SA;
+  L.nx = c.nx;
+  L.ny = c.ny;
+  L.nyh = c.nyh;
+  L.nbx = h->nblocks;
+  L.PX = fc.ax.P;
+  L.PY = fc.ay.P;
+  if (kks_fft_set_attributes(L) != 0) return set_error(KKS_ERR_CUDA, "fft kernel attributes");
+  // every kernel of the pipeline writes one partial-sum row per block: the
+  // buffer holds the largest grid of them (row pairs, column tiles, extras)
+  h->nb_fused = std::max(kks_fft_partial_rows(c.nx, c.ny, L.nbx), h->nblocks);
+  CK(cudaMalloc(&h->partials_fused, (size_t)h->nb_fused * KKS_NPART * sizeof(double)));
+  CK(cudaMemset(h->partials_fused, 0, (size_t)h->nb_fused * KKS_NPART * sizeof(double)));
+  h->f.partials = h->partials_fused;
+  h->fused = true;
+  return KKS_OK;
 }
 
 static int make_plans(kks_handle* h) {
@@ -215,6 +389,9 @@ static void free_handle(kks_handle* h) {
     cufftDestroy(h->plan_c2r2);
   }
   cudaFree(h->fft_work);
+  cudaFree(h->fft_arena);
+  cudaFree(h->d_fc);
+  cudaFree(h->partials_fused);
   cudaFree(h->arena);
   cudaFree(h->dc);
   cudaFree(h->d_ctl);
@@ -258,13 +435,14 @@ static int create_impl(kks_handle* h, const kks_params* prm, int32_t n_steps, co
   c.c12 = c.C12_0 / c.C44_0;
   c.c3 = (c.C11_0 + 2 * c.C12_0) / c.C44_0;
   h->rsize = h->precision == KKS_PRECISION_FP64 ? 8 : 4;
+  c.mixed = h->precision != KKS_PRECISION_FP64;
 
   int nsm = 148;
   CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device));
   h->nblocks = kks_field_blocks(c.N, nsm);
 
   // arena (layout in kks_internal.cuh)
-  const bool mixed = h->precision == KKS_PRECISION_MIXED;
+  const bool mixed = h->precision != KKS_PRECISION_FP64;
   c.mixed = mixed;
   const size_t R = h->rsize, Np = c.Np, NCp = c.NCp, D = sizeof(double);
   const size_t sz_state = mixed ? 2 * Np * D + 2 * Np * R : 5 * Np * D;
@@ -336,6 +514,10 @@ static int create_impl(kks_handle* h, const kks_params* prm, int32_t n_steps, co
 
   int rc = make_plans(h);
   if (rc != KKS_OK) return rc;
+  if (h->precision == KKS_PRECISION_MIXED) {
+    rc = setup_fused(h, kx);
+    if (rc != KKS_OK) return rc;
+  }
   rc = capture_graphs(h);
   if (rc != KKS_OK) return rc;
   CK(cudaStreamSynchronize(h->stream));
@@ -354,8 +536,8 @@ int kks_create(const kks_params* params, int precision, int device, int32_t n_st
   *out = nullptr;
   if (params->nx < 2 || params->ny < 2) return set_error(KKS_ERR_ARG, "nx and ny must be >= 2 (np.gradient)");
   if ((long long)params->nx * params->ny > (1LL << 30)) return set_error(KKS_ERR_ARG, "grid too large");
-  if (precision != KKS_PRECISION_FP64 && precision != KKS_PRECISION_MIXED)
-    return set_error(KKS_ERR_ARG, "precision must be KKS_PRECISION_FP64 or KKS_PRECISION_MIXED");
+  if (precision != KKS_PRECISION_FP64 && precision != KKS_PRECISION_MIXED && precision != KKS_PRECISION_MIXED_CUFFT)
+    return set_error(KKS_ERR_ARG, "precision must be KKS_PRECISION_FP64, _MIXED or _MIXED_CUFFT");
   if (params->n_sched < 1 || params->n_sched > KKS_MAX_SCHED)
     return set_error(KKS_ERR_ARG, "schedule length out of range");
   if (params->n_table < 1 || params->n_table > KKS_MAX_TABLE)
@@ -491,6 +673,62 @@ int kks_run(kks_handle* h, int32_t n_steps, int32_t* status) {
   h->timed_attempts += launched;
   h->attempts_launched += launched;
   if (status) *status = c->status;
+  return KKS_OK;
+}
+
+int kks_run_many(kks_handle** cells, int32_t n_cells, const int32_t* n_steps, int32_t* status) {
+  if (!cells || n_cells < 0 || (n_cells > 0 && !n_steps)) return set_error(KKS_ERR_ARG, "bad argument");
+  std::vector<long long> target(n_cells), launched(n_cells, 0);
+  for (int i = 0; i < n_cells; ++i) {
+    kks_handle* h = cells[i];
+    if (!h || n_steps[i] < 0) return set_error(KKS_ERR_ARG, "bad cell or step count");
+    if (!h->uploaded) return set_error(KKS_ERR_STATE, "kks_run_many before kks_upload");
+    if (i > 0 && h->device != cells[0]->device) return set_error(KKS_ERR_ARG, "cells must share one device");
+    target[i] = (long long)h->h_ctl->istep + n_steps[i];
+    if (target[i] > h->hc.n_steps) return set_error(KKS_ERR_ARG, "run beyond the scheduled number of steps");
+  }
+  if (n_cells == 0) return KKS_OK;
+  CK(cudaSetDevice(cells[0]->device));
+  for (int i = 0; i < n_cells; ++i) {
+    kks_handle* h = cells[i];
+    *h->h_target = (int32_t)target[i];
+    CK(cudaMemcpyAsync(&h->d_ctl->target_step, h->h_target, sizeof(int32_t), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaEventRecord(h->ev0, h->stream));
+  }
+  for (;;) {
+    bool any = false;
+    for (int i = 0; i < n_cells; ++i) {
+      kks_handle* h = cells[i];
+      KksCtl* c = h->h_ctl;
+      if (c->istep >= target[i] || c->status != KKS_STATUS_OK) continue;
+      const long long max_batch = std::max(1LL, std::min(h->ring_cap / 2 - 1, h->row_cap - 1));
+      const long long todo = std::min(target[i] - c->istep, max_batch);
+      for (long long a = 0; a < todo; ++a) {
+        CK(cudaGraphLaunch(h->graph[h->parity], h->stream));
+        h->parity ^= 1;
+      }
+      launched[i] += todo;
+      CK(cudaMemcpyAsync(c, h->d_ctl, sizeof(KksCtl), cudaMemcpyDeviceToHost, h->stream));
+      any = true;
+    }
+    if (!any) break;
+    for (int i = 0; i < n_cells; ++i) {
+      CK(cudaStreamSynchronize(cells[i]->stream));
+      int rc = drain_device(cells[i]);
+      if (rc != KKS_OK) return rc;
+    }
+  }
+  for (int i = 0; i < n_cells; ++i) {
+    kks_handle* h = cells[i];
+    CK(cudaEventRecord(h->ev1, h->stream));
+    CK(cudaEventSynchronize(h->ev1));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+    h->device_ms += ms;
+    h->timed_attempts += launched[i];
+    h->attempts_launched += launched[i];
+    if (status) status[i] = h->h_ctl->status;
+  }
   return KKS_OK;
 }
 

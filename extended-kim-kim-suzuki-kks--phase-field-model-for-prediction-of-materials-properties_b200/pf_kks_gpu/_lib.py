@@ -18,6 +18,7 @@ KKS_STATUS_MAX_ITER = 1
 KKS_STATUS_NONFINITE = 2
 KKS_PRECISION_FP64 = 0
 KKS_PRECISION_MIXED = 1
+KKS_PRECISION_MIXED_CUFFT = 2
 KKS_MAX_SCHED = 64
 KKS_MAX_TABLE = 32
 KKS_NTAB = 13
@@ -44,7 +45,7 @@ H = {
 EXPORTS = (
     "kks_create", "kks_upload", "kks_run", "kks_drain", "kks_get_state", "kks_download", "kks_elastic_fields",
     "kks_checkpoint", "kks_restore", "kks_timing", "kks_destroy", "kks_last_error", "kks_version",
-    "kks_state_sums_noalloc",
+    "kks_state_sums_noalloc", "kks_run_many",
 )
 
 
@@ -124,6 +125,8 @@ def load(path=LIB_PATH):
     lib.kks_restore.argtypes = [vp, vp, ctypes.c_size_t]
     lib.kks_timing.argtypes = [vp, dp, P(ctypes.c_int64)]
     lib.kks_destroy.argtypes = [vp]
+    lib.kks_run_many.argtypes = [P(vp), ctypes.c_int32, P(ctypes.c_int32), P(ctypes.c_int32)]
+    lib.kks_run_many.restype = ctypes.c_int
     lib.kks_state_sums_noalloc.argtypes = [vp, vp, ctypes.c_int32, ctypes.c_int32, vp, vp]
     lib.kks_state_sums_noalloc.restype = ctypes.c_int
     lib.kks_last_error.restype = ctypes.c_char_p

@@ -29,6 +29,7 @@ SOURCES = {
     "kks_scalar.cu": ["-fmad=false"],
     "kks_fields.cu": [],
     "kks_abi.cu": [],
+    "kks_fft.cu": [],
     "kks_noalloc.cu": [],
 }
 
@@ -45,7 +46,8 @@ def cuda_home():
 
 def _deps(src):
     """Sources plus the headers they include."""
-    return [src, os.path.join(CSRC, "kks_internal.cuh"), os.path.join(INCLUDE, "kks.h")]
+    return [src, os.path.join(CSRC, "kks_internal.cuh"), os.path.join(CSRC, "kks_fft.cuh"),
+            os.path.join(INCLUDE, "kks.h")]
 
 
 def _stale(target, deps):

@@ -16,16 +16,18 @@ from dataclasses import asdict, dataclass, field, fields
 
 import tomllib
 
-PRECISIONS = ("fp64", "mixed")
+PRECISIONS = ("fp64", "mixed", "mixed-cufft")
 
 
 @dataclass
 class GpuOptions:
     """Options of the GPU step (``[gpu]`` TOML section).
 
-    precision : "fp64" (all-FP64 step, parity with the reference) or "mixed"
-        (FP32 fields, transforms and pointwise math; FP64 scalars, phase
-        compositions, mean mode of X and reductions).
+    precision : "fp64" (all-FP64 step, parity with the reference), "mixed"
+        (FP32 transforms and pointwise math on the step increments with
+        hand-written shared-memory FFTs; FP64 state, scalars, phase
+        compositions and reductions) or "mixed-cufft" (the same step with
+        cuFFT transforms).
     device : CUDA device ordinal.
     records_capacity : size of the device ring of per-attempt log records.
     """

@@ -59,32 +59,49 @@ def gather_results(local, group=None):
     return merged
 
 
-def run_shard(cells, n_steps, device=0):
-    """Advance every (cfg, tables, state) cell of this shard by ``n_steps``
-    steps on one GPU, interleaving their batches so that cells overlap.
+class Ensemble:
+    """Cells of one shard resident on one GPU, advanced together by
+    ``kks_run_many`` (each cell on its own stream with its own graphs, one host
+    synchronisation per batch for all of them)."""
 
-    Returns {index: dict(status, steps, attempts, device_ms, fields)}.
-    """
-    from .solver import Cell
+    def __init__(self, members, precision="mixed", device=0):
+        import ctypes
 
-    handles = {}
-    for idx, (cfg, tables, state) in cells.items():
-        c = Cell(cfg, tables, precision=cfg.gpu_options.precision, device=device)
-        c.upload(*state)
-        handles[idx] = c
-    t0 = time.perf_counter()
-    out = {}
-    for idx, c in handles.items():
-        st = c.run(n_steps)
-        c.drain()
-        s = c.state()
-        ms, att = c.timing()
-        out[idx] = {"status": st, "steps": int(s.istep), "attempts": int(s.attempts), "device_ms": ms,
-                    "eta": None, "X": None}
-    wall = time.perf_counter() - t0
-    for idx, c in handles.items():
-        e, x, _, _ = c.download()
-        out[idx]["eta_mean"] = float(np.mean(e))
-        out[idx]["X_mean"] = float(np.mean(x))
-        c.close()
-    return out, wall
+        from .materials import MaterialTables
+        from .solver import Cell
+
+        self.cells = []
+        for cfg, state in members:
+            tables = MaterialTables.from_npz(cfg.material_tables, cfg.c_gamma, cfg.c_eps0)
+            c = Cell(cfg, tables, precision=precision, device=device)
+            c.upload(*state)
+            self.cells.append(c)
+        self._ptrs = (ctypes.c_void_p * len(self.cells))(*[c.h.value for c in self.cells])
+        self.points = [c.N for c in self.cells]
+
+    def run(self, n_steps):
+        """Advance every cell by ``n_steps`` steps; returns the status per cell."""
+        import ctypes
+
+        from . import _lib as L
+
+        n = len(self.cells)
+        steps = (ctypes.c_int32 * n)(*([int(n_steps)] * n))
+        status = (ctypes.c_int32 * n)()
+        L.check(L.load().kks_run_many(self._ptrs, n, steps, status), "kks_run_many")
+        for c in self.cells:
+            c.drain()
+        return list(status)
+
+    def run_sequential(self, n_steps):
+        """The same steps, one cell after the other (the comparison baseline)."""
+        out = []
+        for c in self.cells:
+            out.append(c.run(n_steps))
+            c.drain()
+        return out
+
+    def close(self):
+        for c in self.cells:
+            c.close()
+        self.cells = []

@@ -138,7 +138,8 @@ class Cell:
             if 1 <= s <= self.n_steps:
                 flags[s - 1] |= 1
         self._flags = flags
-        prec = {"fp64": L.KKS_PRECISION_FP64, "mixed": L.KKS_PRECISION_MIXED}[precision]
+        prec = {"fp64": L.KKS_PRECISION_FP64, "mixed": L.KKS_PRECISION_MIXED,
+                "mixed-cufft": L.KKS_PRECISION_MIXED_CUFFT}[precision]
         self.precision = precision
         self.params = make_params(cfg, tables)
         h = ctypes.c_void_p()

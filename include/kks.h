@@ -41,7 +41,10 @@ extern "C" {
 #define KKS_STATUS_NONFINITE 2  /* AdaptiveStepError: non-finite energy residual */
 
 #define KKS_PRECISION_FP64 0  /* all-FP64 step */
-#define KKS_PRECISION_MIXED 1 /* FP32 fields / FFTs / pointwise; FP64 scalars, phase compositions, mean X mode, sums */
+#define KKS_PRECISION_MIXED 1 /* FP32 transforms and pointwise math on the step increments; FP64 state, scalars,
+                                 phase compositions and sums; hand-written shared-memory FFTs where the grid
+                                 factors into 2, 3, 4, 5, 7 and at most one of 11, 19, 71, else cuFFT */
+#define KKS_PRECISION_MIXED_CUFFT 2 /* the mixed step with cuFFT transforms (comparison path) */
 
 #define KKS_MAX_SCHED 64
 #define KKS_MAX_TABLE 32
@@ -131,6 +134,13 @@ int kks_upload(kks_handle* h, const double* eta, const double* X, const double* 
  * without a host synchronisation per attempt; returns when the steps are done
  * or the device status is not OK. *status receives KKS_STATUS_*. */
 int kks_run(kks_handle* h, int32_t n_steps, int32_t* status);
+
+/* Advance several cells together (an ensemble): cell i by n_steps[i] steps.
+ * Each cell keeps its own stream, graphs, adaptive dt and rejections; the
+ * batches of all cells are launched before one synchronisation, so small
+ * cells run concurrently on the GPU. status[i] receives KKS_STATUS_* per cell.
+ * Replaces running pf_kks.solver.run (pf_kks/solver.py:76-414) once per cell. */
+int kks_run_many(kks_handle** cells, int32_t n_cells, const int32_t* n_steps, int32_t* status);
 
 /* Copy the log records and history rows produced since the last drain. */
 int kks_drain(kks_handle* h, kks_record* records, int64_t record_cap, int64_t* n_records, kks_step_row* rows,

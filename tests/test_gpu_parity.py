@@ -187,3 +187,46 @@ def test_checkpoint_restore_is_exact(precision):
     assert b.state().istep == a.state().istep == 25
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("shape", [(160, 160), (45, 38), (33, 64), (64, 31), (40, 50)])
+def test_fused_fft_path_matches_oracle(tmp_path, shape):
+    """The mixed step with the hand-written shared-memory FFTs (radices 2, 3,
+    4, 5, 7 and the prime stages 11, 19, 71) against the FP64 oracle, and
+    against the same step with cuFFT transforms."""
+    from oracle import kks_oracle
+    from pf_kks_gpu import workloads
+    from pf_kks_gpu.generator import MicrostructureSpec
+
+    nx, ny = shape
+    cfg = workloads.base_config(nx=nx, ny=ny, n_steps=15, n_map_saves=2, n_surface_samples=5)
+    spec = MicrostructureSpec(nx, ny, n_cells=3, n_particles=max(3, nx * ny // 600), seed=11)
+    state = workloads.initial_state(cfg, spec)
+    fused = _run_gpu(cfg, state, tmp_path / "fused", precision="mixed")
+    cuf = _run_gpu(cfg, state, tmp_path / "cufft", precision="mixed-cufft")
+    ref = kks_oracle.run(cfg, *copy_state(state), cfg.material_tables, out_dir=str(tmp_path / "cpu"))
+    for name in ("eta", "X"):
+        assert rel_l2(getattr(fused, name), getattr(ref, name)) <= 1e-6, name
+        assert rel_l2(getattr(fused, name), getattr(cuf, name)) <= 1e-6, name
+    for name in ("X_al", "X_th"):
+        assert rel_l2(getattr(fused, name), getattr(ref, name)) <= 1e-5, name
+    for name in ("eta_mean", "X_al_mean", "surf", "energy_s"):
+        np.testing.assert_allclose(np.asarray(fused.history[name], float), np.asarray(ref.history[name], float),
+                                   rtol=1e-5, atol=1e-12, err_msg=name)
+    # mass moves only by the FP32 round-off of the increments (large on these
+    # small, sharp initial states)
+    assert abs(fused.X.mean() - state[1].mean()) <= 1e-8
+
+
+def test_fused_fft_1420_short_run(tmp_path):
+    """The bench grid (1420 = 4 * 5 * 71): three steps of the fused mixed step
+    against the FP64 GPU step."""
+    from pf_kks_gpu import workloads
+
+    cfg, spec = workloads.ramp1420(n_steps=3)
+    state = workloads.initial_state(cfg, spec)
+    fused = _run_gpu(cfg, state, tmp_path / "fused", precision="mixed")
+    f64 = _run_gpu(cfg, state, tmp_path / "fp64", precision="fp64")
+    for name in ("eta", "X"):
+        assert rel_l2(getattr(fused, name), getattr(f64, name)) <= 1e-6, name
+    np.testing.assert_allclose(fused.history["energy_s"], f64.history["energy_s"], rtol=1e-6)
