@@ -184,9 +184,13 @@ static int enqueue(kks_handle* h, int p) {
 // most one larger prime from KKS_FFT_PRIMES as the last DIF stage.
 struct AxisTables {
   std::vector<float2> tw;
-  std::vector<float4> prow;
   std::vector<int> slot;
 };
+
+// ceil(2^32 / d) for the device's x / d == __umulhi(x, m) (x, d < 2^16); 0 for d = 1
+static uint32_t div_magic(int d) {
+  return d <= 1 ? 0u : (uint32_t)((((uint64_t)1 << 32) + (uint64_t)d - 1) / (uint64_t)d);
+}
 
 static bool build_axis(int n, KksFftAxis& ax, AxisTables& t) {
   std::vector<int> rad;
@@ -201,7 +205,7 @@ static bool build_axis(int n, KksFftAxis& ax, AxisTables& t) {
     P = m;
     rad.push_back(m);
   }
-  if ((int)rad.size() > KKS_FFT_MAXST || rad.empty()) return false;
+  if ((int)rad.size() > KKS_FFT_MAXST || rad.empty() || n > KKS_FFT_MAXN) return false;
   memset(&ax, 0, sizeof(ax));
   ax.n = n;
   ax.nst = (int)rad.size();
@@ -214,6 +218,8 @@ static bool build_axis(int n, KksFftAxis& ax, AxisTables& t) {
     ax.L[s] = L;
     ax.q[s] = q;
     ax.tw_off[s] = (int)t.tw.size();
+    ax.qm[s] = div_magic(q);
+    ax.pm[s] = div_magic(n / r);
     if (q > 1)
       for (int j = 0; j < q; ++j)
         for (int mm = 0; mm < r; ++mm) {
@@ -223,24 +229,6 @@ static bool build_axis(int n, KksFftAxis& ax, AxisTables& t) {
     L = q;
   }
   if (t.tw.empty()) t.tw.push_back(make_float2(1.f, 0.f));
-  t.prow.clear();
-  if (P) {
-    const int H = (P - 1) / 2, H2 = (H + 1) / 2;
-    for (int k = 1; k <= H; ++k)
-      for (int h = 0; h < H2; ++h) {
-        const int n0 = 2 * h + 1, n1 = 2 * h + 2;
-        const double a0 = 2.0 * M_PI * (double)((long long)n0 * k % P) / P;
-        const double a1 = 2.0 * M_PI * (double)((long long)n1 * k % P) / P;
-        float4 v;
-        v.x = (float)cos(a0);
-        v.y = (float)sin(a0);
-        v.z = n1 <= H ? (float)cos(a1) : 0.f;
-        v.w = n1 <= H ? (float)sin(a1) : 0.f;
-        t.prow.push_back(v);
-      }
-  } else {
-    t.prow.push_back(make_float4(0.f, 0.f, 0.f, 0.f));
-  }
   // position of frequency k after the DIF: digits d_s of the position (weights q_s)
   // are the digits of k read with weights r_0 r_1 ... r_{s-1}
   t.slot.assign(n, 0);
@@ -272,36 +260,34 @@ static int setup_fused(kks_handle* h, const std::vector<double>& kx) {
   if (!build_axis(c.nx, fc.ax, tx) || !build_axis(c.ny, fc.ay, ty)) return KKS_OK;  // not supported: cuFFT
   int optin = 0;
   CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device));
-  const size_t col_smem = 2 * (size_t)KKS_FFT_COLS * c.nx * sizeof(float2) + 4096;
-  const size_t row_smem = 3 * (size_t)c.ny * sizeof(float2) + 4096;
-  if (col_smem > (size_t)optin || row_smem > (size_t)optin) return KKS_OK;
+  if (kks_fft_smem_bytes(c.nx, c.ny) > (size_t)optin) return KKS_OK;
+  if (kks_fft_upload_prime_tables() != 0) return set_error(KKS_ERR_CUDA, "fft prime tables");
   std::vector<float> kx_slot(c.nx);
   for (int k = 0; k < c.nx; ++k) kx_slot[tx.slot[k]] = (float)kx[k];
   // device tables and buffers in one allocation
   const size_t fs = (size_t)c.nx * c.nyh * sizeof(float2);
   auto al = [](size_t b) { return (b + 255) / 256 * 256; };
   const size_t b_twx = al(tx.tw.size() * sizeof(float2)), b_twy = al(ty.tw.size() * sizeof(float2));
-  const size_t b_prx = al(tx.prow.size() * sizeof(float4)), b_pry = al(ty.prow.size() * sizeof(float4));
   const size_t b_slx = al(tx.slot.size() * sizeof(int)), b_sly = al(ty.slot.size() * sizeof(int));
   const size_t b_kxs = al(kx_slot.size() * sizeof(float));
   const size_t b_spec = al(3 * fs) * 2 + al(2 * fs);
-  const size_t total = b_twx + b_twy + b_prx + b_pry + b_slx + b_sly + b_kxs + b_spec;
+  const size_t total = b_twx + b_twy + b_slx + b_sly + b_kxs + b_spec;
   CK(cudaMalloc(&h->fft_arena, total));
   char* a = (char*)h->fft_arena;
+  cudaError_t put_err = cudaSuccess;
   auto put = [&](const void* src, size_t n, size_t b) -> char* {
     char* p = a;
-    cudaMemcpy(p, src, n, cudaMemcpyHostToDevice);
+    const cudaError_t e = cudaMemcpy(p, src, n, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) put_err = e;
     a += b;
     return p;
   };
   fc.ax.tw = (const float2*)put(tx.tw.data(), tx.tw.size() * sizeof(float2), b_twx);
   fc.ay.tw = (const float2*)put(ty.tw.data(), ty.tw.size() * sizeof(float2), b_twy);
-  fc.ax.prow = (const float2*)put(tx.prow.data(), tx.prow.size() * sizeof(float4), b_prx);
-  fc.ay.prow = (const float2*)put(ty.prow.data(), ty.prow.size() * sizeof(float4), b_pry);
   fc.ax.slot = (const int*)put(tx.slot.data(), tx.slot.size() * sizeof(int), b_slx);
   fc.ay.slot = (const int*)put(ty.slot.data(), ty.slot.size() * sizeof(int), b_sly);
   fc.kx_slot = (const float*)put(kx_slot.data(), kx_slot.size() * sizeof(float), b_kxs);
-  CK(cudaGetLastError());
+  CK(put_err);
   void* RA = a; a += al(3 * fs);
   void* RB = a; a += al(3 * fs);
   void* SA = a; a += al(2 * fs);

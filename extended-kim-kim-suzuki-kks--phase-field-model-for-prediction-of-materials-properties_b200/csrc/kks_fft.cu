@@ -7,11 +7,11 @@
 // a column pass, every 1-D transform runs in shared memory, and the pointwise
 // stages are fused into the passes around them:
 //
-//   rows_A    read eta, X (f64)   -> eta, X, eta^2 row spectra (RA)      + old-state history sums
+//   rows_A    eta, X (f64) rows -> eta, X, eta^2 row spectra (RA)       + old-state history sums
 //   cols_AB   RA columns: forward FFT -> FT(eta), FT(X) kept (SA); tr eps^, i k_x FT(eta),
-//             i k_y FT(eta) -> inverse FFT -> row spectra (RB)          + Parseval sums
-//   rows_BC   RB rows: inverse FFT -> tr eps, d_x eta, d_y eta; free energy, drive, fluxes
-//             (pointwise, old state) -> forward FFT -> row spectra (RC) + sum G
+//             i k_y FT(eta) -> inverse FFT -> row spectra (RB)         + Parseval sums
+//   rows_BC   RB rows: inverse FFT -> tr eps, d_x eta, d_y eta; Allen-Cahn drive and
+//             Cahn-Hilliard fluxes (pointwise, old state) -> forward FFT -> RC  + sum G
 //   cols_CD   RC columns: forward FFT; with SA the semi-implicit increments d_eta^, d_X^
 //             -> inverse FFT -> row spectra (RD)
 //   rows_D    RD rows: inverse FFT -> d_eta, d_X; new state, phase compositions, new free
@@ -19,28 +19,41 @@
 //   extras    np.gradient energy of the new state and, at surface steps, interface counts
 //
 // so that the spectra never make a round trip through HBM between a transform
-// and the operation that consumes it. Rows are transformed in pairs as one
-// complex sequence (row a + i row b) and split / merged with the Hermitian
-// symmetry; row spectra hold the ny/2+1 non-negative y frequencies in natural
-// order, one row per x. Each 1-D transform is an in-place mixed-radix DIF
-// (natural order in, digit-reversed out) for forward transforms and the
-// matching DIT (digit-reversed in, natural out) for inverse ones, so spectra
-// inside a column pass are indexed through a slot -> frequency table and no
+// and the operation that consumes it. A row-pass block owns one pair of rows of
+// one field, transformed as one complex sequence (row a + i row b) and split /
+// merged with the Hermitian symmetry; a column-pass block owns one y-frequency
+// column. Blocks are small (128 threads, one or two sequences) so that many of
+// them share an SM and hide each other's latency. Spectra between passes are
+// column-major (x fastest), so a column pass moves one contiguous run.
+//
+// Each 1-D transform is an in-place mixed-radix DIF (natural order in,
+// digit-reversed out) for forward transforms and the matching DIT
+// (digit-reversed in, natural out) for inverse ones, so spectra inside a
+// column pass are indexed through a slot -> frequency table and no
 // permutation pass exists. Radices 2, 3, 4, 5, 7 are butterflies with
-// compile-time constants; one larger prime factor (71 for 1420) is a direct
-// DFT in registers using the symmetry of its cosine / sine matrix (a pair of
-// outputs per 35 x 4 FMA), as the last DIF stage where it needs no twiddles.
+// compile-time constants. One larger prime factor P (71 for 1420) is the last
+// DIF stage (no twiddles): a direct DFT that folds its inputs into
+// s_n = x_n + x_{P-n}, d_n = x_n - x_{P-n} and produces output pairs (k, P-k)
+// from H = (P-1)/2 real-by-complex products each. It runs out of place into a
+// second buffer as warp tasks: the 32 lanes of a warp take 32 DFTs and one
+// group of G output pairs, with the cos / sin factors of that group read from
+// constant memory (uniform across the warp), so no thread keeps the whole
+// folded input (4 H floats) in registers.
 // Only the mixed path uses these kernels (FP32 transforms on the increments of
 // an FP64 state; see kks_fields.cu); the FP64 path keeps cuFFT.
 
 #include <math.h>
+
+#include <vector>
 
 #include "kks_internal.cuh"
 #include "kks_fft.cuh"
 
 namespace {
 
-constexpr int kThreads = 128;
+constexpr int kThreads = KKS_FFT_THREADS;
+// blocks per SM the register allocation must allow
+constexpr int kMinBlocks = 4;
 
 __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
@@ -166,85 +179,140 @@ __device__ __forceinline__ void bfly_small(float2* base, int q, int j, const flo
   for (int m = 0; m < R; ++m) base[m * q] = x[m];
 }
 
-// Direct DFT of prime length P on P consecutive elements (q = 1, no twiddles):
-// the inputs are folded into s_n = x_n + x_{P-n}, d_n = x_n - x_{P-n} (in
-// registers) and each output pair (k, P-k) costs H complex-by-real FMAs on s
-// and d with cos / sin (2 pi n k / P) read from the table prow (row k-1, H
-// float2 padded to an even count, broadcast to the warp).
-template <int P, int DIR>
-__device__ __forceinline__ void bfly_prime(float2* base, const float4* __restrict__ prow) {
-  constexpr int H = (P - 1) / 2;
-  constexpr int H2 = (H + 1) / 2;  // float4 per table row
-  float2 s[H], d[H];
-  const float2 x0 = base[0];
-  float2 sum = x0;
-#pragma unroll
-  for (int n = 1; n <= H; ++n) {
-    const float2 a = base[n], b = base[P - n];
-    s[n - 1] = cadd(a, b);
-    d[n - 1] = csub(a, b);
-    sum = cadd(sum, s[n - 1]);
-  }
-#pragma unroll 1
-  for (int k = 1; k <= H; ++k) {
-    const float4* row = prow + (k - 1) * H2;
-    float2 A = x0, B = make_float2(0.f, 0.f);
-#pragma unroll
-    for (int h = 0; h < H2; ++h) {
-      const float4 w = __ldg(row + h);
-      const int n0 = 2 * h;
-      A.x += s[n0].x * w.x;
-      A.y += s[n0].y * w.x;
-      B.x += d[n0].x * w.y;
-      B.y += d[n0].y * w.y;
-      if (n0 + 1 < H) {
-        A.x += s[n0 + 1].x * w.z;
-        A.y += s[n0 + 1].y * w.z;
-        B.x += d[n0 + 1].x * w.w;
-        B.y += d[n0 + 1].y * w.w;
-      }
-    }
-    if (DIR < 0) {
-      base[k] = make_float2(A.x + B.y, A.y - B.x);
-      base[P - k] = make_float2(A.x - B.y, A.y + B.x);
-    } else {
-      base[k] = make_float2(A.x - B.y, A.y + B.x);
-      base[P - k] = make_float2(A.x + B.y, A.y - B.x);
-    }
-  }
-  base[0] = sum;
+// ---------------------------------------------------------------------------
+// Prime stages. The H = (P-1)/2 output pairs are split into NG groups of G;
+// the table of prime P holds (cos, sin)(2 pi ((n k) mod P) / P) at
+// [(g H + n - 1) G + j] for output k = g G + j + 1 and input n = 1..H
+// (filled from the host in double precision, see kks_fft_upload_prime_tables).
+template <int P>
+struct PrimeShape {
+  static constexpr int H = (P - 1) / 2;
+  static constexpr int G = P == 71 ? 7 : (P == 19 ? 3 : H);
+  static constexpr int NG = H / G;
+  static_assert(NG * G == H, "prime group size must divide (P-1)/2");
+};
+
+__constant__ float2 kPrimeTw11[5 * 5];
+__constant__ float2 kPrimeTw19[9 * 9];
+__constant__ float2 kPrimeTw71[35 * 35];
+
+template <int P>
+__device__ __forceinline__ float2 prime_tw(int i) {
+  if constexpr (P == 11) return kPrimeTw11[i];
+  else if constexpr (P == 19) return kPrimeTw19[i];
+  else return kPrimeTw71[i];
 }
 
-// nseq in-place transforms of length ax.n, sequence s at buf + s * sstride.
-// DIR = -1: forward DIF (natural -> digit-reversed); DIR = +1: inverse DIT
+// Out-of-place prime stage over nseq sequences of length n (DFTs of P
+// consecutive elements at b * P): in -> out. Work item = (32 DFTs, group g)
+// per warp.
+template <int P, int DIR>
+__device__ __forceinline__ void prime_stage(const float2* in, float2* out, int nseq, int n) {
+  using S = PrimeShape<P>;
+  constexpr int H = S::H, G = S::G, NG = S::NG;
+  const int per = n / P;
+  const int D = nseq * per;
+  const int ntask = ((D + 31) >> 5) * NG;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int task = warp; task < ntask; task += kThreads / 32) {
+    const int lg = task / NG;
+    const int g = task - lg * NG;
+    const int d = (lg << 5) + lane;
+    if (d >= D) continue;
+    int sq = 0, b = d;
+    while (b >= per) {
+      b -= per;
+      ++sq;
+    }
+    const float2* x = in + sq * n + b * P;
+    float2* y = out + sq * n + b * P;
+    const float2 x0 = x[0];
+    float2 sum = x0;
+    float2 A[G], B[G];
+#pragma unroll
+    for (int j = 0; j < G; ++j) {
+      A[j] = make_float2(0.f, 0.f);
+      B[j] = make_float2(0.f, 0.f);
+    }
+    const int tb = g * (H * G);
+#pragma unroll
+    for (int nn = 1; nn <= H; ++nn) {
+      const float2 a = x[nn], c = x[P - nn];
+      const float2 s = cadd(a, c), dd = csub(a, c);
+      sum = cadd(sum, s);
+#pragma unroll
+      for (int j = 0; j < G; ++j) {
+        const float2 w = prime_tw<P>(tb + (nn - 1) * G + j);
+        A[j].x += s.x * w.x;
+        A[j].y += s.y * w.x;
+        B[j].x += dd.x * w.y;
+        B[j].y += dd.y * w.y;
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < G; ++j) {
+      const int k = g * G + j + 1;
+      const float ax = x0.x + A[j].x, ay = x0.y + A[j].y;
+      if (DIR < 0) {
+        y[k] = make_float2(ax + B[j].y, ay - B[j].x);
+        y[P - k] = make_float2(ax - B[j].y, ay + B[j].x);
+      } else {
+        y[k] = make_float2(ax - B[j].y, ay + B[j].x);
+        y[P - k] = make_float2(ax + B[j].y, ay - B[j].x);
+      }
+    }
+    if (g == 0) y[0] = sum;
+  }
+}
+
+__device__ __forceinline__ int fdiv(int x, int d, uint32_t m) {
+  return d == 1 ? x : (int)__umulhi((uint32_t)x, m);
+}
+
+// nseq transforms of length ax.n, sequence s at cur + s * n; `other` has room
+// for as many (the prime stage writes there and the two swap). DIR = -1:
+// forward DIF (natural -> digit-reversed); DIR = +1: inverse DIT
 // (digit-reversed -> natural), unnormalised. P: the large prime of the axis
-// (0 if none); its stage is the last DIF stage (q = 1).
+// (0 if none). Returns the buffer holding the result; ends with a barrier.
 template <int DIR, int P>
-__device__ void fft_run(float2* buf, int nseq, int sstride, const KksFftAxis& ax) {
+__device__ float2* fft_run(float2* cur, float2* other, int nseq, const KksFftAxis& ax) {
+  const int n = ax.n;
   for (int si = 0; si < ax.nst; ++si) {
     const int s = DIR < 0 ? si : ax.nst - 1 - si;
-    const int r = ax.r[s], L = ax.L[s], q = ax.q[s];
-    const int per = ax.n / r;
-    const int total = nseq * per;
+    const int r = ax.r[s];
+    if constexpr (P > 7) {
+      if (r == P) {
+        prime_stage<P, DIR>(cur, other, nseq, n);
+        float2* t = cur;
+        cur = other;
+        other = t;
+        __syncthreads();
+        continue;
+      }
+    }
+    const int L = ax.L[s], q = ax.q[s];
+    const int per = n / r;
+    const uint32_t qm = ax.qm[s], pm = ax.pm[s];
     const float2* tw = ax.tw + ax.tw_off[s];
-    for (int t = threadIdx.x; t < total; t += blockDim.x) {
-      const int seq = t / per;
-      const int rem = t - seq * per;
-      const int b = rem / q, j = rem - b * q;
-      float2* base = buf + (size_t)seq * sstride + b * L + j;
+    const int total = nseq * per;
+    for (int t = threadIdx.x; t < total; t += kThreads) {
+      const int sq = nseq == 1 ? 0 : fdiv(t, per, pm);
+      const int bt = t - sq * per;
+      const int b = fdiv(bt, q, qm);
+      const int j = bt - b * q;
+      float2* base = cur + sq * n + b * L + j;
       switch (r) {
         case 2: bfly_small<2, DIR>(base, q, j, tw); break;
         case 3: bfly_small<3, DIR>(base, q, j, tw); break;
         case 4: bfly_small<4, DIR>(base, q, j, tw); break;
         case 5: bfly_small<5, DIR>(base, q, j, tw); break;
         case 7: bfly_small<7, DIR>(base, q, j, tw); break;
-        default:
-          if constexpr (P > 7) bfly_prime<P, DIR>(base, (const float4*)ax.prow);
-          break;
+        default: break;
       }
     }
     __syncthreads();
   }
+  return cur;
 }
 
 template <int NV>
@@ -273,138 +341,119 @@ __device__ __forceinline__ void block_reduce_store(double (&v)[NV], double* out)
 
 __device__ __forceinline__ bool in_iface(double e) { return e >= 0.1 && e <= 0.9; }
 
-// Split the transform of (row a + i row b) into the half spectra of a and b
-// and write them to rows ix0, ix0+1 of field f of a row-spectrum array.
-__device__ __forceinline__ void split_store(const float2* z, const KksFftAxis& ay, float2* dst, int ix0, bool has1,
-                                            int nyh) {
+// Split the transform of (row a + i row b) (digit-reversed) into the half
+// spectra of rows ix0 (a) and ix0+1 (b) of a column-major row-spectrum field.
+__device__ __forceinline__ void split_store(const float2* z, const KksFftAxis& ay, float2* __restrict__ dst, int ix0,
+                                            bool has1, int nx, int nyh) {
   const int ny = ay.n;
-  for (int k = threadIdx.x; k < nyh; k += blockDim.x) {
-    const float2 Zk = z[ay.slot[k]];
-    const float2 Zm = z[ay.slot[k == 0 ? 0 : ny - k]];
+  for (int k = threadIdx.x; k < nyh; k += kThreads) {
+    const float2 Zk = z[__ldg(ay.slot + k)];
+    const float2 Zm = z[__ldg(ay.slot + (k == 0 ? 0 : ny - k))];
     // A = (Z_k + conj Z_{-k}) / 2, B = (Z_k - conj Z_{-k}) / (2i)
-    dst[(size_t)ix0 * nyh + k] = make_float2(0.5f * (Zk.x + Zm.x), 0.5f * (Zk.y - Zm.y));
-    if (has1) dst[(size_t)(ix0 + 1) * nyh + k] = make_float2(0.5f * (Zk.y + Zm.y), -0.5f * (Zk.x - Zm.x));
+    float2* d = dst + (size_t)k * nx + ix0;
+    d[0] = make_float2(0.5f * (Zk.x + Zm.x), 0.5f * (Zk.y - Zm.y));
+    if (has1) d[1] = make_float2(0.5f * (Zk.y + Zm.y), -0.5f * (Zk.x - Zm.x));
   }
 }
 
-// Inverse of split_store: z (digit-reversed) = A + i B with the Hermitian
-// extension. The y = 0 and Nyquist bins of a real row are real: their
-// imaginary round-off is dropped (as a C2R transform does), so that it cannot
-// leak into the other row of the pair.
-__device__ __forceinline__ void merge_load(float2* z, const KksFftAxis& ay, const float2* src, int ix0, bool has1,
-                                           int nyh) {
+// Inverse of split_store: z (digit-reversed) = A + i B over all ny
+// frequencies, the negative ones from the Hermitian extension. The y = 0 and
+// Nyquist bins of a real row are real: their imaginary round-off is dropped
+// (as a C2R transform does), so that it cannot leak into the other row.
+__device__ __forceinline__ void merge_load(float2* z, const KksFftAxis& ay, const float2* __restrict__ src, int ix0,
+                                           bool has1, int nx, int nyh) {
   const int ny = ay.n;
-  for (int k = threadIdx.x; k < ny; k += blockDim.x) {
-    float2 A, B;
-    if (k < nyh) {
-      A = src[(size_t)ix0 * nyh + k];
-      B = has1 ? src[(size_t)(ix0 + 1) * nyh + k] : make_float2(0.f, 0.f);
-      if (k == 0 || 2 * k == ny) {
-        A.y = 0.f;
-        B.y = 0.f;
-      }
-    } else {
-      const float2 a = src[(size_t)ix0 * nyh + (ny - k)];
-      const float2 b = has1 ? src[(size_t)(ix0 + 1) * nyh + (ny - k)] : make_float2(0.f, 0.f);
-      A = make_float2(a.x, -a.y);
-      B = make_float2(b.x, -b.y);
+  for (int k = threadIdx.x; k < nyh; k += kThreads) {
+    const float2* s = src + (size_t)k * nx + ix0;
+    float2 A = s[0];
+    float2 B = has1 ? s[1] : make_float2(0.f, 0.f);
+    const bool self = k == 0 || 2 * k == ny;
+    if (self) {
+      A.y = 0.f;
+      B.y = 0.f;
     }
-    z[ay.slot[k]] = make_float2(A.x - B.y, A.y + B.x);
+    z[__ldg(ay.slot + k)] = make_float2(A.x - B.y, A.y + B.x);
+    // conj(A) + i conj(B) at -k
+    if (!self) z[__ldg(ay.slot + (ny - k))] = make_float2(A.x + B.y, B.x - A.y);
   }
 }
 
 // ---------------------------------------------------------------------------
-// pass 1: eta, X rows -> row spectra of eta, X, eta^2; old-state history sums
+// pass 1: one row pair of one field (blockIdx.y: 0 eta, 1 X, 2 eta^2) ->
+// row spectra RA; the eta blocks also take the old-state history sums.
 template <int PY>
-__global__ void __launch_bounds__(kThreads) kf_rows_A(const KksConst* __restrict__ c, const KksPar* __restrict__ par,
-                                                      const KksFftConst* __restrict__ fc,
-                                                      const double* __restrict__ eta, const double* __restrict__ X,
-                                                      float2* __restrict__ RA, double* __restrict__ partials) {
+__global__ void __launch_bounds__(kThreads, kMinBlocks)
+    kf_rows_A(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const KksFftConst* __restrict__ fc,
+              const double* __restrict__ eta, const double* __restrict__ X, float2* __restrict__ RA,
+              double* __restrict__ partials) {
   if (!par->active) return;
   extern __shared__ float2 sm[];
   const KksFftAxis& ay = fc->ay;
   const int nx = c->nx, ny = c->ny, nyh = c->nyh;
+  const int f = blockIdx.y;
   const int ix0 = 2 * blockIdx.x;
   const bool has1 = ix0 + 1 < nx;
+  const double* src = f == 1 ? X : eta;
+  const double* r0 = src + (size_t)ix0 * ny;
+  const double* r1 = r0 + ny;
   double acc[5] = {0, 0, 0, 0, 0};
-  for (int y = threadIdx.x; y < ny; y += blockDim.x) {
-    const double e0 = eta[(size_t)ix0 * ny + y], x0 = X[(size_t)ix0 * ny + y];
-    const double e1 = has1 ? eta[(size_t)(ix0 + 1) * ny + y] : 0.0, x1 = has1 ? X[(size_t)(ix0 + 1) * ny + y] : 0.0;
-    sm[y] = make_float2((float)e0, (float)e1);
-    sm[ny + y] = make_float2((float)x0, (float)x1);
-    sm[2 * ny + y] = make_float2((float)(e0 * e0), (float)(e1 * e1));
-    acc[0] += e0;
-    if (e0 < 0.05) { acc[1] += x0; acc[2] += 1.0; }
-    if (e0 > 0.95) { acc[3] += x0; acc[4] += 1.0; }
-    if (has1) {
-      acc[0] += e1;
-      if (e1 < 0.05) { acc[1] += x1; acc[2] += 1.0; }
-      if (e1 > 0.95) { acc[3] += x1; acc[4] += 1.0; }
+  for (int y = threadIdx.x; y < ny; y += kThreads) {
+    const double a0 = r0[y];
+    const double a1 = has1 ? r1[y] : 0.0;
+    sm[y] = f == 2 ? make_float2((float)(a0 * a0), (float)(a1 * a1)) : make_float2((float)a0, (float)a1);
+    if (f == 0) {
+      const double x0 = X[(size_t)ix0 * ny + y];
+      acc[0] += a0;
+      if (a0 < 0.05) { acc[1] += x0; acc[2] += 1.0; }
+      if (a0 > 0.95) { acc[3] += x0; acc[4] += 1.0; }
+      if (has1) {
+        const double x1 = X[(size_t)(ix0 + 1) * ny + y];
+        acc[0] += a1;
+        if (a1 < 0.05) { acc[1] += x1; acc[2] += 1.0; }
+        if (a1 > 0.95) { acc[3] += x1; acc[4] += 1.0; }
+      }
     }
   }
   __syncthreads();
-  fft_run<-1, PY>(sm, 3, ny, ay);
-  const size_t fs = (size_t)nx * nyh;
-  for (int f = 0; f < 3; ++f) split_store(sm + f * ny, ay, RA + f * fs, ix0, has1, nyh);
-  block_reduce_store<5>(acc, partials + (size_t)blockIdx.x * KKS_NPART + P3_ETA);
+  const float2* res = fft_run<-1, PY>(sm, sm + ny, 1, ay);
+  split_store(res, ay, RA + (size_t)f * nx * nyh, ix0, has1, nx, nyh);
+  if (f == 0) block_reduce_store<5>(acc, partials + (size_t)blockIdx.x * KKS_NPART + P3_ETA);
 }
 
-// column tile: C consecutive y-frequency columns, every x
-template <int C>
-__device__ __forceinline__ void col_load(float2* sm, const float2* __restrict__ src, int nx, int nyh, int ky0,
-                                         int ncol) {
-  for (int idx = threadIdx.x; idx < nx * C; idx += blockDim.x) {
-    const int p = idx / C, cc = idx - p * C;
-    sm[cc * nx + p] = cc < ncol ? src[(size_t)p * nyh + ky0 + cc] : make_float2(0.f, 0.f);
-  }
-}
-
-template <int C>
-__device__ __forceinline__ void col_store(const float2* sm, float2* __restrict__ dst, int nx, int nyh, int ky0,
-                                          int ncol) {
-  for (int idx = threadIdx.x; idx < nx * C; idx += blockDim.x) {
-    const int p = idx / C, cc = idx - p * C;
-    if (cc < ncol) dst[(size_t)p * nyh + ky0 + cc] = sm[cc * nx + p];
-  }
-}
-
-// pass 2: columns of RA. blockIdx.y: 0 eta -> keep FT(eta), i k_x FT(eta);
-// 1 eta -> i k_y FT(eta); 2 eta^2 -> tr eps^ (+ Parseval sums); 3 X -> keep FT(X).
-template <int PX, int C>
-__global__ void __launch_bounds__(kThreads) kf_cols_AB(const KksConst* __restrict__ c,
-                                                       const KksPar* __restrict__ par,
-                                                       const KksFftConst* __restrict__ fc,
-                                                       const float2* __restrict__ RA, float2* __restrict__ SA,
-                                                       float2* __restrict__ RB, const double* __restrict__ kys,
-                                                       double* __restrict__ partials) {
+// pass 2: one y-frequency column of RA. blockIdx.y: 0 eta -> keep FT(eta),
+// i k_x FT(eta); 1 eta -> i k_y FT(eta); 2 eta^2 -> tr eps^ (+ Parseval sums);
+// 3 X -> keep FT(X).
+template <int PX>
+__global__ void __launch_bounds__(kThreads, kMinBlocks)
+    kf_cols_AB(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const KksFftConst* __restrict__ fc,
+               const float2* __restrict__ RA, float2* __restrict__ SA, float2* __restrict__ RB,
+               const double* __restrict__ kys, double* __restrict__ partials) {
   if (!par->active) return;
   extern __shared__ float2 sm[];
   const KksFftAxis& ax = fc->ax;
   const int nx = c->nx, ny = c->ny, nyh = c->nyh;
   const size_t fs = (size_t)nx * nyh;
-  const int g = blockIdx.y;
-  const int ky0 = blockIdx.x * C;
-  const int ncol = min(C, nyh - ky0);
+  const int iy = blockIdx.x, g = blockIdx.y;
   const int src_field = g < 2 ? 0 : (g == 2 ? 2 : 1);
-  col_load<C>(sm, RA + src_field * fs, nx, nyh, ky0, ncol);
+  const float2* col = RA + src_field * fs + (size_t)iy * nx;
+  for (int p = threadIdx.x; p < nx; p += kThreads) sm[p] = col[p];
   __syncthreads();
-  fft_run<-1, PX>(sm, C, nx, ax);
-  if (g == 3) {
-    col_store<C>(sm, SA + fs, nx, nyh, ky0, ncol);
-    return;
+  float2* cur = fft_run<-1, PX>(sm, sm + nx, 1, ax);
+  float2* other = cur == sm ? sm + nx : sm;
+  if (g == 3 || g == 0) {
+    float2* dst = SA + (g == 3 ? fs : 0) + (size_t)iy * nx;
+    for (int p = threadIdx.x; p < nx; p += kThreads) dst[p] = cur[p];
+    if (g == 3) return;
   }
-  if (g == 0) col_store<C>(sm, SA, nx, nyh, ky0, ncol);
   const float inv_N = (float)c->inv_N;
   const float a = (float)(par->epsX * c->c3) * inv_N;
   const float c11 = (float)c->c11, c12 = (float)c->c12;
+  const float ky = (float)kys[iy];
+  const double w = (iy == 0 || 2 * iy == ny) ? 1.0 : 2.0;
   double acc[6] = {0, 0, 0, 0, 0, 0};
-  for (int idx = threadIdx.x; idx < nx * C; idx += blockDim.x) {
-    const int cc = idx / nx, p = idx - cc * nx;
-    if (cc >= ncol) continue;
-    const float kx = fc->kx_slot[p];
-    const int iy = ky0 + cc;
-    const float ky = (float)kys[iy];
-    float2 v = sm[idx];
+  for (int p = threadIdx.x; p < nx; p += kThreads) {
+    const float kx = __ldg(fc->kx_slot + p);
+    float2 v = cur[p];
     if (g == 0) {
       v = make_float2(-kx * inv_N * v.y, kx * inv_N * v.x);
     } else if (g == 1) {
@@ -422,7 +471,6 @@ __global__ void __launch_bounds__(kThreads) kf_cols_AB(const KksConst* __restric
         oyy = Nky * ky;
         oxy = 0.5f * (Nky * kx + Nkx * ky);
       }
-      const double w = (iy == 0 || 2 * iy == ny) ? 1.0 : 2.0;
       const double pw = w * ((double)v.x * v.x + (double)v.y * v.y);
       const double dxx = oxx, dyy = oyy, dxy = oxy;
       acc[0] += pw * dxx * dxx;
@@ -434,19 +482,22 @@ __global__ void __launch_bounds__(kThreads) kf_cols_AB(const KksConst* __restric
       const float st = a * (oxx + oyy);
       v = make_float2(st * v.x, st * v.y);
     }
-    sm[idx] = v;
+    cur[p] = v;
   }
-  if (g == 2) block_reduce_store<6>(acc, partials + (size_t)blockIdx.x * KKS_NPART + P2_OXX2);
+  if (g == 2) block_reduce_store<6>(acc, partials + (size_t)iy * KKS_NPART + P2_OXX2);
   __syncthreads();
-  fft_run<+1, PX>(sm, C, nx, ax);
+  const float2* res = fft_run<+1, PX>(cur, other, 1, ax);
   const int dst_field = g == 2 ? 0 : (g == 0 ? 1 : 2);
-  col_store<C>(sm, RB + dst_field * fs, nx, nyh, ky0, ncol);
+  float2* dst = RB + dst_field * fs + (size_t)iy * nx;
+  for (int p = threadIdx.x; p < nx; p += kThreads) dst[p] = res[p];
 }
 
-// pass 3: RB rows -> tr eps, d_x eta, d_y eta; pointwise old-state free
-// energy, Allen-Cahn drive and Cahn-Hilliard fluxes -> row spectra RC
+// pass 3: one row pair of RB field f (0 tr eps, 1 d_x eta, 2 d_y eta) ->
+// inverse FFT -> pointwise with the old state: f = 0 the Allen-Cahn drive
+// (free energy + elastic), f = 1, 2 the Cahn-Hilliard fluxes -> forward FFT
+// -> row spectra RC field f. The f = 0 blocks take sum G.
 template <int PY>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, kMinBlocks)
     kf_rows_BC(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const KksFftConst* __restrict__ fc,
                const float2* __restrict__ RB, float2* __restrict__ RC, const double* __restrict__ eta,
                const float* __restrict__ Xal, const float* __restrict__ Xth, float* g0, float* g1, float* g2,
@@ -456,11 +507,13 @@ __global__ void __launch_bounds__(kThreads)
   const KksFftAxis& ay = fc->ay;
   const int nx = c->nx, ny = c->ny, nyh = c->nyh;
   const size_t fs = (size_t)nx * nyh;
+  const int f = blockIdx.y;
   const int ix0 = 2 * blockIdx.x;
   const bool has1 = ix0 + 1 < nx;
-  for (int f = 0; f < 3; ++f) merge_load(sm + f * ny, ay, RB + f * fs, ix0, has1, nyh);
+  merge_load(sm, ay, RB + f * fs, ix0, has1, nx, nyh);
   __syncthreads();
-  fft_run<+1, PY>(sm, 3, ny, ay);
+  float2* cur = fft_run<+1, PY>(sm, sm + ny, 1, ay);
+  float2* other = cur == sm ? sm + ny : sm;
   const KksPar q = *par;
   float* gs_buf = q.gs == 0 ? g0 : (q.gs == 1 ? g1 : g2);
   const float A_a = (float)q.A_alp_s, va = (float)q.va, fa0 = (float)q.fa0;
@@ -468,110 +521,129 @@ __global__ void __launch_bounds__(kThreads)
   const float epsX = (float)q.epsX;
   const float c3 = (float)((c->C11_0 + 2 * c->C12_0) * q.inv_C44);
   double accG = 0.0;
-  for (int y = threadIdx.x; y < ny; y += blockDim.x) {
-    const float2 tr = sm[y], gx = sm[ny + y], gy = sm[2 * ny + y];
-    float dr[2], fxv[2], fyv[2];
+  for (int y = threadIdx.x; y < ny; y += kThreads) {
+    const float2 v = cur[y];
+    float o[2] = {0.f, 0.f};
 #pragma unroll
     for (int r = 0; r < 2; ++r) {
-      dr[r] = fxv[r] = fyv[r] = 0.f;
       if (r == 1 && !has1) continue;
       const size_t i = (size_t)(ix0 + r) * ny + y;
       const float e = (float)eta[i];
       const float ca = Xal[i], ct = Xth[i];
-      const float da = ca - va, dtt = ct - vt;
-      const float fa_s = A_a * da * da + fa0;
-      const float fa_ca_s = 2.0f * A_a * da;
-      const float ft_s = A_t * dtt * dtt + ft0;
-      const float e2 = e * e, e3 = e2 * e;
-      const float h = 3.0f * e2 - 2.0f * e3;
+      const float e2 = e * e;
       const float h_eta = 6.0f * e - 6.0f * e2;
-      const float gw = e2 - 2.0f * e3 + e2 * e2;
-      const float g_eta = 2.0f * e - 6.0f * e2 + 4.0f * e3;
-      const float G = (1.0f - h) * fa_s + h * ft_s + w_s * gw;
-      const float G_eta = -h_eta * (fa_s - ft_s - (ca - ct) * fa_ca_s) + w_s * g_eta;
-      const float flux = h_eta * (ca - ct);
-      const float trv = r == 0 ? tr.x : tr.y;
-      const float el_eta_s = 2.0f * epsX * e * c3 * (3.0f * epsX * e2 - trv);
-      dr[r] = G_eta + el_eta_s;
-      fxv[r] = flux * (r == 0 ? gx.x : gx.y);
-      fyv[r] = flux * (r == 0 ? gy.x : gy.y);
-      if (q.armed_write) gs_buf[i] = G;
-      accG += (double)G;
+      const float vr = r == 0 ? v.x : v.y;
+      if (f == 0) {
+        const float da = ca - va, dtt = ct - vt;
+        const float fa_s = A_a * da * da + fa0;
+        const float fa_ca_s = 2.0f * A_a * da;
+        const float ft_s = A_t * dtt * dtt + ft0;
+        const float e3 = e2 * e;
+        const float h = 3.0f * e2 - 2.0f * e3;
+        const float gw = e2 - 2.0f * e3 + e2 * e2;
+        const float g_eta = 2.0f * e - 6.0f * e2 + 4.0f * e3;
+        const float G = (1.0f - h) * fa_s + h * ft_s + w_s * gw;
+        const float G_eta = -h_eta * (fa_s - ft_s - (ca - ct) * fa_ca_s) + w_s * g_eta;
+        const float el_eta_s = 2.0f * epsX * e * c3 * (3.0f * epsX * e2 - vr);
+        o[r] = G_eta + el_eta_s;
+        if (q.armed_write) gs_buf[i] = G;
+        accG += (double)G;
+      } else {
+        const float flux = h_eta * (ca - ct);
+        o[r] = flux * vr;
+      }
     }
-    sm[y] = make_float2(dr[0], dr[1]);
-    sm[ny + y] = make_float2(fxv[0], fxv[1]);
-    sm[2 * ny + y] = make_float2(fyv[0], fyv[1]);
+    cur[y] = make_float2(o[0], o[1]);
   }
   __syncthreads();
-  fft_run<-1, PY>(sm, 3, ny, ay);
-  for (int f = 0; f < 3; ++f) split_store(sm + f * ny, ay, RC + f * fs, ix0, has1, nyh);
-  double acc[1] = {accG};
-  block_reduce_store<1>(acc, partials + (size_t)blockIdx.x * KKS_NPART + P3_G);
+  const float2* res = fft_run<-1, PY>(cur, other, 1, ay);
+  split_store(res, ay, RC + f * fs, ix0, has1, nx, nyh);
+  if (f == 0) {
+    double acc[1] = {accG};
+    block_reduce_store<1>(acc, partials + (size_t)blockIdx.x * KKS_NPART + P3_G);
+  }
 }
 
-// pass 4: columns of RC. blockIdx.y: 0 -> d_eta^ from FT(drive) and FT(eta);
-// 1 -> d_X^ from FT(flux_x), FT(flux_y) and FT(X). Output row spectra RD.
-template <int PX, int C>
-__global__ void __launch_bounds__(kThreads) kf_cols_CD(const KksConst* __restrict__ c,
-                                                       const KksPar* __restrict__ par,
-                                                       const KksFftConst* __restrict__ fc,
-                                                       const float2* __restrict__ RC, const float2* __restrict__ SA,
-                                                       float2* __restrict__ RD, const double* __restrict__ kys) {
+// pass 4a: one column of FT(drive) with FT(eta) -> d_eta^ -> row spectra RD[0]
+template <int PX>
+__global__ void __launch_bounds__(kThreads, kMinBlocks)
+    kf_cols_CD_eta(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const KksFftConst* __restrict__ fc,
+                   const float2* __restrict__ RC, const float2* __restrict__ SA, float2* __restrict__ RD,
+                   const double* __restrict__ kys) {
+  if (!par->active) return;
+  extern __shared__ float2 sm[];
+  const KksFftAxis& ax = fc->ax;
+  const int nx = c->nx;
+  const int iy = blockIdx.x;
+  const float2* col = RC + (size_t)iy * nx;
+  for (int p = threadIdx.x; p < nx; p += kThreads) sm[p] = col[p];
+  __syncthreads();
+  float2* cur = fft_run<-1, PX>(sm, sm + nx, 1, ax);
+  float2* other = cur == sm ? sm + nx : sm;
+  const float inv_N = (float)c->inv_N;
+  const float ac_mul = (float)par->ac_mul, ac_den = (float)par->ac_den;
+  const float ky = (float)kys[iy];
+  const float2* ecol = SA + (size_t)iy * nx;
+  for (int p = threadIdx.x; p < nx; p += kThreads) {
+    const float kx = __ldg(fc->kx_slot + p);
+    const float k2 = kx * kx + ky * ky;
+    const float2 dh = cur[p];
+    const float2 eh = ecol[p];
+    const float ak = ac_den * k2, den = 1.f + ak;
+    cur[p] = make_float2((ac_mul * dh.x - ak * eh.x) / den * inv_N, (ac_mul * dh.y - ak * eh.y) / den * inv_N);
+  }
+  __syncthreads();
+  const float2* res = fft_run<+1, PX>(cur, other, 1, ax);
+  float2* dst = RD + (size_t)iy * nx;
+  for (int p = threadIdx.x; p < nx; p += kThreads) dst[p] = res[p];
+}
+
+// pass 4b: one column of FT(flux_x), FT(flux_y) with FT(X) -> d_X^ -> row spectra RD[1]
+template <int PX>
+__global__ void __launch_bounds__(kThreads, kMinBlocks)
+    kf_cols_CD_X(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const KksFftConst* __restrict__ fc,
+                 const float2* __restrict__ RC, const float2* __restrict__ SA, float2* __restrict__ RD,
+                 const double* __restrict__ kys) {
   if (!par->active) return;
   extern __shared__ float2 sm[];
   const KksFftAxis& ax = fc->ax;
   const int nx = c->nx, nyh = c->nyh;
   const size_t fs = (size_t)nx * nyh;
-  const int g = blockIdx.y;
-  const int ky0 = blockIdx.x * C;
-  const int ncol = min(C, nyh - ky0);
-  const float inv_N = (float)c->inv_N;
-  const float ac_mul = (float)par->ac_mul, ac_den = (float)par->ac_den, ch_mul = (float)par->ch_mul;
-  const float dtD = (float)(par->dt * par->D_s);
-  if (g == 0) {
-    col_load<C>(sm, RC, nx, nyh, ky0, ncol);
-    __syncthreads();
-    fft_run<-1, PX>(sm, C, nx, ax);
-    for (int idx = threadIdx.x; idx < nx * C; idx += blockDim.x) {
-      const int cc = idx / nx, p = idx - cc * nx;
-      if (cc >= ncol) continue;
-      const float kx = fc->kx_slot[p], ky = (float)kys[ky0 + cc];
-      const float k2 = kx * kx + ky * ky;
-      const float2 dh = sm[idx];
-      const float2 eh = SA[(size_t)p * nyh + ky0 + cc];
-      const float ak = ac_den * k2, den = 1.f + ak;
-      sm[idx] = make_float2((ac_mul * dh.x - ak * eh.x) / den * inv_N, (ac_mul * dh.y - ak * eh.y) / den * inv_N);
-    }
-    __syncthreads();
-    fft_run<+1, PX>(sm, C, nx, ax);
-    col_store<C>(sm, RD, nx, nyh, ky0, ncol);
-  } else {
-    col_load<C>(sm, RC + fs, nx, nyh, ky0, ncol);
-    col_load<C>(sm + C * nx, RC + 2 * fs, nx, nyh, ky0, ncol);
-    __syncthreads();
-    fft_run<-1, PX>(sm, 2 * C, nx, ax);
-    for (int idx = threadIdx.x; idx < nx * C; idx += blockDim.x) {
-      const int cc = idx / nx, p = idx - cc * nx;
-      if (cc >= ncol) continue;
-      const float kx = fc->kx_slot[p], ky = (float)kys[ky0 + cc];
-      const float k2 = kx * kx + ky * ky;
-      const float2 fx = sm[idx], fy = sm[C * nx + idx];
-      const float flx = -(kx * fx.y) - ky * fy.y;
-      const float fly = kx * fx.x + ky * fy.x;
-      const float2 xh = SA[fs + (size_t)p * nyh + ky0 + cc];
-      const float bk = dtD * k2, den = 1.f + bk;
-      sm[idx] = make_float2((ch_mul * flx - bk * xh.x) / den * inv_N, (ch_mul * fly - bk * xh.y) / den * inv_N);
-    }
-    __syncthreads();
-    fft_run<+1, PX>(sm, C, nx, ax);
-    col_store<C>(sm, RD + fs, nx, nyh, ky0, ncol);
+  const int iy = blockIdx.x;
+  const float2* cx = RC + fs + (size_t)iy * nx;
+  const float2* cy = RC + 2 * fs + (size_t)iy * nx;
+  for (int p = threadIdx.x; p < nx; p += kThreads) {
+    sm[p] = cx[p];
+    sm[nx + p] = cy[p];
   }
+  __syncthreads();
+  float2* cur = fft_run<-1, PX>(sm, sm + 2 * nx, 2, ax);
+  float2* other = cur == sm ? sm + 2 * nx : sm;
+  const float inv_N = (float)c->inv_N;
+  const float ch_mul = (float)par->ch_mul;
+  const float dtD = (float)(par->dt * par->D_s);
+  const float ky = (float)kys[iy];
+  const float2* xcol = SA + fs + (size_t)iy * nx;
+  for (int p = threadIdx.x; p < nx; p += kThreads) {
+    const float kx = __ldg(fc->kx_slot + p);
+    const float k2 = kx * kx + ky * ky;
+    const float2 fx = cur[p], fy = cur[nx + p];
+    const float flx = -(kx * fx.y) - ky * fy.y;
+    const float fly = kx * fx.x + ky * fy.x;
+    const float2 xh = xcol[p];
+    const float bk = dtD * k2, den = 1.f + bk;
+    cur[p] = make_float2((ch_mul * flx - bk * xh.x) / den * inv_N, (ch_mul * fly - bk * xh.y) / den * inv_N);
+  }
+  __syncthreads();
+  const float2* res = fft_run<+1, PX>(cur, other, 1, ax);
+  float2* dst = RD + fs + (size_t)iy * nx;
+  for (int p = threadIdx.x; p < nx; p += kThreads) dst[p] = res[p];
 }
 
-// pass 5: RD rows -> d_eta, d_X; new state, phase compositions, new free
-// energy and diffusion potential, residual and history sums
+// pass 5: one row pair of RD -> d_eta, d_X; new state, phase compositions,
+// new free energy and diffusion potential, residual and history sums
 template <int PY>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, kMinBlocks)
     kf_rows_D(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const KksFftConst* __restrict__ fc,
               const float2* __restrict__ RD, const double* __restrict__ eta_o, const double* __restrict__ X_o,
               double* __restrict__ eta_b, double* __restrict__ X_b, float* __restrict__ Xal_b,
@@ -584,10 +656,10 @@ __global__ void __launch_bounds__(kThreads)
   const size_t fs = (size_t)nx * nyh;
   const int ix0 = 2 * blockIdx.x;
   const bool has1 = ix0 + 1 < nx;
-  merge_load(sm, ay, RD, ix0, has1, nyh);
-  merge_load(sm + ny, ay, RD + fs, ix0, has1, nyh);
+  merge_load(sm, ay, RD, ix0, has1, nx, nyh);
+  merge_load(sm + ny, ay, RD + fs, ix0, has1, nx, nyh);
   __syncthreads();
-  fft_run<+1, PY>(sm, 2, ny, ay);
+  const float2* z = fft_run<+1, PY>(sm, sm + 2 * ny, 2, ay);
   const KksPar q = *par;
   float* gb_buf = q.gb == 0 ? g0 : (q.gb == 1 ? g1 : g2);
   const float* gm_buf = q.gm == 0 ? g0 : (q.gm == 1 ? g1 : g2);
@@ -597,8 +669,8 @@ __global__ void __launch_bounds__(kThreads)
   const float A_t = (float)q.A_thet_s, vt = (float)q.vt, ft0 = (float)q.ft0, w_s = (float)q.w_s;
   const double dt = q.dt;
   double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-  for (int y = threadIdx.x; y < ny; y += blockDim.x) {
-    const float2 de = sm[y], dX = sm[ny + y];
+  for (int y = threadIdx.x; y < ny; y += kThreads) {
+    const float2 de = z[y], dX = z[ny + y];
 #pragma unroll
     for (int r = 0; r < 2; ++r) {
       if (r == 1 && !has1) continue;
@@ -692,26 +764,29 @@ __global__ void __launch_bounds__(kThreads)
   if (do_iface) block_reduce_store<1>(a2, partials + (size_t)blockIdx.x * KKS_NPART + slot_iface);
 }
 
+// shared memory of each pass (bytes): its sequences plus as many for the
+// out-of-place prime stage
+inline size_t row_smem(int ny, int nseq) { return 2 * (size_t)nseq * ny * sizeof(float2); }
+inline size_t col_smem(int nx, int nseq) { return 2 * (size_t)nseq * nx * sizeof(float2); }
+
 template <int PY>
 void launch_rows(const KksFftLaunch& L, int p, int stage, cudaStream_t s) {
   const KksConst* dc = L.dc;
   const KksPar* par = L.par;
   const KksFieldPtrs& f = *L.f;
   const int q = 1 - p;
-  const int npairs = (L.nx + 1) / 2;
-  const size_t row_smem3 = 3 * (size_t)L.ny * sizeof(float2);
-  const size_t row_smem2 = 2 * (size_t)L.ny * sizeof(float2);
+  const int npairs = kks_fft_row_blocks(L.nx);
   float2* RA = (float2*)L.RA;
   float2* RB = (float2*)L.RB;
   if (stage == 0) {
-    kf_rows_A<PY><<<npairs, kThreads, row_smem3, s>>>(dc, par, L.fc, (const double*)f.eta[p], (const double*)f.X[p],
-                                                      RA, f.partials);
+    kf_rows_A<PY><<<dim3(npairs, 3), kThreads, row_smem(L.ny, 1), s>>>(
+        dc, par, L.fc, (const double*)f.eta[p], (const double*)f.X[p], RA, f.partials);
   } else if (stage == 1) {
-    kf_rows_BC<PY><<<npairs, kThreads, row_smem3, s>>>(dc, par, L.fc, RB, RA, (const double*)f.eta[p],
-                                                       (const float*)f.X_al[p], (const float*)f.X_th[p],
-                                                       (float*)f.g[0], (float*)f.g[1], (float*)f.g[2], f.partials);
+    kf_rows_BC<PY><<<dim3(npairs, 3), kThreads, row_smem(L.ny, 1), s>>>(
+        dc, par, L.fc, RB, RA, (const double*)f.eta[p], (const float*)f.X_al[p], (const float*)f.X_th[p],
+        (float*)f.g[0], (float*)f.g[1], (float*)f.g[2], f.partials);
   } else {
-    kf_rows_D<PY><<<npairs, kThreads, row_smem2, s>>>(
+    kf_rows_D<PY><<<npairs, kThreads, row_smem(L.ny, 2), s>>>(
         dc, par, L.fc, RB, (const double*)f.eta[p], (const double*)f.X[p], (double*)f.eta[q], (double*)f.X[q],
         (float*)f.X_al[q], (float*)f.X_th[q], (const double*)f.eta_m, (const double*)f.X_m, (float*)f.mu,
         (float*)f.g[0], (float*)f.g[1], (float*)f.g[2], f.partials);
@@ -720,37 +795,39 @@ void launch_rows(const KksFftLaunch& L, int p, int stage, cudaStream_t s) {
 
 template <int PX>
 void launch_cols(const KksFftLaunch& L, int stage, cudaStream_t s) {
-  constexpr int C = KKS_FFT_COLS;
-  const int ntiles = (L.nyh + C - 1) / C;
-  const size_t col_smem1 = (size_t)C * L.nx * sizeof(float2);
   float2* RA = (float2*)L.RA;
   float2* RB = (float2*)L.RB;
   float2* SA = (float2*)L.SA;
   if (stage == 0) {
-    kf_cols_AB<PX, C><<<dim3(ntiles, 4), kThreads, col_smem1, s>>>(L.dc, L.par, L.fc, RA, SA, RB, L.f->ky,
-                                                                    L.f->partials);
+    kf_cols_AB<PX><<<dim3(L.nyh, 4), kThreads, col_smem(L.nx, 1), s>>>(L.dc, L.par, L.fc, RA, SA, RB, L.f->ky,
+                                                                        L.f->partials);
   } else {
-    kf_cols_CD<PX, C><<<dim3(ntiles, 2), kThreads, 2 * col_smem1, s>>>(L.dc, L.par, L.fc, RA, SA, RB, L.f->ky);
+    kf_cols_CD_eta<PX><<<L.nyh, kThreads, col_smem(L.nx, 1), s>>>(L.dc, L.par, L.fc, RA, SA, RB, L.f->ky);
+    kf_cols_CD_X<PX><<<L.nyh, kThreads, col_smem(L.nx, 2), s>>>(L.dc, L.par, L.fc, RA, SA, RB, L.f->ky);
   }
+}
+
+template <typename K>
+cudaError_t set_attr(K* kernel, size_t smem) {
+  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+  return e;
 }
 
 template <int PY>
 int set_row_attrs(int ny) {
-  const int row3 = 3 * ny * (int)sizeof(float2);
-  const int row2 = 2 * ny * (int)sizeof(float2);
-  cudaError_t e = cudaFuncSetAttribute(kf_rows_A<PY>, cudaFuncAttributeMaxDynamicSharedMemorySize, row3);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(kf_rows_BC<PY>, cudaFuncAttributeMaxDynamicSharedMemorySize, row3);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(kf_rows_D<PY>, cudaFuncAttributeMaxDynamicSharedMemorySize, row2);
+  cudaError_t e = set_attr(kf_rows_A<PY>, row_smem(ny, 1));
+  if (e == cudaSuccess) e = set_attr(kf_rows_BC<PY>, row_smem(ny, 1));
+  if (e == cudaSuccess) e = set_attr(kf_rows_D<PY>, row_smem(ny, 2));
   return (int)e;
 }
 
 template <int PX>
 int set_col_attrs(int nx) {
-  constexpr int C = KKS_FFT_COLS;
-  const int col1 = C * nx * (int)sizeof(float2);
-  cudaError_t e = cudaFuncSetAttribute(kf_cols_AB<PX, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, col1);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(kf_cols_CD<PX, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * col1);
+  cudaError_t e = set_attr(kf_cols_AB<PX>, col_smem(nx, 1));
+  if (e == cudaSuccess) e = set_attr(kf_cols_CD_eta<PX>, col_smem(nx, 1));
+  if (e == cudaSuccess) e = set_attr(kf_cols_CD_X<PX>, col_smem(nx, 2));
   return (int)e;
 }
 
@@ -763,12 +840,32 @@ int set_col_attrs(int nx) {
     default: break;                  \
   }
 
+template <int P>
+void prime_table(std::vector<float2>& t) {
+  using S = PrimeShape<P>;
+  t.assign(S::H * S::H, make_float2(0.f, 0.f));
+  for (int g = 0; g < S::NG; ++g)
+    for (int n = 1; n <= S::H; ++n)
+      for (int j = 0; j < S::G; ++j) {
+        const int k = g * S::G + j + 1;
+        const double th = 2.0 * M_PI * (double)((n * k) % P) / (double)P;
+        t[(g * S::H + n - 1) * S::G + j] = make_float2((float)cos(th), (float)sin(th));
+      }
+}
+
 }  // namespace
 
+size_t kks_fft_smem_bytes(int nx, int ny) {
+  const size_t r = row_smem(ny, 2), c = col_smem(nx, 2);
+  return (r > c ? r : c) + 1024;  // + the reduction scratch
+}
+
+int kks_fft_row_blocks(int nx) { return (nx + 1) / 2; }
+
 int kks_fft_partial_rows(int nx, int ny, int nbx) {
-  const int npairs = (nx + 1) / 2;
-  const int ntiles = (ny / 2 + 1 + KKS_FFT_COLS - 1) / KKS_FFT_COLS;
-  int m = npairs > ntiles ? npairs : ntiles;
+  int m = kks_fft_row_blocks(nx);
+  const int nyh = ny / 2 + 1;  // the column pass that writes sums has one block per column
+  if (nyh > m) m = nyh;
   return m > nbx ? m : nbx;
 }
 
@@ -782,6 +879,19 @@ int kks_fft_set_attributes(const KksFftLaunch& L) {
 #undef KKS_ROWS_ATTR
 #undef KKS_COLS_ATTR
   return rc != 0 ? rc : rc2;
+}
+
+int kks_fft_upload_prime_tables() {
+  std::vector<float2> t;
+  prime_table<11>(t);
+  cudaError_t e = cudaMemcpyToSymbol(kPrimeTw11, t.data(), t.size() * sizeof(float2));
+  if (e != cudaSuccess) return (int)e;
+  prime_table<19>(t);
+  e = cudaMemcpyToSymbol(kPrimeTw19, t.data(), t.size() * sizeof(float2));
+  if (e != cudaSuccess) return (int)e;
+  prime_table<71>(t);
+  e = cudaMemcpyToSymbol(kPrimeTw71, t.data(), t.size() * sizeof(float2));
+  return (int)e;
 }
 
 void kks_fft_launch_attempt(const KksFftLaunch& L, int p, cudaStream_t s) {

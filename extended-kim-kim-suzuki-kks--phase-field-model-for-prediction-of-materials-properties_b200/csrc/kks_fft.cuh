@@ -3,23 +3,27 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <stdint.h>
 
 #include "kks_internal.cuh"
 
 #define KKS_FFT_MAXST 16
-#define KKS_FFT_COLS 4  // y-frequency columns per column-pass block
+#define KKS_FFT_THREADS 128   // threads of every pass block
+#define KKS_FFT_MAXN 8192     // longest axis of the pipeline (shared memory and 32-bit index magic)
 
 // In-place mixed-radix transform of length n along one axis. Stage s has radix
 // r[s], current sub-transform length L[s] and stride q[s] = L[s] / r[s]; the
 // DIF runs the stages in order, the DIT in reverse. tw + tw_off[s] holds
 // (cos, sin)(2 pi j m / L[s]) at [j * r[s] + m] (stages with q = 1 have none).
-// A large prime factor P (> 7) is the last stage; prow holds its cos / sin
-// table. slot[k] is the position of frequency k after the DIF.
+// qm[s] / pm[s] are ceil(2^32 / q[s]) and ceil(2^32 / (n / r[s])) (0 for a
+// divisor of 1): x / d == __umulhi(x, m) for x, d < 2^16. A large prime factor
+// P (> 7) is the last DIF stage (q = 1). slot[k] is the position of frequency k
+// after the DIF.
 struct KksFftAxis {
   int n, nst, P;
   int r[KKS_FFT_MAXST], L[KKS_FFT_MAXST], q[KKS_FFT_MAXST], tw_off[KKS_FFT_MAXST];
+  uint32_t qm[KKS_FFT_MAXST], pm[KKS_FFT_MAXST];
   const float2* tw;
-  const float2* prow;
   const int* slot;
 };
 
@@ -29,6 +33,9 @@ struct KksFftConst {
   const float* kx_slot;  // k_x of the frequency held at each x slot after the DIF
 };
 
+// Spectrum buffers are column-major: element (ix, ky) of field f at
+// f * nx * nyh + ky * nx + ix, so that a column pass reads and writes one
+// contiguous run of nx values and a row pass one 16-byte pair per frequency.
 struct KksFftLaunch {
   const KksConst* dc;
   const KksPar* par;
@@ -36,16 +43,22 @@ struct KksFftLaunch {
   const KksFieldPtrs* f;
   void* RA;  // 3 row-spectrum fields (also RC)
   void* RB;  // 3 row-spectrum fields (also RD)
-  void* SA;  // 2 full spectra FT(eta), FT(X)
+  void* SA;  // 2 full spectra FT(eta), FT(X), x in DIF slot order
   int nx, ny, nyh;
   int nbx;   // grid of the pointwise extras kernel
   int PX, PY;
 };
 
-// Largest prime factors with a register-resident direct DFT; other sizes use cuFFT.
+// Largest prime factors with a direct DFT stage; other sizes use cuFFT.
 #define KKS_FFT_PRIMES {11, 19, 71}
 
-// Number of partial-sum rows the pipeline writes (the decide kernel reduces them).
+// Shared memory of the largest pass block for an nx x ny grid (bytes).
+size_t kks_fft_smem_bytes(int nx, int ny);
+// Blocks of a row pass, and the number of partial-sum rows the pipeline
+// writes (the decide kernel reduces them).
+int kks_fft_row_blocks(int nx);
 int kks_fft_partial_rows(int nx, int ny, int nbx);
 int kks_fft_set_attributes(const KksFftLaunch& L);
+// cos / sin tables of the prime stages into constant memory of the current device.
+int kks_fft_upload_prime_tables();
 void kks_fft_launch_attempt(const KksFftLaunch& L, int parity, cudaStream_t s);
