@@ -19,12 +19,14 @@
 //   extras    np.gradient energy of the new state and, at surface steps, interface counts
 //
 // so that the spectra never make a round trip through HBM between a transform
-// and the operation that consumes it. A row-pass block owns one pair of rows of
-// one field, transformed as one complex sequence (row a + i row b) and split /
-// merged with the Hermitian symmetry; a column-pass block owns one y-frequency
-// column. Blocks are small (128 threads, one or two sequences) so that many of
-// them share an SM and hide each other's latency. Spectra between passes are
-// column-major (x fastest), so a column pass moves one contiguous run.
+// and the operation that consumes it. A row-pass block owns one pair of rows
+// (all fields of the pass), each field's pair transformed as one complex
+// sequence (row a + i row b) and split / merged with the Hermitian symmetry; a
+// column-pass block owns KKS_FFT_COLS adjacent y-frequency columns. A block has
+// ten warps for two to six sequences, so that every stage (butterflies, the
+// prime DFTs, loads and stores) has several warps of independent work. Spectra
+// between passes are column-major (x fastest): a column pass moves one
+// contiguous run, a row pass one 16-byte pair per frequency.
 //
 // Each 1-D transform is an in-place mixed-radix DIF (natural order in,
 // digit-reversed out) for forward transforms and the matching DIT
@@ -33,12 +35,12 @@
 // permutation pass exists. Radices 2, 3, 4, 5, 7 are butterflies with
 // compile-time constants. One larger prime factor P (71 for 1420) is the last
 // DIF stage (no twiddles): a direct DFT that folds its inputs into
-// s_n = x_n + x_{P-n}, d_n = x_n - x_{P-n} and produces output pairs (k, P-k)
-// from H = (P-1)/2 real-by-complex products each. It runs out of place into a
-// second buffer as warp tasks: the 32 lanes of a warp take 32 DFTs and one
-// group of G output pairs, with the cos / sin factors of that group read from
-// constant memory (uniform across the warp), so no thread keeps the whole
-// folded input (4 H floats) in registers.
+// s_n = x_n + x_{P-n}, d_n = x_n - x_{P-n} and forms each output pair (k, P-k)
+// from H = (P-1)/2 real-by-complex products on s and d. It runs as warp tasks:
+// the lanes of a warp take 32 DFTs and one group of G output pairs, the warp's
+// cos / sin factors come from constant memory (uniform across the warp), and
+// the outputs wait in registers for a block barrier before they overwrite the
+// inputs, so the stage is in place and no thread holds the whole folded input.
 // Only the mixed path uses these kernels (FP32 transforms on the increments of
 // an FP64 state; see kks_fields.cu); the FP64 path keeps cuFFT.
 
@@ -52,8 +54,9 @@
 namespace {
 
 constexpr int kThreads = KKS_FFT_THREADS;
+constexpr int kCols = KKS_FFT_COLS;
 // blocks per SM the register allocation must allow
-constexpr int kMinBlocks = 4;
+constexpr int kMinBlocks = 2;
 
 __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
@@ -180,9 +183,9 @@ __device__ __forceinline__ void bfly_small(float2* base, int q, int j, const flo
 }
 
 // ---------------------------------------------------------------------------
-// Prime stages. The H = (P-1)/2 output pairs are split into NG groups of G;
-// the table of prime P holds (cos, sin)(2 pi ((n k) mod P) / P) at
-// [(g H + n - 1) G + j] for output k = g G + j + 1 and input n = 1..H
+// Prime stages. The H = (P-1)/2 output pairs (k, P-k) of a DFT are split into
+// NG groups of G; the table of prime P holds (cos, sin)(2 pi ((n k) mod P) / P)
+// at [(g H + n - 1) G + j] for output k = g G + j + 1 and input n = 1..H
 // (filled from the host in double precision, see kks_fft_upload_prime_tables).
 template <int P>
 struct PrimeShape {
@@ -190,6 +193,7 @@ struct PrimeShape {
   static constexpr int G = P == 71 ? 7 : (P == 19 ? 3 : H);
   static constexpr int NG = H / G;
   static_assert(NG * G == H, "prime group size must divide (P-1)/2");
+  static_assert(NG <= kThreads / 32, "a round needs one warp per group");
 };
 
 __constant__ float2 kPrimeTw11[5 * 5];
@@ -203,65 +207,71 @@ __device__ __forceinline__ float2 prime_tw(int i) {
   else return kPrimeTw71[i];
 }
 
-// Out-of-place prime stage over nseq sequences of length n (DFTs of P
-// consecutive elements at b * P): in -> out. Work item = (32 DFTs, group g)
-// per warp.
+// The prime stage of nseq sequences of length n at the start of the block's
+// dynamic shared memory, in place. DFT d = (sequence d / per, block d % per)
+// covers d's P consecutive values. A warp takes 32 DFTs (one per lane) and one
+// group g of output pairs; with W warps a round covers W / NG lane groups. The
+// outputs stay in registers until every warp of the round has read its
+// inputs, then overwrite them.
 template <int P, int DIR>
-__device__ __forceinline__ void prime_stage(const float2* in, float2* out, int nseq, int n) {
+__device__ __forceinline__ void prime_stage(int nseq, int n, uint32_t pm) {
   using S = PrimeShape<P>;
   constexpr int H = S::H, G = S::G, NG = S::NG;
+  constexpr int W = kThreads / 32, R = W / NG;
+  extern __shared__ float2 sm[];
   const int per = n / P;
   const int D = nseq * per;
-  const int ntask = ((D + 31) >> 5) * NG;
+  const int LG = (D + 31) >> 5;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int task = warp; task < ntask; task += kThreads / 32) {
-    const int lg = task / NG;
-    const int g = task - lg * NG;
+  const int g = warp % NG;
+  for (int lg0 = 0; lg0 < LG; lg0 += R) {
+    const int lg = lg0 + warp / NG;
     const int d = (lg << 5) + lane;
-    if (d >= D) continue;
-    int sq = 0, b = d;
-    while (b >= per) {
-      b -= per;
-      ++sq;
-    }
-    const float2* x = in + sq * n + b * P;
-    float2* y = out + sq * n + b * P;
-    const float2 x0 = x[0];
-    float2 sum = x0;
-    float2 A[G], B[G];
-#pragma unroll
-    for (int j = 0; j < G; ++j) {
-      A[j] = make_float2(0.f, 0.f);
-      B[j] = make_float2(0.f, 0.f);
-    }
-    const int tb = g * (H * G);
-#pragma unroll
-    for (int nn = 1; nn <= H; ++nn) {
-      const float2 a = x[nn], c = x[P - nn];
-      const float2 s = cadd(a, c), dd = csub(a, c);
-      sum = cadd(sum, s);
+    const bool has = warp < R * NG && lg < LG && d < D;
+    float2* x = sm;
+    float2 A[G], B[G], x0 = make_float2(0.f, 0.f), sum = make_float2(0.f, 0.f);
+    if (has) {
+      const int sq = per == 1 ? d : (int)__umulhi((uint32_t)d, pm);
+      x = sm + sq * n + (d - sq * per) * P;
+      x0 = x[0];
+      sum = x0;
 #pragma unroll
       for (int j = 0; j < G; ++j) {
-        const float2 w = prime_tw<P>(tb + (nn - 1) * G + j);
-        A[j].x += s.x * w.x;
-        A[j].y += s.y * w.x;
-        B[j].x += dd.x * w.y;
-        B[j].y += dd.y * w.y;
+        A[j] = make_float2(0.f, 0.f);
+        B[j] = make_float2(0.f, 0.f);
       }
-    }
+      const int tb = g * (H * G);
 #pragma unroll
-    for (int j = 0; j < G; ++j) {
-      const int k = g * G + j + 1;
-      const float ax = x0.x + A[j].x, ay = x0.y + A[j].y;
-      if (DIR < 0) {
-        y[k] = make_float2(ax + B[j].y, ay - B[j].x);
-        y[P - k] = make_float2(ax - B[j].y, ay + B[j].x);
-      } else {
-        y[k] = make_float2(ax - B[j].y, ay + B[j].x);
-        y[P - k] = make_float2(ax + B[j].y, ay - B[j].x);
+      for (int nn = 1; nn <= H; ++nn) {
+        const float2 a = x[nn], c = x[P - nn];
+        const float2 s = cadd(a, c), dd = csub(a, c);
+        sum = cadd(sum, s);
+#pragma unroll
+        for (int j = 0; j < G; ++j) {
+          const float2 w = prime_tw<P>(tb + (nn - 1) * G + j);
+          A[j].x += s.x * w.x;
+          A[j].y += s.y * w.x;
+          B[j].x += dd.x * w.y;
+          B[j].y += dd.y * w.y;
+        }
       }
     }
-    if (g == 0) y[0] = sum;
+    __syncthreads();
+    if (has) {
+#pragma unroll
+      for (int j = 0; j < G; ++j) {
+        const int k = g * G + j + 1;
+        const float ax = x0.x + A[j].x, ay = x0.y + A[j].y;
+        if (DIR < 0) {
+          x[k] = make_float2(ax + B[j].y, ay - B[j].x);
+          x[P - k] = make_float2(ax - B[j].y, ay + B[j].x);
+        } else {
+          x[k] = make_float2(ax - B[j].y, ay + B[j].x);
+          x[P - k] = make_float2(ax + B[j].y, ay - B[j].x);
+        }
+      }
+      if (g == 0) x[0] = sum;
+    }
   }
 }
 
@@ -269,23 +279,21 @@ __device__ __forceinline__ int fdiv(int x, int d, uint32_t m) {
   return d == 1 ? x : (int)__umulhi((uint32_t)x, m);
 }
 
-// nseq transforms of length ax.n, sequence s at cur + s * n; `other` has room
-// for as many (the prime stage writes there and the two swap). DIR = -1:
-// forward DIF (natural -> digit-reversed); DIR = +1: inverse DIT
-// (digit-reversed -> natural), unnormalised. P: the large prime of the axis
-// (0 if none). Returns the buffer holding the result; ends with a barrier.
+// nseq in-place transforms of length ax.n, sequence s at offset s * n of the
+// block's dynamic shared memory. DIR = -1: forward DIF (natural ->
+// digit-reversed); DIR = +1: inverse DIT (digit-reversed -> natural),
+// unnormalised. P: the large prime of the axis (0 if none). Ends with a barrier.
 template <int DIR, int P>
-__device__ float2* fft_run(float2* cur, float2* other, int nseq, const KksFftAxis& ax) {
+__device__ __forceinline__ void fft_run(int nseq, const KksFftAxis& ax) {
+  extern __shared__ float2 sm[];
+  float2* buf = sm;
   const int n = ax.n;
   for (int si = 0; si < ax.nst; ++si) {
     const int s = DIR < 0 ? si : ax.nst - 1 - si;
     const int r = ax.r[s];
     if constexpr (P > 7) {
       if (r == P) {
-        prime_stage<P, DIR>(cur, other, nseq, n);
-        float2* t = cur;
-        cur = other;
-        other = t;
+        prime_stage<P, DIR>(nseq, n, ax.pm[s]);
         __syncthreads();
         continue;
       }
@@ -300,7 +308,7 @@ __device__ float2* fft_run(float2* cur, float2* other, int nseq, const KksFftAxi
       const int bt = t - sq * per;
       const int b = fdiv(bt, q, qm);
       const int j = bt - b * q;
-      float2* base = cur + sq * n + b * L + j;
+      float2* base = buf + sq * n + b * L + j;
       switch (r) {
         case 2: bfly_small<2, DIR>(base, q, j, tw); break;
         case 3: bfly_small<3, DIR>(base, q, j, tw); break;
@@ -312,12 +320,11 @@ __device__ float2* fft_run(float2* cur, float2* other, int nseq, const KksFftAxi
     }
     __syncthreads();
   }
-  return cur;
 }
 
-template <int NV>
+template <int NV, int NT = kThreads>
 __device__ __forceinline__ void block_reduce_store(double (&v)[NV], double* out) {
-  __shared__ double sh[NV][kThreads / 32];
+  __shared__ double sh[NV][NT / 32];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
   for (int k = 0; k < NV; ++k) {
@@ -331,7 +338,7 @@ __device__ __forceinline__ void block_reduce_store(double (&v)[NV], double* out)
     const int lane2 = threadIdx.x;
 #pragma unroll
     for (int k = 0; k < NV; ++k) {
-      double x = lane2 < kThreads / 32 ? sh[k][lane2] : 0.0;
+      double x = lane2 < NT / 32 ? sh[k][lane2] : 0.0;
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
       if (lane2 == 0) out[k] = x;
@@ -379,8 +386,8 @@ __device__ __forceinline__ void merge_load(float2* z, const KksFftAxis& ay, cons
 }
 
 // ---------------------------------------------------------------------------
-// pass 1: one row pair of one field (blockIdx.y: 0 eta, 1 X, 2 eta^2) ->
-// row spectra RA; the eta blocks also take the old-state history sums.
+// pass 1: one row pair; the sequences are eta, X, eta^2 -> row spectra RA;
+// old-state history sums.
 template <int PY>
 __global__ void __launch_bounds__(kThreads, kMinBlocks)
     kf_rows_A(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const KksFftConst* __restrict__ fc,
@@ -390,39 +397,35 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
   extern __shared__ float2 sm[];
   const KksFftAxis& ay = fc->ay;
   const int nx = c->nx, ny = c->ny, nyh = c->nyh;
-  const int f = blockIdx.y;
   const int ix0 = 2 * blockIdx.x;
   const bool has1 = ix0 + 1 < nx;
-  const double* src = f == 1 ? X : eta;
-  const double* r0 = src + (size_t)ix0 * ny;
-  const double* r1 = r0 + ny;
+  const size_t i0 = (size_t)ix0 * ny;
   double acc[5] = {0, 0, 0, 0, 0};
   for (int y = threadIdx.x; y < ny; y += kThreads) {
-    const double a0 = r0[y];
-    const double a1 = has1 ? r1[y] : 0.0;
-    sm[y] = f == 2 ? make_float2((float)(a0 * a0), (float)(a1 * a1)) : make_float2((float)a0, (float)a1);
-    if (f == 0) {
-      const double x0 = X[(size_t)ix0 * ny + y];
-      acc[0] += a0;
-      if (a0 < 0.05) { acc[1] += x0; acc[2] += 1.0; }
-      if (a0 > 0.95) { acc[3] += x0; acc[4] += 1.0; }
-      if (has1) {
-        const double x1 = X[(size_t)(ix0 + 1) * ny + y];
-        acc[0] += a1;
-        if (a1 < 0.05) { acc[1] += x1; acc[2] += 1.0; }
-        if (a1 > 0.95) { acc[3] += x1; acc[4] += 1.0; }
-      }
+    const double e0 = eta[i0 + y], x0 = X[i0 + y];
+    const double e1 = has1 ? eta[i0 + ny + y] : 0.0, x1 = has1 ? X[i0 + ny + y] : 0.0;
+    sm[y] = make_float2((float)e0, (float)e1);
+    sm[ny + y] = make_float2((float)x0, (float)x1);
+    sm[2 * ny + y] = make_float2((float)(e0 * e0), (float)(e1 * e1));
+    acc[0] += e0;
+    if (e0 < 0.05) { acc[1] += x0; acc[2] += 1.0; }
+    if (e0 > 0.95) { acc[3] += x0; acc[4] += 1.0; }
+    if (has1) {
+      acc[0] += e1;
+      if (e1 < 0.05) { acc[1] += x1; acc[2] += 1.0; }
+      if (e1 > 0.95) { acc[3] += x1; acc[4] += 1.0; }
     }
   }
   __syncthreads();
-  const float2* res = fft_run<-1, PY>(sm, sm + ny, 1, ay);
-  split_store(res, ay, RA + (size_t)f * nx * nyh, ix0, has1, nx, nyh);
-  if (f == 0) block_reduce_store<5>(acc, partials + (size_t)blockIdx.x * KKS_NPART + P3_ETA);
+  fft_run<-1, PY>(3, ay);
+  const size_t fs = (size_t)nx * nyh;
+  for (int f = 0; f < 3; ++f) split_store(sm + f * ny, ay, RA + f * fs, ix0, has1, nx, nyh);
+  block_reduce_store<5>(acc, partials + (size_t)blockIdx.x * KKS_NPART + P3_ETA);
 }
 
-// pass 2: one y-frequency column of RA. blockIdx.y: 0 eta -> keep FT(eta),
-// i k_x FT(eta); 1 eta -> i k_y FT(eta); 2 eta^2 -> tr eps^ (+ Parseval sums);
-// 3 X -> keep FT(X).
+// pass 2: kCols adjacent y-frequency columns of RA. blockIdx.y: 0 eta -> keep
+// FT(eta), i k_x FT(eta); 1 eta -> i k_y FT(eta); 2 eta^2 -> tr eps^
+// (+ Parseval sums); 3 X -> keep FT(X).
 template <int PX>
 __global__ void __launch_bounds__(kThreads, kMinBlocks)
     kf_cols_AB(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const KksFftConst* __restrict__ fc,
@@ -433,69 +436,74 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
   const KksFftAxis& ax = fc->ax;
   const int nx = c->nx, ny = c->ny, nyh = c->nyh;
   const size_t fs = (size_t)nx * nyh;
-  const int iy = blockIdx.x, g = blockIdx.y;
+  const int g = blockIdx.y;
+  const int ky0 = blockIdx.x * kCols;
+  const int ncol = min(kCols, nyh - ky0);
+  const int nv = ncol * nx;
   const int src_field = g < 2 ? 0 : (g == 2 ? 2 : 1);
-  const float2* col = RA + src_field * fs + (size_t)iy * nx;
-  for (int p = threadIdx.x; p < nx; p += kThreads) sm[p] = col[p];
+  const float2* col = RA + src_field * fs + (size_t)ky0 * nx;
+  for (int i = threadIdx.x; i < nv; i += kThreads) sm[i] = col[i];
   __syncthreads();
-  float2* cur = fft_run<-1, PX>(sm, sm + nx, 1, ax);
-  float2* other = cur == sm ? sm + nx : sm;
+  fft_run<-1, PX>(ncol, ax);
   if (g == 3 || g == 0) {
-    float2* dst = SA + (g == 3 ? fs : 0) + (size_t)iy * nx;
-    for (int p = threadIdx.x; p < nx; p += kThreads) dst[p] = cur[p];
+    float2* dst = SA + (g == 3 ? fs : 0) + (size_t)ky0 * nx;
+    for (int i = threadIdx.x; i < nv; i += kThreads) dst[i] = sm[i];
     if (g == 3) return;
   }
   const float inv_N = (float)c->inv_N;
   const float a = (float)(par->epsX * c->c3) * inv_N;
   const float c11 = (float)c->c11, c12 = (float)c->c12;
-  const float ky = (float)kys[iy];
-  const double w = (iy == 0 || 2 * iy == ny) ? 1.0 : 2.0;
   double acc[6] = {0, 0, 0, 0, 0, 0};
-  for (int p = threadIdx.x; p < nx; p += kThreads) {
-    const float kx = __ldg(fc->kx_slot + p);
-    float2 v = cur[p];
-    if (g == 0) {
-      v = make_float2(-kx * inv_N * v.y, kx * inv_N * v.x);
-    } else if (g == 1) {
-      v = make_float2(-ky * inv_N * v.y, ky * inv_N * v.x);
-    } else {
-      // strain multipliers of the 2x2 acoustic tensor (stiffness / C44(T0)), 0 at k = 0
-      const float Kxx = c11 * kx * kx + ky * ky, Kyy = kx * kx + c11 * ky * ky, Kxy = (c12 + 1.f) * kx * ky;
-      const float det = Kxx * Kyy - Kxy * Kxy;
-      float oxx = 0.f, oyy = 0.f, oxy = 0.f;
-      if (det != 0.f) {
-        const float inv = 1.f / det;
-        const float Nxx = Kyy * inv, Nyy = Kxx * inv, Nxy = -Kxy * inv;
-        const float Nkx = Nxx * kx + Nxy * ky, Nky = Nxy * kx + Nyy * ky;
-        oxx = Nkx * kx;
-        oyy = Nky * ky;
-        oxy = 0.5f * (Nky * kx + Nkx * ky);
+  for (int cc = 0; cc < ncol; ++cc) {
+    const int iy = ky0 + cc;
+    const float ky = (float)kys[iy];
+    const double w = (iy == 0 || 2 * iy == ny) ? 1.0 : 2.0;
+    float2* z = sm + cc * nx;
+    for (int p = threadIdx.x; p < nx; p += kThreads) {
+      const float kx = __ldg(fc->kx_slot + p);
+      float2 v = z[p];
+      if (g == 0) {
+        v = make_float2(-kx * inv_N * v.y, kx * inv_N * v.x);
+      } else if (g == 1) {
+        v = make_float2(-ky * inv_N * v.y, ky * inv_N * v.x);
+      } else {
+        // strain multipliers of the 2x2 acoustic tensor (stiffness / C44(T0)), 0 at k = 0
+        const float Kxx = c11 * kx * kx + ky * ky, Kyy = kx * kx + c11 * ky * ky, Kxy = (c12 + 1.f) * kx * ky;
+        const float det = Kxx * Kyy - Kxy * Kxy;
+        float oxx = 0.f, oyy = 0.f, oxy = 0.f;
+        if (det != 0.f) {
+          const float inv = 1.f / det;
+          const float Nxx = Kyy * inv, Nyy = Kxx * inv, Nxy = -Kxy * inv;
+          const float Nkx = Nxx * kx + Nxy * ky, Nky = Nxy * kx + Nyy * ky;
+          oxx = Nkx * kx;
+          oyy = Nky * ky;
+          oxy = 0.5f * (Nky * kx + Nkx * ky);
+        }
+        const double pw = w * ((double)v.x * v.x + (double)v.y * v.y);
+        const double dxx = oxx, dyy = oyy, dxy = oxy;
+        acc[0] += pw * dxx * dxx;
+        acc[1] += pw * dyy * dyy;
+        acc[2] += pw * dxx * dyy;
+        acc[3] += pw * dxy * dxy;
+        acc[4] += pw * (dxx + dyy);
+        acc[5] += pw;
+        const float st = a * (oxx + oyy);
+        v = make_float2(st * v.x, st * v.y);
       }
-      const double pw = w * ((double)v.x * v.x + (double)v.y * v.y);
-      const double dxx = oxx, dyy = oyy, dxy = oxy;
-      acc[0] += pw * dxx * dxx;
-      acc[1] += pw * dyy * dyy;
-      acc[2] += pw * dxx * dyy;
-      acc[3] += pw * dxy * dxy;
-      acc[4] += pw * (dxx + dyy);
-      acc[5] += pw;
-      const float st = a * (oxx + oyy);
-      v = make_float2(st * v.x, st * v.y);
+      z[p] = v;
     }
-    cur[p] = v;
   }
-  if (g == 2) block_reduce_store<6>(acc, partials + (size_t)iy * KKS_NPART + P2_OXX2);
+  if (g == 2) block_reduce_store<6>(acc, partials + (size_t)blockIdx.x * KKS_NPART + P2_OXX2);
   __syncthreads();
-  const float2* res = fft_run<+1, PX>(cur, other, 1, ax);
+  fft_run<+1, PX>(ncol, ax);
   const int dst_field = g == 2 ? 0 : (g == 0 ? 1 : 2);
-  float2* dst = RB + dst_field * fs + (size_t)iy * nx;
-  for (int p = threadIdx.x; p < nx; p += kThreads) dst[p] = res[p];
+  float2* dst = RB + dst_field * fs + (size_t)ky0 * nx;
+  for (int i = threadIdx.x; i < nv; i += kThreads) dst[i] = sm[i];
 }
 
-// pass 3: one row pair of RB field f (0 tr eps, 1 d_x eta, 2 d_y eta) ->
-// inverse FFT -> pointwise with the old state: f = 0 the Allen-Cahn drive
-// (free energy + elastic), f = 1, 2 the Cahn-Hilliard fluxes -> forward FFT
-// -> row spectra RC field f. The f = 0 blocks take sum G.
+// pass 3: one row pair of RB (tr eps, d_x eta, d_y eta) -> inverse FFT ->
+// pointwise with the old state: the Allen-Cahn drive (free energy + elastic)
+// and the Cahn-Hilliard fluxes -> forward FFT -> row spectra RC; sum G.
 template <int PY>
 __global__ void __launch_bounds__(kThreads, kMinBlocks)
     kf_rows_BC(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const KksFftConst* __restrict__ fc,
@@ -507,13 +515,11 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
   const KksFftAxis& ay = fc->ay;
   const int nx = c->nx, ny = c->ny, nyh = c->nyh;
   const size_t fs = (size_t)nx * nyh;
-  const int f = blockIdx.y;
   const int ix0 = 2 * blockIdx.x;
   const bool has1 = ix0 + 1 < nx;
-  merge_load(sm, ay, RB + f * fs, ix0, has1, nx, nyh);
+  for (int f = 0; f < 3; ++f) merge_load(sm + f * ny, ay, RB + f * fs, ix0, has1, nx, nyh);
   __syncthreads();
-  float2* cur = fft_run<+1, PY>(sm, sm + ny, 1, ay);
-  float2* other = cur == sm ? sm + ny : sm;
+  fft_run<+1, PY>(3, ay);
   const KksPar q = *par;
   float* gs_buf = q.gs == 0 ? g0 : (q.gs == 1 ? g1 : g2);
   const float A_a = (float)q.A_alp_s, va = (float)q.va, fa0 = (float)q.fa0;
@@ -522,49 +528,47 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
   const float c3 = (float)((c->C11_0 + 2 * c->C12_0) * q.inv_C44);
   double accG = 0.0;
   for (int y = threadIdx.x; y < ny; y += kThreads) {
-    const float2 v = cur[y];
-    float o[2] = {0.f, 0.f};
+    const float2 tr = sm[y], gx = sm[ny + y], gy = sm[2 * ny + y];
+    float dr[2], fxv[2], fyv[2];
 #pragma unroll
     for (int r = 0; r < 2; ++r) {
+      dr[r] = fxv[r] = fyv[r] = 0.f;
       if (r == 1 && !has1) continue;
       const size_t i = (size_t)(ix0 + r) * ny + y;
       const float e = (float)eta[i];
       const float ca = Xal[i], ct = Xth[i];
-      const float e2 = e * e;
+      const float da = ca - va, dtt = ct - vt;
+      const float fa_s = A_a * da * da + fa0;
+      const float fa_ca_s = 2.0f * A_a * da;
+      const float ft_s = A_t * dtt * dtt + ft0;
+      const float e2 = e * e, e3 = e2 * e;
+      const float h = 3.0f * e2 - 2.0f * e3;
       const float h_eta = 6.0f * e - 6.0f * e2;
-      const float vr = r == 0 ? v.x : v.y;
-      if (f == 0) {
-        const float da = ca - va, dtt = ct - vt;
-        const float fa_s = A_a * da * da + fa0;
-        const float fa_ca_s = 2.0f * A_a * da;
-        const float ft_s = A_t * dtt * dtt + ft0;
-        const float e3 = e2 * e;
-        const float h = 3.0f * e2 - 2.0f * e3;
-        const float gw = e2 - 2.0f * e3 + e2 * e2;
-        const float g_eta = 2.0f * e - 6.0f * e2 + 4.0f * e3;
-        const float G = (1.0f - h) * fa_s + h * ft_s + w_s * gw;
-        const float G_eta = -h_eta * (fa_s - ft_s - (ca - ct) * fa_ca_s) + w_s * g_eta;
-        const float el_eta_s = 2.0f * epsX * e * c3 * (3.0f * epsX * e2 - vr);
-        o[r] = G_eta + el_eta_s;
-        if (q.armed_write) gs_buf[i] = G;
-        accG += (double)G;
-      } else {
-        const float flux = h_eta * (ca - ct);
-        o[r] = flux * vr;
-      }
+      const float gw = e2 - 2.0f * e3 + e2 * e2;
+      const float g_eta = 2.0f * e - 6.0f * e2 + 4.0f * e3;
+      const float G = (1.0f - h) * fa_s + h * ft_s + w_s * gw;
+      const float G_eta = -h_eta * (fa_s - ft_s - (ca - ct) * fa_ca_s) + w_s * g_eta;
+      const float flux = h_eta * (ca - ct);
+      const float trv = r == 0 ? tr.x : tr.y;
+      const float el_eta_s = 2.0f * epsX * e * c3 * (3.0f * epsX * e2 - trv);
+      dr[r] = G_eta + el_eta_s;
+      fxv[r] = flux * (r == 0 ? gx.x : gx.y);
+      fyv[r] = flux * (r == 0 ? gy.x : gy.y);
+      if (q.armed_write) gs_buf[i] = G;
+      accG += (double)G;
     }
-    cur[y] = make_float2(o[0], o[1]);
+    sm[y] = make_float2(dr[0], dr[1]);
+    sm[ny + y] = make_float2(fxv[0], fxv[1]);
+    sm[2 * ny + y] = make_float2(fyv[0], fyv[1]);
   }
   __syncthreads();
-  const float2* res = fft_run<-1, PY>(cur, other, 1, ay);
-  split_store(res, ay, RC + f * fs, ix0, has1, nx, nyh);
-  if (f == 0) {
-    double acc[1] = {accG};
-    block_reduce_store<1>(acc, partials + (size_t)blockIdx.x * KKS_NPART + P3_G);
-  }
+  fft_run<-1, PY>(3, ay);
+  for (int f = 0; f < 3; ++f) split_store(sm + f * ny, ay, RC + f * fs, ix0, has1, nx, nyh);
+  double acc[1] = {accG};
+  block_reduce_store<1>(acc, partials + (size_t)blockIdx.x * KKS_NPART + P3_G);
 }
 
-// pass 4a: one column of FT(drive) with FT(eta) -> d_eta^ -> row spectra RD[0]
+// pass 4a: kCols columns of FT(drive) with FT(eta) -> d_eta^ -> row spectra RD[0]
 template <int PX>
 __global__ void __launch_bounds__(kThreads, kMinBlocks)
     kf_cols_CD_eta(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const KksFftConst* __restrict__ fc,
@@ -573,32 +577,36 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
   if (!par->active) return;
   extern __shared__ float2 sm[];
   const KksFftAxis& ax = fc->ax;
-  const int nx = c->nx;
-  const int iy = blockIdx.x;
-  const float2* col = RC + (size_t)iy * nx;
-  for (int p = threadIdx.x; p < nx; p += kThreads) sm[p] = col[p];
+  const int nx = c->nx, nyh = c->nyh;
+  const int ky0 = blockIdx.x * kCols;
+  const int ncol = min(kCols, nyh - ky0);
+  const int nv = ncol * nx;
+  const float2* col = RC + (size_t)ky0 * nx;
+  for (int i = threadIdx.x; i < nv; i += kThreads) sm[i] = col[i];
   __syncthreads();
-  float2* cur = fft_run<-1, PX>(sm, sm + nx, 1, ax);
-  float2* other = cur == sm ? sm + nx : sm;
+  fft_run<-1, PX>(ncol, ax);
   const float inv_N = (float)c->inv_N;
   const float ac_mul = (float)par->ac_mul, ac_den = (float)par->ac_den;
-  const float ky = (float)kys[iy];
-  const float2* ecol = SA + (size_t)iy * nx;
-  for (int p = threadIdx.x; p < nx; p += kThreads) {
-    const float kx = __ldg(fc->kx_slot + p);
-    const float k2 = kx * kx + ky * ky;
-    const float2 dh = cur[p];
-    const float2 eh = ecol[p];
-    const float ak = ac_den * k2, den = 1.f + ak;
-    cur[p] = make_float2((ac_mul * dh.x - ak * eh.x) / den * inv_N, (ac_mul * dh.y - ak * eh.y) / den * inv_N);
+  for (int cc = 0; cc < ncol; ++cc) {
+    const float ky = (float)kys[ky0 + cc];
+    const float2* ecol = SA + (size_t)(ky0 + cc) * nx;
+    float2* z = sm + cc * nx;
+    for (int p = threadIdx.x; p < nx; p += kThreads) {
+      const float kx = __ldg(fc->kx_slot + p);
+      const float k2 = kx * kx + ky * ky;
+      const float2 dh = z[p];
+      const float2 eh = ecol[p];
+      const float ak = ac_den * k2, den = 1.f + ak;
+      z[p] = make_float2((ac_mul * dh.x - ak * eh.x) / den * inv_N, (ac_mul * dh.y - ak * eh.y) / den * inv_N);
+    }
   }
   __syncthreads();
-  const float2* res = fft_run<+1, PX>(cur, other, 1, ax);
-  float2* dst = RD + (size_t)iy * nx;
-  for (int p = threadIdx.x; p < nx; p += kThreads) dst[p] = res[p];
+  fft_run<+1, PX>(ncol, ax);
+  float2* dst = RD + (size_t)ky0 * nx;
+  for (int i = threadIdx.x; i < nv; i += kThreads) dst[i] = sm[i];
 }
 
-// pass 4b: one column of FT(flux_x), FT(flux_y) with FT(X) -> d_X^ -> row spectra RD[1]
+// pass 4b: kCols columns of FT(flux_x), FT(flux_y) with FT(X) -> d_X^ -> row spectra RD[1]
 template <int PX>
 __global__ void __launch_bounds__(kThreads, kMinBlocks)
     kf_cols_CD_X(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const KksFftConst* __restrict__ fc,
@@ -609,35 +617,41 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
   const KksFftAxis& ax = fc->ax;
   const int nx = c->nx, nyh = c->nyh;
   const size_t fs = (size_t)nx * nyh;
-  const int iy = blockIdx.x;
-  const float2* cx = RC + fs + (size_t)iy * nx;
-  const float2* cy = RC + 2 * fs + (size_t)iy * nx;
-  for (int p = threadIdx.x; p < nx; p += kThreads) {
-    sm[p] = cx[p];
-    sm[nx + p] = cy[p];
+  const int ky0 = blockIdx.x * kCols;
+  const int ncol = min(kCols, nyh - ky0);
+  const int nv = ncol * nx;
+  // flux_x columns at [0, nv), flux_y columns at [nv, 2 nv)
+  const float2* cx = RC + fs + (size_t)ky0 * nx;
+  const float2* cy = RC + 2 * fs + (size_t)ky0 * nx;
+  for (int i = threadIdx.x; i < nv; i += kThreads) {
+    sm[i] = cx[i];
+    sm[nv + i] = cy[i];
   }
   __syncthreads();
-  float2* cur = fft_run<-1, PX>(sm, sm + 2 * nx, 2, ax);
-  float2* other = cur == sm ? sm + 2 * nx : sm;
+  fft_run<-1, PX>(2 * ncol, ax);
   const float inv_N = (float)c->inv_N;
   const float ch_mul = (float)par->ch_mul;
   const float dtD = (float)(par->dt * par->D_s);
-  const float ky = (float)kys[iy];
-  const float2* xcol = SA + fs + (size_t)iy * nx;
-  for (int p = threadIdx.x; p < nx; p += kThreads) {
-    const float kx = __ldg(fc->kx_slot + p);
-    const float k2 = kx * kx + ky * ky;
-    const float2 fx = cur[p], fy = cur[nx + p];
-    const float flx = -(kx * fx.y) - ky * fy.y;
-    const float fly = kx * fx.x + ky * fy.x;
-    const float2 xh = xcol[p];
-    const float bk = dtD * k2, den = 1.f + bk;
-    cur[p] = make_float2((ch_mul * flx - bk * xh.x) / den * inv_N, (ch_mul * fly - bk * xh.y) / den * inv_N);
+  for (int cc = 0; cc < ncol; ++cc) {
+    const float ky = (float)kys[ky0 + cc];
+    const float2* xcol = SA + fs + (size_t)(ky0 + cc) * nx;
+    float2* z = sm + cc * nx;
+    const float2* zy = sm + nv + cc * nx;
+    for (int p = threadIdx.x; p < nx; p += kThreads) {
+      const float kx = __ldg(fc->kx_slot + p);
+      const float k2 = kx * kx + ky * ky;
+      const float2 fx = z[p], fy = zy[p];
+      const float flx = -(kx * fx.y) - ky * fy.y;
+      const float fly = kx * fx.x + ky * fy.x;
+      const float2 xh = xcol[p];
+      const float bk = dtD * k2, den = 1.f + bk;
+      z[p] = make_float2((ch_mul * flx - bk * xh.x) / den * inv_N, (ch_mul * fly - bk * xh.y) / den * inv_N);
+    }
   }
   __syncthreads();
-  const float2* res = fft_run<+1, PX>(cur, other, 1, ax);
-  float2* dst = RD + fs + (size_t)iy * nx;
-  for (int p = threadIdx.x; p < nx; p += kThreads) dst[p] = res[p];
+  fft_run<+1, PX>(ncol, ax);
+  float2* dst = RD + fs + (size_t)ky0 * nx;
+  for (int i = threadIdx.x; i < nv; i += kThreads) dst[i] = sm[i];
 }
 
 // pass 5: one row pair of RD -> d_eta, d_X; new state, phase compositions,
@@ -659,7 +673,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
   merge_load(sm, ay, RD, ix0, has1, nx, nyh);
   merge_load(sm + ny, ay, RD + fs, ix0, has1, nx, nyh);
   __syncthreads();
-  const float2* z = fft_run<+1, PY>(sm, sm + 2 * ny, 2, ay);
+  fft_run<+1, PY>(2, ay);
   const KksPar q = *par;
   float* gb_buf = q.gb == 0 ? g0 : (q.gb == 1 ? g1 : g2);
   const float* gm_buf = q.gm == 0 ? g0 : (q.gm == 1 ? g1 : g2);
@@ -670,7 +684,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
   const double dt = q.dt;
   double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   for (int y = threadIdx.x; y < ny; y += kThreads) {
-    const float2 de = z[y], dX = z[ny + y];
+    const float2 de = sm[y], dX = sm[ny + y];
 #pragma unroll
     for (int r = 0; r < 2; ++r) {
       if (r == 1 && !has1) continue;
@@ -731,7 +745,9 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
 
 // np.gradient energy sum of a state (mode bit 0) and, at surface steps, its
 // interface cell count (mode bit 1) into the given partial slots.
-__global__ void __launch_bounds__(kThreads)
+constexpr int kExtrasThreads = 256;
+
+__global__ void __launch_bounds__(kExtrasThreads)
     kf_extras(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const double* __restrict__ eta,
               int mode, int slot_grad, int slot_iface, double* __restrict__ partials) {
   if (!par->active) return;
@@ -759,15 +775,14 @@ __global__ void __launch_bounds__(kThreads)
   }
   double a1[1] = {acc[0]};
   double a2[1] = {acc[1]};
-  if (do_grad) block_reduce_store<1>(a1, partials + (size_t)blockIdx.x * KKS_NPART + slot_grad);
+  if (do_grad) block_reduce_store<1, kExtrasThreads>(a1, partials + (size_t)blockIdx.x * KKS_NPART + slot_grad);
   __syncthreads();
-  if (do_iface) block_reduce_store<1>(a2, partials + (size_t)blockIdx.x * KKS_NPART + slot_iface);
+  if (do_iface) block_reduce_store<1, kExtrasThreads>(a2, partials + (size_t)blockIdx.x * KKS_NPART + slot_iface);
 }
 
-// shared memory of each pass (bytes): its sequences plus as many for the
-// out-of-place prime stage
-inline size_t row_smem(int ny, int nseq) { return 2 * (size_t)nseq * ny * sizeof(float2); }
-inline size_t col_smem(int nx, int nseq) { return 2 * (size_t)nseq * nx * sizeof(float2); }
+// shared memory of each pass (bytes): its sequences, transformed in place
+inline size_t seq_smem(int n, int nseq) { return (size_t)nseq * n * sizeof(float2); }
+inline int col_blocks(int nyh) { return (nyh + kCols - 1) / kCols; }
 
 template <int PY>
 void launch_rows(const KksFftLaunch& L, int p, int stage, cudaStream_t s) {
@@ -779,14 +794,14 @@ void launch_rows(const KksFftLaunch& L, int p, int stage, cudaStream_t s) {
   float2* RA = (float2*)L.RA;
   float2* RB = (float2*)L.RB;
   if (stage == 0) {
-    kf_rows_A<PY><<<dim3(npairs, 3), kThreads, row_smem(L.ny, 1), s>>>(
-        dc, par, L.fc, (const double*)f.eta[p], (const double*)f.X[p], RA, f.partials);
+    kf_rows_A<PY><<<npairs, kThreads, seq_smem(L.ny, 3), s>>>(dc, par, L.fc, (const double*)f.eta[p],
+                                                              (const double*)f.X[p], RA, f.partials);
   } else if (stage == 1) {
-    kf_rows_BC<PY><<<dim3(npairs, 3), kThreads, row_smem(L.ny, 1), s>>>(
+    kf_rows_BC<PY><<<npairs, kThreads, seq_smem(L.ny, 3), s>>>(
         dc, par, L.fc, RB, RA, (const double*)f.eta[p], (const float*)f.X_al[p], (const float*)f.X_th[p],
         (float*)f.g[0], (float*)f.g[1], (float*)f.g[2], f.partials);
   } else {
-    kf_rows_D<PY><<<npairs, kThreads, row_smem(L.ny, 2), s>>>(
+    kf_rows_D<PY><<<npairs, kThreads, seq_smem(L.ny, 2), s>>>(
         dc, par, L.fc, RB, (const double*)f.eta[p], (const double*)f.X[p], (double*)f.eta[q], (double*)f.X[q],
         (float*)f.X_al[q], (float*)f.X_th[q], (const double*)f.eta_m, (const double*)f.X_m, (float*)f.mu,
         (float*)f.g[0], (float*)f.g[1], (float*)f.g[2], f.partials);
@@ -798,12 +813,13 @@ void launch_cols(const KksFftLaunch& L, int stage, cudaStream_t s) {
   float2* RA = (float2*)L.RA;
   float2* RB = (float2*)L.RB;
   float2* SA = (float2*)L.SA;
+  const int nb = col_blocks(L.nyh);
   if (stage == 0) {
-    kf_cols_AB<PX><<<dim3(L.nyh, 4), kThreads, col_smem(L.nx, 1), s>>>(L.dc, L.par, L.fc, RA, SA, RB, L.f->ky,
-                                                                        L.f->partials);
+    kf_cols_AB<PX><<<dim3(nb, 4), kThreads, seq_smem(L.nx, kCols), s>>>(L.dc, L.par, L.fc, RA, SA, RB, L.f->ky,
+                                                                         L.f->partials);
   } else {
-    kf_cols_CD_eta<PX><<<L.nyh, kThreads, col_smem(L.nx, 1), s>>>(L.dc, L.par, L.fc, RA, SA, RB, L.f->ky);
-    kf_cols_CD_X<PX><<<L.nyh, kThreads, col_smem(L.nx, 2), s>>>(L.dc, L.par, L.fc, RA, SA, RB, L.f->ky);
+    kf_cols_CD_eta<PX><<<nb, kThreads, seq_smem(L.nx, kCols), s>>>(L.dc, L.par, L.fc, RA, SA, RB, L.f->ky);
+    kf_cols_CD_X<PX><<<nb, kThreads, seq_smem(L.nx, 2 * kCols), s>>>(L.dc, L.par, L.fc, RA, SA, RB, L.f->ky);
   }
 }
 
@@ -817,17 +833,17 @@ cudaError_t set_attr(K* kernel, size_t smem) {
 
 template <int PY>
 int set_row_attrs(int ny) {
-  cudaError_t e = set_attr(kf_rows_A<PY>, row_smem(ny, 1));
-  if (e == cudaSuccess) e = set_attr(kf_rows_BC<PY>, row_smem(ny, 1));
-  if (e == cudaSuccess) e = set_attr(kf_rows_D<PY>, row_smem(ny, 2));
+  cudaError_t e = set_attr(kf_rows_A<PY>, seq_smem(ny, 3));
+  if (e == cudaSuccess) e = set_attr(kf_rows_BC<PY>, seq_smem(ny, 3));
+  if (e == cudaSuccess) e = set_attr(kf_rows_D<PY>, seq_smem(ny, 2));
   return (int)e;
 }
 
 template <int PX>
 int set_col_attrs(int nx) {
-  cudaError_t e = set_attr(kf_cols_AB<PX>, col_smem(nx, 1));
-  if (e == cudaSuccess) e = set_attr(kf_cols_CD_eta<PX>, col_smem(nx, 1));
-  if (e == cudaSuccess) e = set_attr(kf_cols_CD_X<PX>, col_smem(nx, 2));
+  cudaError_t e = set_attr(kf_cols_AB<PX>, seq_smem(nx, kCols));
+  if (e == cudaSuccess) e = set_attr(kf_cols_CD_eta<PX>, seq_smem(nx, kCols));
+  if (e == cudaSuccess) e = set_attr(kf_cols_CD_X<PX>, seq_smem(nx, 2 * kCols));
   return (int)e;
 }
 
@@ -856,7 +872,7 @@ void prime_table(std::vector<float2>& t) {
 }  // namespace
 
 size_t kks_fft_smem_bytes(int nx, int ny) {
-  const size_t r = row_smem(ny, 2), c = col_smem(nx, 2);
+  const size_t r = seq_smem(ny, 3), c = seq_smem(nx, 2 * kCols);
   return (r > c ? r : c) + 1024;  // + the reduction scratch
 }
 
@@ -864,8 +880,8 @@ int kks_fft_row_blocks(int nx) { return (nx + 1) / 2; }
 
 int kks_fft_partial_rows(int nx, int ny, int nbx) {
   int m = kks_fft_row_blocks(nx);
-  const int nyh = ny / 2 + 1;  // the column pass that writes sums has one block per column
-  if (nyh > m) m = nyh;
+  const int cb = col_blocks(ny / 2 + 1);  // the column pass that writes sums
+  if (cb > m) m = cb;
   return m > nbx ? m : nbx;
 }
 
@@ -885,18 +901,20 @@ int kks_fft_upload_prime_tables() {
   std::vector<float2> t;
   prime_table<11>(t);
   cudaError_t e = cudaMemcpyToSymbol(kPrimeTw11, t.data(), t.size() * sizeof(float2));
-  if (e != cudaSuccess) return (int)e;
-  prime_table<19>(t);
-  e = cudaMemcpyToSymbol(kPrimeTw19, t.data(), t.size() * sizeof(float2));
-  if (e != cudaSuccess) return (int)e;
-  prime_table<71>(t);
-  e = cudaMemcpyToSymbol(kPrimeTw71, t.data(), t.size() * sizeof(float2));
+  if (e == cudaSuccess) {
+    prime_table<19>(t);
+    e = cudaMemcpyToSymbol(kPrimeTw19, t.data(), t.size() * sizeof(float2));
+  }
+  if (e == cudaSuccess) {
+    prime_table<71>(t);
+    e = cudaMemcpyToSymbol(kPrimeTw71, t.data(), t.size() * sizeof(float2));
+  }
   return (int)e;
 }
 
 void kks_fft_launch_attempt(const KksFftLaunch& L, int p, cudaStream_t s) {
   const KksFieldPtrs& f = *L.f;
-  kf_extras<<<L.nbx, kThreads, 0, s>>>(L.dc, L.par, (const double*)f.eta[p], 2, 0, P3_IFACE, f.partials);
+  kf_extras<<<L.nbx, kExtrasThreads, 0, s>>>(L.dc, L.par, (const double*)f.eta[p], 2, 0, P3_IFACE, f.partials);
 #define KKS_ROWS(P) launch_rows<P>(L, p, stage, s)
 #define KKS_COLS(P) launch_cols<P>(L, stage, s)
   int stage = 0;
@@ -909,6 +927,6 @@ void kks_fft_launch_attempt(const KksFftLaunch& L, int p, cudaStream_t s) {
   KKS_FFT_DISPATCH(L.PY, KKS_ROWS)
 #undef KKS_ROWS
 #undef KKS_COLS
-  kf_extras<<<L.nbx, kThreads, 0, s>>>(L.dc, L.par, (const double*)f.eta[1 - p], 3, P5_GRAD2, P5_IFACE,
+  kf_extras<<<L.nbx, kExtrasThreads, 0, s>>>(L.dc, L.par, (const double*)f.eta[1 - p], 3, P5_GRAD2, P5_IFACE,
                                        f.partials);
 }

@@ -8,7 +8,8 @@
 #include "kks_internal.cuh"
 
 #define KKS_FFT_MAXST 16
-#define KKS_FFT_THREADS 128   // threads of every pass block
+#define KKS_FFT_THREADS 320   // threads of every pass block (ten warps)
+#define KKS_FFT_COLS 3        // y-frequency columns per column-pass block
 #define KKS_FFT_MAXN 8192     // longest axis of the pipeline (shared memory and 32-bit index magic)
 
 // In-place mixed-radix transform of length n along one axis. Stage s has radix
