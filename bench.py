@@ -126,7 +126,7 @@ def bench_config(precision, armed=None, attempts=None):
                     "400->719 K at 20 K/min, adaptive dt; one cell per GPU",
         "grid": [1420, 1420],
         "precision": precision,
-        "l2": "per-attempt working set ~300 MB > 126 MB L2 (no flush needed)",
+        "l2": "inputs larger than L2: an unarmed attempt touches ~160 MB (FP64 state in and out 96 MB, spectra 64 MB) > 126 MB L2; no flush",
     }
     if armed is not None:
         cfg["armed"] = armed
@@ -191,6 +191,35 @@ def cpu_baseline(state, cfg):
             "sample": f"first {k} steps of the same 1420^2 cell, FP64 numpy oracle, scipy.fft with {cores} workers"}
 
 
+def ensemble_leg(precision, device, steps, warmup):
+    """Batched cell-steps/s of the 48-cell ensemble (sides 128..512, heating
+    rates U(5,40) K/min): every cell on its own stream through kks_run_many,
+    against the same steps run one cell after the other."""
+    from pf_kks_gpu import workloads
+    from pf_kks_gpu.ensemble import Ensemble
+
+    members = [(cfg, workloads.initial_state(cfg, spec)) for cfg, spec in workloads.ensemble(48, 100000, precision)]
+    ens = Ensemble(members, precision=precision, device=device)
+    try:
+        ens.run(warmup)
+
+        def advance(fn):
+            before = [c.state().istep for c in ens.cells]
+            t0 = time.perf_counter()
+            fn(steps)
+            dt = time.perf_counter() - t0
+            done = [c.state().istep - b for c, b in zip(ens.cells, before)]
+            return sum(n * d for n, d in zip(ens.points, done)) / dt
+
+        concurrent = advance(ens.run)
+        sequential = advance(ens.run_sequential)
+    finally:
+        ens.close()
+    return {"cells": len(members), "points": int(sum(c.nx * c.ny for c, _ in members)), "steps": steps,
+            "cell_steps_per_s": concurrent, "sequential_cell_steps_per_s": sequential,
+            "speedup": concurrent / sequential, "timing": "host wall clock around kks_run_many (one sync per batch)"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -199,6 +228,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
     ap.add_argument("--precision", default="mixed", choices=("mixed", "mixed-cufft", "fp64"))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the 48-cell ensemble leg")
     ap.add_argument("--only-timed", action="store_true",
                     help="skip the FP64 comparison and end-to-end cells (profiling runs)")
     args = ap.parse_args()
@@ -242,6 +272,7 @@ def main():
         return float(t.item())
 
     cell = solver.Cell(cfg, tables, precision=args.precision, device=local_rank)
+    fused, kernels_per_attempt = cell.pipeline()
     cell.upload(*state)
     cell.run(args.warmup)
     cell.drain()
@@ -345,7 +376,9 @@ def main():
             "unit": "GB/s",
             "frac": achieved / peak,
             "traffic": traffic,
-            "kernel": "one attempt (captured CUDA graph: 8 own kernels + cuFFT R2C/C2R)",
+            "kernel": ("one attempt (captured CUDA graph of 11 kernels: shared-memory FFT passes fused with the "
+                       "pointwise stages)") if fused else
+                      "one attempt (captured CUDA graph: 8 own kernels + cuFFT R2C/C2R)",
             "algorithmic_bytes": alg_bytes,
             "peak_kind": peak_kind,
         },
@@ -357,8 +390,10 @@ def main():
             "d2h_bytes_per_step": (4 * N * 8 + len(rows) * 256 + len(recs) * 128) / max(e2e_steps, 1),
             "note": "kks_upload (4 fields) + kks_run(K) + kks_drain + kks_download (4 fields) per call of K steps",
         },
-        "gpu_launches": int(8 * attempts),
+        "gpu_launches": int(kernels_per_attempt * attempts),
     }
+    if not args.no_ensemble and args.precision != "fp64":
+        line["ensemble"] = ensemble_leg(args.precision, local_rank, steps=20, warmup=3)
     if not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline(state, cfg)
     print(json.dumps(line), flush=True)

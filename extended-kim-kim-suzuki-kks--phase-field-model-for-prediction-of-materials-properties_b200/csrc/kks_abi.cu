@@ -913,6 +913,17 @@ int kks_timing(kks_handle* h, double* device_ms, int64_t* attempts) {
   return KKS_OK;
 }
 
+int kks_pipeline(kks_handle* h, int32_t* fused, int32_t* kernels) {
+  if (!h) return set_error(KKS_ERR_ARG, "null handle");
+  if (fused) *fused = h->fused ? 1 : 0;
+  // fused: prologue, extras (old state), rows A, cols AB, rows BC, cols CD (2),
+  // rows D, extras (new state), decide, restore; cuFFT pipeline: prologue,
+  // prep, spectral_mid, pre_pointwise, spectral_update, post_pointwise,
+  // decide, restore
+  if (kernels) *kernels = h->fused ? 11 : 8;
+  return KKS_OK;
+}
+
 int kks_destroy(kks_handle* h) {
   free_handle(h);
   return KKS_OK;

@@ -45,7 +45,7 @@ H = {
 EXPORTS = (
     "kks_create", "kks_upload", "kks_run", "kks_drain", "kks_get_state", "kks_download", "kks_elastic_fields",
     "kks_checkpoint", "kks_restore", "kks_timing", "kks_destroy", "kks_last_error", "kks_version",
-    "kks_state_sums_noalloc", "kks_run_many",
+    "kks_state_sums_noalloc", "kks_run_many", "kks_pipeline",
 )
 
 
@@ -124,6 +124,7 @@ def load(path=LIB_PATH):
     lib.kks_checkpoint.argtypes = [vp, vp, ctypes.c_size_t, P(ctypes.c_size_t)]
     lib.kks_restore.argtypes = [vp, vp, ctypes.c_size_t]
     lib.kks_timing.argtypes = [vp, dp, P(ctypes.c_int64)]
+    lib.kks_pipeline.argtypes = [vp, P(ctypes.c_int32), P(ctypes.c_int32)]
     lib.kks_destroy.argtypes = [vp]
     lib.kks_run_many.argtypes = [P(vp), ctypes.c_int32, P(ctypes.c_int32), P(ctypes.c_int32)]
     lib.kks_run_many.restype = ctypes.c_int
@@ -132,7 +133,7 @@ def load(path=LIB_PATH):
     lib.kks_last_error.restype = ctypes.c_char_p
     lib.kks_version.restype = ctypes.c_char_p
     for name in ("kks_create", "kks_upload", "kks_run", "kks_drain", "kks_get_state", "kks_download",
-                 "kks_elastic_fields", "kks_checkpoint", "kks_restore", "kks_timing", "kks_destroy"):
+                 "kks_elastic_fields", "kks_checkpoint", "kks_restore", "kks_timing", "kks_pipeline", "kks_destroy"):
         getattr(lib, name).restype = ctypes.c_int
     _lib = lib
     return lib

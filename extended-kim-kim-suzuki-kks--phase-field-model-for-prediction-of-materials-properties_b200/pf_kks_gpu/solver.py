@@ -207,6 +207,14 @@ class Cell:
         L.check(self.lib.kks_timing(self.h, ctypes.byref(ms), ctypes.byref(n)), "kks_timing")
         return ms.value, n.value
 
+    def pipeline(self):
+        """(fused, kernels): 1 if the attempt runs the shared-memory FFT passes,
+        and the kernels of this library one attempt launches."""
+        fused = ctypes.c_int32(0)
+        kernels = ctypes.c_int32(0)
+        L.check(self.lib.kks_pipeline(self.h, ctypes.byref(fused), ctypes.byref(kernels)), "kks_pipeline")
+        return bool(fused.value), int(kernels.value)
+
     def close(self):
         if getattr(self, "h", None):
             self.lib.kks_destroy(self.h)

@@ -167,6 +167,12 @@ int kks_restore(kks_handle* h, const void* buf, size_t size);
  * handle's stream) and the attempts they covered. */
 int kks_timing(kks_handle* h, double* device_ms, int64_t* attempts);
 
+/* No counterpart in the reference. The attempt pipeline of the handle:
+ * *fused = 1 for the shared-memory FFT passes of the mixed path, 0 for the
+ * cuFFT pipeline; *kernels = kernels of this library one attempt launches
+ * (cuFFT's own kernels not counted). Either pointer may be NULL. */
+int kks_pipeline(kks_handle* h, int32_t* fused, int32_t* kernels);
+
 int kks_destroy(kks_handle* h);
 
 /* No counterpart in the reference. For callers that cannot allocate device
