@@ -297,6 +297,7 @@ static int setup_fused(kks_handle* h, const std::vector<double>& kx) {
   KksFftLaunch& L = h->fl;
   L.dc = h->dc;
   L.par = h->d_par;
+  L.ctl = h->d_ctl;
   L.fc = h->d_fc;
   L.f = &h->f;
   L.RA = RA;
@@ -308,6 +309,8 @@ static int setup_fused(kks_handle* h, const std::vector<double>& kx) {
   L.nbx = h->nblocks;
   L.PX = fc.ax.P;
   L.PY = fc.ay.P;
+  // bulk copies of whole row pairs need 16-byte multiples for the f32 rows
+  L.bulk_rows = c.ny % 4 == 0 ? 1 : 0;
   if (kks_fft_set_attributes(L) != 0) return set_error(KKS_ERR_CUDA, "fft kernel attributes");
   // every kernel of the pipeline writes one partial-sum row per block: the
   // buffer holds the largest grid of them (row pairs, column tiles, extras)

@@ -279,6 +279,54 @@ __device__ __forceinline__ int fdiv(int x, int d, uint32_t m) {
   return d == 1 ? x : (int)__umulhi((uint32_t)x, m);
 }
 
+// ---------------------------------------------------------------------------
+// Bulk copies (global -> shared, completion counted on an mbarrier): a row
+// pass stages the state rows its pointwise phase needs at kernel entry, so the
+// loads overlap the merge and the inverse FFT. Source, destination and size
+// are multiples of 16 bytes (the host enables this only for ny % 4 == 0).
+constexpr int kWaitLimit = 1 << 20;  // try_wait polls before a wait is declared lost
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Wait for phase 0 of bar with a bounded number of polls. If it runs out the
+// cell's status becomes KKS_STATUS_TIMEOUT (the host stops the run and reports
+// it) and the block waits once more, again bounded, for its copies in flight.
+__device__ __forceinline__ void bulk_wait(uint64_t* bar, KksCtl* ctl) {
+  bool done = false;
+  for (int i = 0; i < kWaitLimit && !done; ++i) done = mbar_try_wait(bar, 0);
+  if (!done) {
+    atomicCAS(&ctl->status, KKS_STATUS_OK, KKS_STATUS_TIMEOUT);
+    for (int i = 0; i < kWaitLimit && !done; ++i) done = mbar_try_wait(bar, 0);
+  }
+}
+
 // nseq in-place transforms of length ax.n, sequence s at offset s * n of the
 // block's dynamic shared memory. DIR = -1: forward DIF (natural ->
 // digit-reversed); DIR = +1: inverse DIT (digit-reversed -> natural),
@@ -509,17 +557,35 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
     kf_rows_BC(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const KksFftConst* __restrict__ fc,
                const float2* __restrict__ RB, float2* __restrict__ RC, const double* __restrict__ eta,
                const float* __restrict__ Xal, const float* __restrict__ Xth, float* g0, float* g1, float* g2,
-               double* __restrict__ partials) {
+               double* __restrict__ partials, KksCtl* ctl, int bulk) {
   if (!par->active) return;
   extern __shared__ float2 sm[];
+  __shared__ __align__(8) uint64_t bar;
   const KksFftAxis& ay = fc->ay;
   const int nx = c->nx, ny = c->ny, nyh = c->nyh;
   const size_t fs = (size_t)nx * nyh;
   const int ix0 = 2 * blockIdx.x;
   const bool has1 = ix0 + 1 < nx;
+  // staged rows ix0 (and ix0+1) of eta, X_al, X_th after the three sequences
+  double* s_eta = (double*)(sm + 3 * ny);
+  float* s_al = (float*)(s_eta + 2 * ny);
+  float* s_th = s_al + 2 * ny;
+  if (bulk) {
+    if (threadIdx.x == 0) mbar_init(&bar);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const uint32_t n = (has1 ? 2u : 1u) * (uint32_t)ny;
+      const size_t i0 = (size_t)ix0 * ny;
+      mbar_expect_tx(&bar, n * 16u);
+      bulk_g2s(s_eta, eta + i0, n * 8u, &bar);
+      bulk_g2s(s_al, Xal + i0, n * 4u, &bar);
+      bulk_g2s(s_th, Xth + i0, n * 4u, &bar);
+    }
+  }
   for (int f = 0; f < 3; ++f) merge_load(sm + f * ny, ay, RB + f * fs, ix0, has1, nx, nyh);
   __syncthreads();
   fft_run<+1, PY>(3, ay);
+  if (bulk) bulk_wait(&bar, ctl);
   const KksPar q = *par;
   float* gs_buf = q.gs == 0 ? g0 : (q.gs == 1 ? g1 : g2);
   const float A_a = (float)q.A_alp_s, va = (float)q.va, fa0 = (float)q.fa0;
@@ -535,8 +601,9 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
       dr[r] = fxv[r] = fyv[r] = 0.f;
       if (r == 1 && !has1) continue;
       const size_t i = (size_t)(ix0 + r) * ny + y;
-      const float e = (float)eta[i];
-      const float ca = Xal[i], ct = Xth[i];
+      const int is = r * ny + y;
+      const float e = (float)(bulk ? s_eta[is] : eta[i]);
+      const float ca = bulk ? s_al[is] : Xal[i], ct = bulk ? s_th[is] : Xth[i];
       const float da = ca - va, dtt = ct - vt;
       const float fa_s = A_a * da * da + fa0;
       const float fa_ca_s = 2.0f * A_a * da;
@@ -662,18 +729,35 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
               const float2* __restrict__ RD, const double* __restrict__ eta_o, const double* __restrict__ X_o,
               double* __restrict__ eta_b, double* __restrict__ X_b, float* __restrict__ Xal_b,
               float* __restrict__ Xth_b, const double* __restrict__ eta_m, const double* __restrict__ X_m,
-              float* __restrict__ mu, float* g0, float* g1, float* g2, double* __restrict__ partials) {
+              float* __restrict__ mu, float* g0, float* g1, float* g2, double* __restrict__ partials, KksCtl* ctl,
+              int bulk) {
   if (!par->active) return;
   extern __shared__ float2 sm[];
+  __shared__ __align__(8) uint64_t bar;
   const KksFftAxis& ay = fc->ay;
   const int nx = c->nx, ny = c->ny, nyh = c->nyh;
   const size_t fs = (size_t)nx * nyh;
   const int ix0 = 2 * blockIdx.x;
   const bool has1 = ix0 + 1 < nx;
+  // staged rows ix0 (and ix0+1) of the old eta and X after the two sequences
+  double* s_eta = (double*)(sm + 2 * ny);
+  double* s_X = s_eta + 2 * ny;
+  if (bulk) {
+    if (threadIdx.x == 0) mbar_init(&bar);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const uint32_t n = (has1 ? 2u : 1u) * (uint32_t)ny;
+      const size_t i0 = (size_t)ix0 * ny;
+      mbar_expect_tx(&bar, n * 16u);
+      bulk_g2s(s_eta, eta_o + i0, n * 8u, &bar);
+      bulk_g2s(s_X, X_o + i0, n * 8u, &bar);
+    }
+  }
   merge_load(sm, ay, RD, ix0, has1, nx, nyh);
   merge_load(sm + ny, ay, RD + fs, ix0, has1, nx, nyh);
   __syncthreads();
   fft_run<+1, PY>(2, ay);
+  if (bulk) bulk_wait(&bar, ctl);
   const KksPar q = *par;
   float* gb_buf = q.gb == 0 ? g0 : (q.gb == 1 ? g1 : g2);
   const float* gm_buf = q.gm == 0 ? g0 : (q.gm == 1 ? g1 : g2);
@@ -689,8 +773,9 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
     for (int r = 0; r < 2; ++r) {
       if (r == 1 && !has1) continue;
       const size_t i = (size_t)(ix0 + r) * ny + y;
-      const double xo = X_o[i];
-      const double eb = eta_o[i] + (double)(r == 0 ? de.x : de.y);
+      const int is = r * ny + y;
+      const double xo = bulk ? s_X[is] : X_o[i];
+      const double eb = (bulk ? s_eta[is] : eta_o[i]) + (double)(r == 0 ? de.x : de.y);
       const double xb = xo + (double)(r == 0 ? dX.x : dX.y);
       eta_b[i] = eb;
       X_b[i] = xb;
@@ -780,8 +865,11 @@ __global__ void __launch_bounds__(kExtrasThreads)
   if (do_iface) block_reduce_store<1, kExtrasThreads>(a2, partials + (size_t)blockIdx.x * KKS_NPART + slot_iface);
 }
 
-// shared memory of each pass (bytes): its sequences, transformed in place
+// shared memory of each pass (bytes): its sequences, transformed in place,
+// and for rows_BC / rows_D the staged state rows of the pair
 inline size_t seq_smem(int n, int nseq) { return (size_t)nseq * n * sizeof(float2); }
+inline size_t rows_bc_smem(int ny) { return seq_smem(ny, 3) + (size_t)2 * ny * (8 + 4 + 4); }
+inline size_t rows_d_smem(int ny) { return seq_smem(ny, 2) + (size_t)2 * ny * (8 + 8); }
 inline int col_blocks(int nyh) { return (nyh + kCols - 1) / kCols; }
 
 template <int PY>
@@ -797,14 +885,14 @@ void launch_rows(const KksFftLaunch& L, int p, int stage, cudaStream_t s) {
     kf_rows_A<PY><<<npairs, kThreads, seq_smem(L.ny, 3), s>>>(dc, par, L.fc, (const double*)f.eta[p],
                                                               (const double*)f.X[p], RA, f.partials);
   } else if (stage == 1) {
-    kf_rows_BC<PY><<<npairs, kThreads, seq_smem(L.ny, 3), s>>>(
+    kf_rows_BC<PY><<<npairs, kThreads, rows_bc_smem(L.ny), s>>>(
         dc, par, L.fc, RB, RA, (const double*)f.eta[p], (const float*)f.X_al[p], (const float*)f.X_th[p],
-        (float*)f.g[0], (float*)f.g[1], (float*)f.g[2], f.partials);
+        (float*)f.g[0], (float*)f.g[1], (float*)f.g[2], f.partials, L.ctl, L.bulk_rows);
   } else {
-    kf_rows_D<PY><<<npairs, kThreads, seq_smem(L.ny, 2), s>>>(
+    kf_rows_D<PY><<<npairs, kThreads, rows_d_smem(L.ny), s>>>(
         dc, par, L.fc, RB, (const double*)f.eta[p], (const double*)f.X[p], (double*)f.eta[q], (double*)f.X[q],
         (float*)f.X_al[q], (float*)f.X_th[q], (const double*)f.eta_m, (const double*)f.X_m, (float*)f.mu,
-        (float*)f.g[0], (float*)f.g[1], (float*)f.g[2], f.partials);
+        (float*)f.g[0], (float*)f.g[1], (float*)f.g[2], f.partials, L.ctl, L.bulk_rows);
   }
 }
 
@@ -834,8 +922,8 @@ cudaError_t set_attr(K* kernel, size_t smem) {
 template <int PY>
 int set_row_attrs(int ny) {
   cudaError_t e = set_attr(kf_rows_A<PY>, seq_smem(ny, 3));
-  if (e == cudaSuccess) e = set_attr(kf_rows_BC<PY>, seq_smem(ny, 3));
-  if (e == cudaSuccess) e = set_attr(kf_rows_D<PY>, seq_smem(ny, 2));
+  if (e == cudaSuccess) e = set_attr(kf_rows_BC<PY>, rows_bc_smem(ny));
+  if (e == cudaSuccess) e = set_attr(kf_rows_D<PY>, rows_d_smem(ny));
   return (int)e;
 }
 
@@ -872,7 +960,8 @@ void prime_table(std::vector<float2>& t) {
 }  // namespace
 
 size_t kks_fft_smem_bytes(int nx, int ny) {
-  const size_t r = seq_smem(ny, 3), c = seq_smem(nx, 2 * kCols);
+  const size_t r = rows_bc_smem(ny) > rows_d_smem(ny) ? rows_bc_smem(ny) : rows_d_smem(ny);
+  const size_t c = seq_smem(nx, 2 * kCols);
   return (r > c ? r : c) + 1024;  // + the reduction scratch
 }
 

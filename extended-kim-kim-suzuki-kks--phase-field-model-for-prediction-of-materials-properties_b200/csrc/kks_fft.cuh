@@ -40,6 +40,7 @@ struct KksFftConst {
 struct KksFftLaunch {
   const KksConst* dc;
   const KksPar* par;
+  KksCtl* ctl;            // status word (a bounded wait that runs out sets KKS_STATUS_TIMEOUT)
   const KksFftConst* fc;  // device copy
   const KksFieldPtrs* f;
   void* RA;  // 3 row-spectrum fields (also RC)
@@ -48,6 +49,7 @@ struct KksFftLaunch {
   int nx, ny, nyh;
   int nbx;   // grid of the pointwise extras kernel
   int PX, PY;
+  int bulk_rows;  // 1: row passes stage their state rows with bulk copies (needs ny % 4 == 0)
 };
 
 // Largest prime factors with a direct DFT stage; other sizes use cuFFT.

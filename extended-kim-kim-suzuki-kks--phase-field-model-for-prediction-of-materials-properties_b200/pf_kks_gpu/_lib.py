@@ -16,6 +16,7 @@ KKS_OK = 0
 KKS_STATUS_OK = 0
 KKS_STATUS_MAX_ITER = 1
 KKS_STATUS_NONFINITE = 2
+KKS_STATUS_TIMEOUT = 3
 KKS_PRECISION_FP64 = 0
 KKS_PRECISION_MIXED = 1
 KKS_PRECISION_MIXED_CUFFT = 2

@@ -356,6 +356,8 @@ def run(cfg, eta, X, X_al, X_th, out_dir=".", base_dir=".", write_logs=True, ver
             log.flush()
             if status != L.KKS_STATUS_OK:
                 s = cell.state()
+                if status == L.KKS_STATUS_TIMEOUT:
+                    raise L.KksError(f"step {s.istep}: a bounded device wait ran out (bulk copy not completed)")
                 if status == L.KKS_STATUS_MAX_ITER:
                     raise AdaptiveStepError(f"step {s.error_istep}: no admissible time step after "
                                             f"{s.error_iteration} attempts (dtime_s={s.error_dtime_s:.2e})")

@@ -39,6 +39,7 @@ extern "C" {
 #define KKS_STATUS_OK 0
 #define KKS_STATUS_MAX_ITER 1   /* AdaptiveStepError: no admissible step after max_iterations attempts */
 #define KKS_STATUS_NONFINITE 2  /* AdaptiveStepError: non-finite energy residual */
+#define KKS_STATUS_TIMEOUT 3    /* a bounded device wait (bulk-copy completion) ran out; state undefined */
 
 #define KKS_PRECISION_FP64 0  /* all-FP64 step */
 #define KKS_PRECISION_MIXED 1 /* FP32 transforms and pointwise math on the step increments; FP64 state, scalars,
