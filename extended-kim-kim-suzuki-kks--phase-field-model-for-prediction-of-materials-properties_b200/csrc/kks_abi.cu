@@ -12,6 +12,8 @@
 // for the steps that rejections consumed: one host synchronisation per batch
 // of steps, none per attempt.
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 #include <cufft.h>
 #include <math.h>
@@ -245,6 +247,30 @@ static bool build_axis(int n, KksFftAxis& ax, AxisTables& t) {
   return true;
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against libcuda); nullptr when the driver does not provide it.
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  void* fn = nullptr;
+  cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+  if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+      q != cudaDriverEntryPointSuccess)
+    return nullptr;
+  return (PFN_cuTensorMapEncodeTiled_v12000)fn;
+}
+
+// Tensor map of F column-major row-spectrum fields at base (kks_fft.cuh).
+static bool encode_spectrum_map(CUtensorMap* map, void* base, int nx, int nyh, int F) {
+  PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (!enc) return false;
+  const cuuint64_t dims[3] = {(cuuint64_t)nx, (cuuint64_t)nyh, (cuuint64_t)F};
+  const cuuint64_t strides[2] = {(cuuint64_t)nx * 8, (cuuint64_t)nx * nyh * 8};
+  const cuuint32_t box[3] = {2, (cuuint32_t)(nyh < 256 ? nyh : 256), (cuuint32_t)F};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  return enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT64, 3, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 template <typename T>
 static int upload_vec(const std::vector<T>& v, T** dst) {
   CK(cudaMalloc(dst, v.size() * sizeof(T)));
@@ -309,8 +335,12 @@ static int setup_fused(kks_handle* h, const std::vector<double>& kx) {
   L.nbx = h->nblocks;
   L.PX = fc.ax.P;
   L.PY = fc.ay.P;
-  // bulk copies of whole row pairs need 16-byte multiples for the f32 rows
-  L.bulk_rows = c.ny % 4 == 0 ? 1 : 0;
+  // bulk copies of whole row pairs need 16-byte multiples for the f32 rows, the
+  // tensor maps 16-byte strides (nx even; every pair then has both rows)
+  L.bulk_rows = 0;
+  if (c.nx % 2 == 0 && c.ny % 4 == 0 && encode_spectrum_map(&L.map_RA3, RA, c.nx, c.nyh, 3) &&
+      encode_spectrum_map(&L.map_RB3, RB, c.nx, c.nyh, 3) && encode_spectrum_map(&L.map_RB2, RB, c.nx, c.nyh, 2))
+    L.bulk_rows = 1;
   if (kks_fft_set_attributes(L) != 0) return set_error(KKS_ERR_CUDA, "fft kernel attributes");
   // every kernel of the pipeline writes one partial-sum row per block: the
   // buffer holds the largest grid of them (row pairs, column tiles, extras)

@@ -48,6 +48,8 @@
 
 #include <vector>
 
+#include <cuda.h>
+
 #include "kks_internal.cuh"
 #include "kks_fft.cuh"
 
@@ -315,16 +317,60 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Wait for phase 0 of bar with a bounded number of polls. If it runs out the
-// cell's status becomes KKS_STATUS_TIMEOUT (the host stops the run and reports
-// it) and the block waits once more, again bounded, for its copies in flight.
-__device__ __forceinline__ void bulk_wait(uint64_t* bar, KksCtl* ctl) {
+// Wait for the phase of bar with the given parity, with a bounded number of
+// polls. If it runs out the cell's status becomes KKS_STATUS_TIMEOUT (the host
+// stops the run and reports it) and the block waits once more, again bounded,
+// for its copies in flight.
+__device__ __forceinline__ void bulk_wait(uint64_t* bar, uint32_t parity, KksCtl* ctl) {
   bool done = false;
-  for (int i = 0; i < kWaitLimit && !done; ++i) done = mbar_try_wait(bar, 0);
+  for (int i = 0; i < kWaitLimit && !done; ++i) done = mbar_try_wait(bar, parity);
   if (!done) {
     atomicCAS(&ctl->status, KKS_STATUS_OK, KKS_STATUS_TIMEOUT);
-    for (int i = 0; i < kWaitLimit && !done; ++i) done = mbar_try_wait(bar, 0);
+    for (int i = 0; i < kWaitLimit && !done; ++i) done = mbar_try_wait(bar, parity);
   }
+}
+
+// Orders this thread's generic shared-memory accesses before later bulk /
+// tensor copies that read or overwrite the same bytes.
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// Tensor copies of a row pair's half spectra. A spectrum buffer is viewed as a
+// 3-D tensor of 8-byte elements (x: nx, ky: nyh, field: F) and a box is
+// {2, kb, F}: rows ix0, ix0 + 1 of kb consecutive frequencies of every field.
+// Box b lands at stage + b * F * kb * 2 (float2 units) as [field][ky][x].
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void tma_store_3d(const CUtensorMap* map, int x, int y, int z, const void* src) {
+  asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(
+                   reinterpret_cast<uint64_t>(map)),
+               "r"(x), "r"(y), "r"(z), "r"(smem_u32(src))
+               : "memory");
+}
+
+// Commit the bulk stores issued by this thread and wait until they are done.
+__device__ __forceinline__ void bulk_store_drain() {
+  asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+  asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+}
+
+// Position of (frequency k, field f, row xi) in a staged box set with box
+// height kb (256, or nyh when a single box holds them all).
+__device__ __forceinline__ int stage_at(int k, int f, int F, int kb, int xi) {
+  const int b = kb == 256 ? (k >> 8) : 0;
+  return ((b * F + f) * kb + (k - b * kb)) * 2 + xi;
+}
+
+// The staging area: 128-byte aligned, after `seq_bytes` of sequences.
+__device__ __forceinline__ char* stage_base(void* sm, uint32_t seq_bytes) {
+  const uint32_t base = smem_u32(sm);
+  const uint32_t off = ((base + seq_bytes + 127u) & ~127u) - base;
+  return (char*)sm + off;
 }
 
 // nseq in-place transforms of length ax.n, sequence s at offset s * n of the
@@ -433,6 +479,50 @@ __device__ __forceinline__ void merge_load(float2* z, const KksFftAxis& ay, cons
   }
 }
 
+// split_store / merge_load against a staged box set (field f of F) instead of
+// global memory; the tensor copies move the boxes.
+__device__ __forceinline__ void split_stage(const float2* z, const KksFftAxis& ay, float2* stage, int f, int F,
+                                            int kb, int nyh) {
+  const int ny = ay.n;
+  for (int k = threadIdx.x; k < nyh; k += kThreads) {
+    const float2 Zk = z[__ldg(ay.slot + k)];
+    const float2 Zm = z[__ldg(ay.slot + (k == 0 ? 0 : ny - k))];
+    const int i = stage_at(k, f, F, kb, 0);
+    stage[i] = make_float2(0.5f * (Zk.x + Zm.x), 0.5f * (Zk.y - Zm.y));
+    stage[i + 1] = make_float2(0.5f * (Zk.y + Zm.y), -0.5f * (Zk.x - Zm.x));
+  }
+}
+
+__device__ __forceinline__ void merge_stage(float2* z, const KksFftAxis& ay, const float2* stage, int f, int F, int kb,
+                                            int nyh) {
+  const int ny = ay.n;
+  for (int k = threadIdx.x; k < nyh; k += kThreads) {
+    const int i = stage_at(k, f, F, kb, 0);
+    float2 A = stage[i], B = stage[i + 1];
+    const bool self = k == 0 || 2 * k == ny;
+    if (self) {
+      A.y = 0.f;
+      B.y = 0.f;
+    }
+    z[__ldg(ay.slot + k)] = make_float2(A.x - B.y, A.y + B.x);
+    if (!self) z[__ldg(ay.slot + (ny - k))] = make_float2(A.x + B.y, B.x - A.y);
+  }
+}
+
+// Issue the tensor loads of all boxes of a row pair (thread 0) on bar.
+__device__ __forceinline__ void stage_load(float2* stage, const CUtensorMap* map, int ix0, int F, int kb, int nb,
+                                           uint64_t* bar) {
+  mbar_expect_tx(bar, (uint32_t)(nb * F * kb * 16));
+  for (int b = 0; b < nb; ++b) tma_load_3d(stage + b * F * kb * 2, map, ix0, b * kb, 0, bar);
+}
+
+// Store all boxes of a row pair (thread 0, after a fence and a barrier).
+__device__ __forceinline__ void stage_store(const CUtensorMap* map, const float2* stage, int ix0, int F, int kb,
+                                            int nb) {
+  for (int b = 0; b < nb; ++b) tma_store_3d(map, ix0, b * kb, 0, stage + b * F * kb * 2);
+  bulk_store_drain();
+}
+
 // ---------------------------------------------------------------------------
 // pass 1: one row pair; the sequences are eta, X, eta^2 -> row spectra RA;
 // old-state history sums.
@@ -440,18 +530,39 @@ template <int PY>
 __global__ void __launch_bounds__(kThreads, kMinBlocks)
     kf_rows_A(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const KksFftConst* __restrict__ fc,
               const double* __restrict__ eta, const double* __restrict__ X, float2* __restrict__ RA,
-              double* __restrict__ partials) {
+              double* __restrict__ partials, KksCtl* ctl, int bulk, const __grid_constant__ CUtensorMap map_RA) {
   if (!par->active) return;
   extern __shared__ float2 sm[];
+  __shared__ __align__(8) uint64_t bar;
   const KksFftAxis& ay = fc->ay;
   const int nx = c->nx, ny = c->ny, nyh = c->nyh;
   const int ix0 = 2 * blockIdx.x;
   const bool has1 = ix0 + 1 < nx;
   const size_t i0 = (size_t)ix0 * ny;
+  // staging after the three sequences: rows ix0, ix0+1 of eta and X, later
+  // the three split half spectra of the pair
+  char* stage = stage_base(sm, 3u * ny * (uint32_t)sizeof(float2));
+  const double* s_eta = (const double*)stage;
+  const double* s_X = s_eta + 2 * ny;
+  if (bulk) {
+    if (threadIdx.x == 0) mbar_init(&bar);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      mbar_expect_tx(&bar, 32u * (uint32_t)ny);
+      bulk_g2s((void*)s_eta, eta + i0, 16u * ny, &bar);
+      bulk_g2s((void*)s_X, X + i0, 16u * ny, &bar);
+    }
+    bulk_wait(&bar, 0, ctl);
+  }
   double acc[5] = {0, 0, 0, 0, 0};
   for (int y = threadIdx.x; y < ny; y += kThreads) {
-    const double e0 = eta[i0 + y], x0 = X[i0 + y];
-    const double e1 = has1 ? eta[i0 + ny + y] : 0.0, x1 = has1 ? X[i0 + ny + y] : 0.0;
+    double e0, x0, e1, x1;
+    if (bulk) {
+      e0 = s_eta[y], x0 = s_X[y], e1 = s_eta[ny + y], x1 = s_X[ny + y];
+    } else {
+      e0 = eta[i0 + y], x0 = X[i0 + y];
+      e1 = has1 ? eta[i0 + ny + y] : 0.0, x1 = has1 ? X[i0 + ny + y] : 0.0;
+    }
     sm[y] = make_float2((float)e0, (float)e1);
     sm[ny + y] = make_float2((float)x0, (float)x1);
     sm[2 * ny + y] = make_float2((float)(e0 * e0), (float)(e1 * e1));
@@ -467,7 +578,16 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
   __syncthreads();
   fft_run<-1, PY>(3, ay);
   const size_t fs = (size_t)nx * nyh;
-  for (int f = 0; f < 3; ++f) split_store(sm + f * ny, ay, RA + f * fs, ix0, has1, nx, nyh);
+  if (bulk) {
+    const int kb = nyh < 256 ? nyh : 256, nb = (nyh + kb - 1) / kb;
+    float2* st = (float2*)stage;
+    for (int f = 0; f < 3; ++f) split_stage(sm + f * ny, ay, st, f, 3, kb, nyh);
+    fence_async_smem();
+    __syncthreads();
+    if (threadIdx.x == 0) stage_store(&map_RA, st, ix0, 3, kb, nb);
+  } else {
+    for (int f = 0; f < 3; ++f) split_store(sm + f * ny, ay, RA + f * fs, ix0, has1, nx, nyh);
+  }
   block_reduce_store<5>(acc, partials + (size_t)blockIdx.x * KKS_NPART + P3_ETA);
 }
 
@@ -557,7 +677,8 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
     kf_rows_BC(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const KksFftConst* __restrict__ fc,
                const float2* __restrict__ RB, float2* __restrict__ RC, const double* __restrict__ eta,
                const float* __restrict__ Xal, const float* __restrict__ Xth, float* g0, float* g1, float* g2,
-               double* __restrict__ partials, KksCtl* ctl, int bulk) {
+               double* __restrict__ partials, KksCtl* ctl, int bulk, const __grid_constant__ CUtensorMap map_RB,
+               const __grid_constant__ CUtensorMap map_RC) {
   if (!par->active) return;
   extern __shared__ float2 sm[];
   __shared__ __align__(8) uint64_t bar;
@@ -566,26 +687,38 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
   const size_t fs = (size_t)nx * nyh;
   const int ix0 = 2 * blockIdx.x;
   const bool has1 = ix0 + 1 < nx;
-  // staged rows ix0 (and ix0+1) of eta, X_al, X_th after the three sequences
-  double* s_eta = (double*)(sm + 3 * ny);
-  float* s_al = (float*)(s_eta + 2 * ny);
-  float* s_th = s_al + 2 * ny;
+  const int kb = nyh < 256 ? nyh : 256, nb = (nyh + kb - 1) / kb;
+  // staging after the three sequences: the pair's three half spectra (tensor
+  // load), then rows ix0, ix0+1 of eta, X_al, X_th (bulk copies, overlapping
+  // the inverse FFT), then the three split half spectra (tensor store)
+  char* stage = stage_base(sm, 3u * ny * (uint32_t)sizeof(float2));
+  float2* st = (float2*)stage;
+  const double* s_eta = (const double*)stage;
+  const float* s_al = (const float*)(s_eta + 2 * ny);
+  const float* s_th = s_al + 2 * ny;
   if (bulk) {
-    if (threadIdx.x == 0) mbar_init(&bar);
+    if (threadIdx.x == 0) {
+      mbar_init(&bar);
+      stage_load(st, &map_RB, ix0, 3, kb, nb, &bar);
+    }
+    __syncthreads();
+    bulk_wait(&bar, 0, ctl);
+    for (int f = 0; f < 3; ++f) merge_stage(sm + f * ny, ay, st, f, 3, kb, nyh);
     __syncthreads();
     if (threadIdx.x == 0) {
-      const uint32_t n = (has1 ? 2u : 1u) * (uint32_t)ny;
       const size_t i0 = (size_t)ix0 * ny;
-      mbar_expect_tx(&bar, n * 16u);
-      bulk_g2s(s_eta, eta + i0, n * 8u, &bar);
-      bulk_g2s(s_al, Xal + i0, n * 4u, &bar);
-      bulk_g2s(s_th, Xth + i0, n * 4u, &bar);
+      fence_async_smem();
+      mbar_expect_tx(&bar, 32u * (uint32_t)ny);
+      bulk_g2s((void*)s_eta, eta + i0, 16u * ny, &bar);
+      bulk_g2s((void*)s_al, Xal + i0, 8u * ny, &bar);
+      bulk_g2s((void*)s_th, Xth + i0, 8u * ny, &bar);
     }
+  } else {
+    for (int f = 0; f < 3; ++f) merge_load(sm + f * ny, ay, RB + f * fs, ix0, has1, nx, nyh);
+    __syncthreads();
   }
-  for (int f = 0; f < 3; ++f) merge_load(sm + f * ny, ay, RB + f * fs, ix0, has1, nx, nyh);
-  __syncthreads();
   fft_run<+1, PY>(3, ay);
-  if (bulk) bulk_wait(&bar, ctl);
+  if (bulk) bulk_wait(&bar, 1, ctl);
   const KksPar q = *par;
   float* gs_buf = q.gs == 0 ? g0 : (q.gs == 1 ? g1 : g2);
   const float A_a = (float)q.A_alp_s, va = (float)q.va, fa0 = (float)q.fa0;
@@ -630,7 +763,14 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
   }
   __syncthreads();
   fft_run<-1, PY>(3, ay);
-  for (int f = 0; f < 3; ++f) split_store(sm + f * ny, ay, RC + f * fs, ix0, has1, nx, nyh);
+  if (bulk) {
+    for (int f = 0; f < 3; ++f) split_stage(sm + f * ny, ay, st, f, 3, kb, nyh);
+    fence_async_smem();
+    __syncthreads();
+    if (threadIdx.x == 0) stage_store(&map_RC, st, ix0, 3, kb, nb);
+  } else {
+    for (int f = 0; f < 3; ++f) split_store(sm + f * ny, ay, RC + f * fs, ix0, has1, nx, nyh);
+  }
   double acc[1] = {accG};
   block_reduce_store<1>(acc, partials + (size_t)blockIdx.x * KKS_NPART + P3_G);
 }
@@ -730,7 +870,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
               double* __restrict__ eta_b, double* __restrict__ X_b, float* __restrict__ Xal_b,
               float* __restrict__ Xth_b, const double* __restrict__ eta_m, const double* __restrict__ X_m,
               float* __restrict__ mu, float* g0, float* g1, float* g2, double* __restrict__ partials, KksCtl* ctl,
-              int bulk) {
+              int bulk, const __grid_constant__ CUtensorMap map_RD) {
   if (!par->active) return;
   extern __shared__ float2 sm[];
   __shared__ __align__(8) uint64_t bar;
@@ -739,25 +879,38 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
   const size_t fs = (size_t)nx * nyh;
   const int ix0 = 2 * blockIdx.x;
   const bool has1 = ix0 + 1 < nx;
-  // staged rows ix0 (and ix0+1) of the old eta and X after the two sequences
-  double* s_eta = (double*)(sm + 2 * ny);
-  double* s_X = s_eta + 2 * ny;
+  // staging after the two sequences: the pair's two half spectra (tensor
+  // load), then rows ix0, ix0+1 of the old eta and X (bulk copies,
+  // overlapping the inverse FFT)
+  char* stage = stage_base(sm, 2u * ny * (uint32_t)sizeof(float2));
+  const double* s_eta = (const double*)stage;
+  const double* s_X = s_eta + 2 * ny;
   if (bulk) {
-    if (threadIdx.x == 0) mbar_init(&bar);
+    const int kb = nyh < 256 ? nyh : 256, nb = (nyh + kb - 1) / kb;
+    float2* st = (float2*)stage;
+    if (threadIdx.x == 0) {
+      mbar_init(&bar);
+      stage_load(st, &map_RD, ix0, 2, kb, nb, &bar);
+    }
+    __syncthreads();
+    bulk_wait(&bar, 0, ctl);
+    merge_stage(sm, ay, st, 0, 2, kb, nyh);
+    merge_stage(sm + ny, ay, st, 1, 2, kb, nyh);
     __syncthreads();
     if (threadIdx.x == 0) {
-      const uint32_t n = (has1 ? 2u : 1u) * (uint32_t)ny;
       const size_t i0 = (size_t)ix0 * ny;
-      mbar_expect_tx(&bar, n * 16u);
-      bulk_g2s(s_eta, eta_o + i0, n * 8u, &bar);
-      bulk_g2s(s_X, X_o + i0, n * 8u, &bar);
+      fence_async_smem();
+      mbar_expect_tx(&bar, 32u * (uint32_t)ny);
+      bulk_g2s((void*)s_eta, eta_o + i0, 16u * ny, &bar);
+      bulk_g2s((void*)s_X, X_o + i0, 16u * ny, &bar);
     }
+  } else {
+    merge_load(sm, ay, RD, ix0, has1, nx, nyh);
+    merge_load(sm + ny, ay, RD + fs, ix0, has1, nx, nyh);
+    __syncthreads();
   }
-  merge_load(sm, ay, RD, ix0, has1, nx, nyh);
-  merge_load(sm + ny, ay, RD + fs, ix0, has1, nx, nyh);
-  __syncthreads();
   fft_run<+1, PY>(2, ay);
-  if (bulk) bulk_wait(&bar, ctl);
+  if (bulk) bulk_wait(&bar, 1, ctl);
   const KksPar q = *par;
   float* gb_buf = q.gb == 0 ? g0 : (q.gb == 1 ? g1 : g2);
   const float* gm_buf = q.gm == 0 ? g0 : (q.gm == 1 ? g1 : g2);
@@ -868,8 +1021,17 @@ __global__ void __launch_bounds__(kExtrasThreads)
 // shared memory of each pass (bytes): its sequences, transformed in place,
 // and for rows_BC / rows_D the staged state rows of the pair
 inline size_t seq_smem(int n, int nseq) { return (size_t)nseq * n * sizeof(float2); }
-inline size_t rows_bc_smem(int ny) { return seq_smem(ny, 3) + (size_t)2 * ny * (8 + 4 + 4); }
-inline size_t rows_d_smem(int ny) { return seq_smem(ny, 2) + (size_t)2 * ny * (8 + 8); }
+// staging of a row pass: the larger of the pair's state rows (32 ny bytes)
+// and its F staged half spectra (boxes of 2 x kb x F 8-byte elements), plus
+// 128 bytes of alignment slack
+inline size_t row_stage_bytes(int ny, int F) {
+  const int nyh = ny / 2 + 1, kb = nyh < 256 ? nyh : 256, nb = (nyh + kb - 1) / kb;
+  const size_t spec = (size_t)nb * F * kb * 16, rows = (size_t)32 * ny;
+  return (spec > rows ? spec : rows) + 128;
+}
+inline size_t rows_a_smem(int ny) { return seq_smem(ny, 3) + row_stage_bytes(ny, 3); }
+inline size_t rows_bc_smem(int ny) { return seq_smem(ny, 3) + row_stage_bytes(ny, 3); }
+inline size_t rows_d_smem(int ny) { return seq_smem(ny, 2) + row_stage_bytes(ny, 2); }
 inline int col_blocks(int nyh) { return (nyh + kCols - 1) / kCols; }
 
 template <int PY>
@@ -882,17 +1044,18 @@ void launch_rows(const KksFftLaunch& L, int p, int stage, cudaStream_t s) {
   float2* RA = (float2*)L.RA;
   float2* RB = (float2*)L.RB;
   if (stage == 0) {
-    kf_rows_A<PY><<<npairs, kThreads, seq_smem(L.ny, 3), s>>>(dc, par, L.fc, (const double*)f.eta[p],
-                                                              (const double*)f.X[p], RA, f.partials);
+    kf_rows_A<PY><<<npairs, kThreads, rows_a_smem(L.ny), s>>>(dc, par, L.fc, (const double*)f.eta[p],
+                                                               (const double*)f.X[p], RA, f.partials, L.ctl,
+                                                               L.bulk_rows, L.map_RA3);
   } else if (stage == 1) {
     kf_rows_BC<PY><<<npairs, kThreads, rows_bc_smem(L.ny), s>>>(
         dc, par, L.fc, RB, RA, (const double*)f.eta[p], (const float*)f.X_al[p], (const float*)f.X_th[p],
-        (float*)f.g[0], (float*)f.g[1], (float*)f.g[2], f.partials, L.ctl, L.bulk_rows);
+        (float*)f.g[0], (float*)f.g[1], (float*)f.g[2], f.partials, L.ctl, L.bulk_rows, L.map_RB3, L.map_RA3);
   } else {
     kf_rows_D<PY><<<npairs, kThreads, rows_d_smem(L.ny), s>>>(
         dc, par, L.fc, RB, (const double*)f.eta[p], (const double*)f.X[p], (double*)f.eta[q], (double*)f.X[q],
         (float*)f.X_al[q], (float*)f.X_th[q], (const double*)f.eta_m, (const double*)f.X_m, (float*)f.mu,
-        (float*)f.g[0], (float*)f.g[1], (float*)f.g[2], f.partials, L.ctl, L.bulk_rows);
+        (float*)f.g[0], (float*)f.g[1], (float*)f.g[2], f.partials, L.ctl, L.bulk_rows, L.map_RB2);
   }
 }
 
@@ -921,7 +1084,7 @@ cudaError_t set_attr(K* kernel, size_t smem) {
 
 template <int PY>
 int set_row_attrs(int ny) {
-  cudaError_t e = set_attr(kf_rows_A<PY>, seq_smem(ny, 3));
+  cudaError_t e = set_attr(kf_rows_A<PY>, rows_a_smem(ny));
   if (e == cudaSuccess) e = set_attr(kf_rows_BC<PY>, rows_bc_smem(ny));
   if (e == cudaSuccess) e = set_attr(kf_rows_D<PY>, rows_d_smem(ny));
   return (int)e;

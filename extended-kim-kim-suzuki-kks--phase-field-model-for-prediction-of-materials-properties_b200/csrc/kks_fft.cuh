@@ -2,6 +2,7 @@
 // pipeline of the mixed path (kks_fft.cu).
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -49,7 +50,12 @@ struct KksFftLaunch {
   int nx, ny, nyh;
   int nbx;   // grid of the pointwise extras kernel
   int PX, PY;
-  int bulk_rows;  // 1: row passes stage their state rows with bulk copies (needs ny % 4 == 0)
+  int bulk_rows;  // 1: row passes move their spectra with tensor copies and stage their state
+                  // rows with bulk copies (needs nx % 2 == 0, ny % 4 == 0 and encoded maps)
+  // tensor maps (x: nx, ky: nyh, field: F; 8-byte elements; box {2, min(nyh, 256), F})
+  CUtensorMap map_RA3;  // RA (also RC), F = 3
+  CUtensorMap map_RB3;  // RB, F = 3
+  CUtensorMap map_RB2;  // RB as RD, F = 2
 };
 
 // Largest prime factors with a direct DFT stage; other sizes use cuFFT.
