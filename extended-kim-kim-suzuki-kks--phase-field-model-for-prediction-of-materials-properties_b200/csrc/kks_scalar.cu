@@ -1,14 +1,16 @@
 // kks_scalar.cu - the scalar part of an attempt, on the device.
 //
-// Two single-thread stages bracket the field kernels of every attempt:
+// Two small stages bracket the field kernels of every attempt:
 //
-//  * kks_prologue: temperature from the heat-treatment schedule, vacancy
+//  * kks_prologue (one warp: the table interpolations in parallel, the rest on
+//    one thread): temperature from the heat-treatment schedule, vacancy
 //    model, Si diffusivity, interface mobility, Allen-Cahn coefficient, table
 //    interpolation and the dimensionless parameter set
 //    (pf_kks/solver.py:179-240, pf_kks/kinetics.py:9-107, pf_kks/materials.py:57-59);
-//  * kks_decide: finishes the block reductions, forms the total energy and the
-//    energy residual, and takes the reject / accept / enlarge decision and the
-//    end-of-step bookkeeping (pf_kks/solver.py:270-404, pf_kks/residual.py:26-66).
+//  * kks_decide (one block finishes the block reductions, then one thread):
+//    forms the total energy and the energy residual, and takes the reject /
+//    accept / enlarge decision and the end-of-step bookkeeping
+//    (pf_kks/solver.py:270-404, pf_kks/residual.py:26-66).
 //
 // This file is compiled with -fmad=false: every scalar expression is evaluated
 // with the same operation order and roundings as the reference's float64
@@ -89,14 +91,24 @@ __device__ void push_record(KksCtl* ctl, kks_record* ring, long long cap, const 
 
 __global__ void kks_prologue(const KksConst* __restrict__ c, KksCtl* ctl, KksPar* par,
                              const uint8_t* __restrict__ step_flags, kks_record* ring, long long ring_cap) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  // one warp: lane 0 runs the scalar chain; the material tables are
+  // interpolated at T by one lane each (same expressions, same roundings)
+  __shared__ int s_go;
+  __shared__ double s_T, s_tab[KKS_NTAB];
   const kks_params& p = c->p;
-  if (ctl->status != KKS_STATUS_OK || ctl->istep >= ctl->target_step) {
-    par->active = 0;
-    return;
+  const int lane = threadIdx.x;
+  if (lane == 0) {
+    s_go = ctl->status == KKS_STATUS_OK && ctl->istep < ctl->target_step;
+    if (!s_go) par->active = 0;
+    else s_T = interp(ctl->t, p.sched_time, p.sched_temp, p.n_sched);
   }
+  __syncwarp();
+  if (!s_go) return;
+  if (lane < KKS_NTAB) s_tab[lane] = tab(p, lane, s_T);
+  __syncwarp();
+  if (lane != 0) return;
   const int istep = ctl->istep;
-  const double T = interp(ctl->t, p.sched_time, p.sched_temp, p.n_sched);
+  const double T = s_T;
   const int surface = step_flags[istep] & 1;
 
   double Xv = ctl->Xv;
@@ -123,17 +135,17 @@ __global__ void kks_prologue(const KksConst* __restrict__ c, KksCtl* ctl, KksPar
     ctl->Xv = Xv + dXv;
   }
 
-  const double A_alp = tab(p, KKS_TAB_A_ALP, T);
-  const double B_alp = tab(p, KKS_TAB_B_ALP, T);
-  const double C_alp = tab(p, KKS_TAB_C_ALP, T);
-  const double C44 = tab(p, KKS_TAB_C44, T);
-  const double A_thet = tab(p, KKS_TAB_A_THET, T);
-  const double B_thet = tab(p, KKS_TAB_B_THET, T);
-  const double C_thet = tab(p, KKS_TAB_C_THET, T);
-  const double sigma = tab(p, KKS_TAB_GAMMA, T);
-  const double Omega0 = tab(p, KKS_TAB_VM, T);
-  const double epsX = tab(p, KKS_TAB_EPSX, T);
-  const double X_Si_fcc = tab(p, KKS_TAB_X_SI_FCC, T);
+  const double A_alp = s_tab[KKS_TAB_A_ALP];
+  const double B_alp = s_tab[KKS_TAB_B_ALP];
+  const double C_alp = s_tab[KKS_TAB_C_ALP];
+  const double C44 = s_tab[KKS_TAB_C44];
+  const double A_thet = s_tab[KKS_TAB_A_THET];
+  const double B_thet = s_tab[KKS_TAB_B_THET];
+  const double C_thet = s_tab[KKS_TAB_C_THET];
+  const double sigma = s_tab[KKS_TAB_GAMMA];
+  const double Omega0 = s_tab[KKS_TAB_VM];
+  const double epsX = s_tab[KKS_TAB_EPSX];
+  const double X_Si_fcc = s_tab[KKS_TAB_X_SI_FCC];
 
   // pf_kks/kinetics.py:60-80
   const double kappa2 = 2 * p.lambd * sigma * 3 / p.alpha;
@@ -200,33 +212,30 @@ __global__ void kks_prologue(const KksConst* __restrict__ c, KksCtl* ctl, KksPar
   ctl->attempts += 1;
 }
 
-// Finish a sum over the partials of all blocks (fixed order, deterministic).
-__device__ double block_sum(double v) {
-  __shared__ double sh[32];
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  __syncthreads();
-  if (lane == 0) sh[wid] = v;
-  __syncthreads();
-  v = 0;
-  if (wid == 0) {
-    const int nw = (blockDim.x + 31) >> 5;
-    v = lane < nw ? sh[lane] : 0.0;
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-  }
-  return v;  // valid in thread 0
-}
+// The partial sums of all blocks are finished in a fixed order (deterministic).
+constexpr int kDecideWarps = 16;  // warps of the decide block (one row group each)
+static_assert(KKS_NPART == 32, "one lane per partial-sum slot");
 
-__global__ void kks_decide(const KksConst* __restrict__ c, KksCtl* ctl, const KksPar* __restrict__ par,
+__global__ void __launch_bounds__(32 * kDecideWarps) kks_decide(const KksConst* __restrict__ c, KksCtl* ctl, const KksPar* __restrict__ par,
                            const double* __restrict__ partials, int nblocks, kks_record* ring, long long ring_cap,
                            kks_step_row* rows, long long row_cap) {
   __shared__ double S[P_COUNT];
+  __shared__ double G[kDecideWarps][KKS_NPART + 1];
   if (!par->active) return;
-  for (int k = 0; k < P_COUNT; ++k) {
+  // warp w sums rows w, w + W, ...: lane k reads slot k, so a warp reads one
+  // whole row per load; the W row groups are then added in a fixed order
+  {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     double v = 0;
-    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) v += partials[(size_t)b * KKS_NPART + k];
-    v = block_sum(v);
-    if (threadIdx.x == 0) S[k] = v;
+    for (int b = w; b < nblocks; b += kDecideWarps) v += partials[(size_t)b * KKS_NPART + lane];
+    G[w][lane] = v;
+    __syncthreads();
+    if (threadIdx.x < P_COUNT) {
+      double t = 0;
+      for (int g = 0; g < kDecideWarps; ++g) t += G[g][threadIdx.x];
+      S[threadIdx.x] = t;
+    }
+    __syncthreads();
   }
   if (threadIdx.x != 0) return;
 
@@ -408,5 +417,5 @@ void kks_launch_prologue(const KksConst* c, KksCtl* ctl, KksPar* par, const uint
 
 void kks_launch_decide(const KksConst* c, KksCtl* ctl, const KksPar* par, const double* partials, int nblocks,
                        kks_record* ring, long long ring_cap, kks_step_row* rows, long long row_cap, cudaStream_t s) {
-  kks_decide<<<1, 256, 0, s>>>(c, ctl, par, partials, nblocks, ring, ring_cap, rows, row_cap);
+  kks_decide<<<1, 32 * kDecideWarps, 0, s>>>(c, ctl, par, partials, nblocks, ring, ring_cap, rows, row_cap);
 }
