@@ -337,6 +337,8 @@ static int setup_fused(kks_handle* h, const std::vector<double>& kx) {
   L.PY = fc.ay.P;
   // bulk copies of whole row pairs need 16-byte multiples for the f32 rows, the
   // tensor maps 16-byte strides (nx even; every pair then has both rows)
+  // column runs start at multiples of nx * 8 bytes: bulk copies need nx even
+  L.bulk_cols = c.nx % 2 == 0 ? 1 : 0;
   L.bulk_rows = 0;
   if (c.nx % 2 == 0 && c.ny % 4 == 0 && encode_spectrum_map(&L.map_RA3, RA, c.nx, c.nyh, 3) &&
       encode_spectrum_map(&L.map_RB3, RB, c.nx, c.nyh, 3) && encode_spectrum_map(&L.map_RB2, RB, c.nx, c.nyh, 2))

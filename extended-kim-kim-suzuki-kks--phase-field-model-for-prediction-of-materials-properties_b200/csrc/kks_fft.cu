@@ -598,9 +598,11 @@ template <int PX>
 __global__ void __launch_bounds__(kThreads, kMinBlocks)
     kf_cols_AB(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const KksFftConst* __restrict__ fc,
                const float2* __restrict__ RA, float2* __restrict__ SA, float2* __restrict__ RB,
-               const double* __restrict__ kys, double* __restrict__ partials) {
+               const double* __restrict__ kys, double* __restrict__ partials, KksCtl* ctl, int bulk) {
   if (!par->active) return;
   extern __shared__ float2 sm[];
+  __shared__ __align__(8) uint64_t bar;
+  bulk = bulk && (smem_u32(sm) & 15u) == 0;  // bulk destinations need 16-byte alignment
   const KksFftAxis& ax = fc->ax;
   const int nx = c->nx, ny = c->ny, nyh = c->nyh;
   const size_t fs = (size_t)nx * nyh;
@@ -610,8 +612,18 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
   const int nv = ncol * nx;
   const int src_field = g < 2 ? 0 : (g == 2 ? 2 : 1);
   const float2* col = RA + src_field * fs + (size_t)ky0 * nx;
-  for (int i = threadIdx.x; i < nv; i += kThreads) sm[i] = col[i];
-  __syncthreads();
+  if (bulk) {  // the block's columns are one contiguous run: one bulk copy
+    if (threadIdx.x == 0) {
+      mbar_init(&bar);
+      mbar_expect_tx(&bar, 8u * nv);
+      bulk_g2s(sm, col, 8u * nv, &bar);
+    }
+    __syncthreads();
+    bulk_wait(&bar, 0, ctl);
+  } else {
+    for (int i = threadIdx.x; i < nv; i += kThreads) sm[i] = col[i];
+    __syncthreads();
+  }
   fft_run<-1, PX>(ncol, ax);
   if (g == 3 || g == 0) {
     float2* dst = SA + (g == 3 ? fs : 0) + (size_t)ky0 * nx;
@@ -780,23 +792,42 @@ template <int PX>
 __global__ void __launch_bounds__(kThreads, kMinBlocks)
     kf_cols_CD_eta(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const KksFftConst* __restrict__ fc,
                    const float2* __restrict__ RC, const float2* __restrict__ SA, float2* __restrict__ RD,
-                   const double* __restrict__ kys) {
+                   const double* __restrict__ kys, KksCtl* ctl, int bulk) {
   if (!par->active) return;
   extern __shared__ float2 sm[];
+  __shared__ __align__(8) uint64_t bar;
+  bulk = bulk && (smem_u32(sm) & 15u) == 0;  // bulk destinations need 16-byte alignment
   const KksFftAxis& ax = fc->ax;
   const int nx = c->nx, nyh = c->nyh;
   const int ky0 = blockIdx.x * kCols;
   const int ncol = min(kCols, nyh - ky0);
   const int nv = ncol * nx;
   const float2* col = RC + (size_t)ky0 * nx;
-  for (int i = threadIdx.x; i < nv; i += kThreads) sm[i] = col[i];
-  __syncthreads();
+  // FT(eta) of the same columns, staged during the forward FFT
+  float2* s_sa = (float2*)stage_base(sm, (uint32_t)(kCols * nx * sizeof(float2)));
+  if (bulk) {
+    if (threadIdx.x == 0) {
+      mbar_init(&bar);
+      mbar_expect_tx(&bar, 8u * nv);
+      bulk_g2s(sm, col, 8u * nv, &bar);
+    }
+    __syncthreads();
+    bulk_wait(&bar, 0, ctl);
+    if (threadIdx.x == 0) {
+      mbar_expect_tx(&bar, 8u * nv);
+      bulk_g2s(s_sa, SA + (size_t)ky0 * nx, 8u * nv, &bar);
+    }
+  } else {
+    for (int i = threadIdx.x; i < nv; i += kThreads) sm[i] = col[i];
+    __syncthreads();
+  }
   fft_run<-1, PX>(ncol, ax);
+  if (bulk) bulk_wait(&bar, 1, ctl);
   const float inv_N = (float)c->inv_N;
   const float ac_mul = (float)par->ac_mul, ac_den = (float)par->ac_den;
   for (int cc = 0; cc < ncol; ++cc) {
     const float ky = (float)kys[ky0 + cc];
-    const float2* ecol = SA + (size_t)(ky0 + cc) * nx;
+    const float2* ecol = bulk ? s_sa + cc * nx : SA + (size_t)(ky0 + cc) * nx;
     float2* z = sm + cc * nx;
     for (int p = threadIdx.x; p < nx; p += kThreads) {
       const float kx = __ldg(fc->kx_slot + p);
@@ -818,30 +849,50 @@ template <int PX>
 __global__ void __launch_bounds__(kThreads, kMinBlocks)
     kf_cols_CD_X(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const KksFftConst* __restrict__ fc,
                  const float2* __restrict__ RC, const float2* __restrict__ SA, float2* __restrict__ RD,
-                 const double* __restrict__ kys) {
+                 const double* __restrict__ kys, KksCtl* ctl, int bulk) {
   if (!par->active) return;
   extern __shared__ float2 sm[];
+  __shared__ __align__(8) uint64_t bar;
+  bulk = bulk && (smem_u32(sm) & 15u) == 0;  // bulk destinations need 16-byte alignment
   const KksFftAxis& ax = fc->ax;
   const int nx = c->nx, nyh = c->nyh;
   const size_t fs = (size_t)nx * nyh;
   const int ky0 = blockIdx.x * kCols;
   const int ncol = min(kCols, nyh - ky0);
   const int nv = ncol * nx;
-  // flux_x columns at [0, nv), flux_y columns at [nv, 2 nv)
+  // flux_x columns at [0, nv), flux_y columns at [nv, 2 nv); FT(X) of the same
+  // columns staged during the forward FFT
   const float2* cx = RC + fs + (size_t)ky0 * nx;
   const float2* cy = RC + 2 * fs + (size_t)ky0 * nx;
-  for (int i = threadIdx.x; i < nv; i += kThreads) {
-    sm[i] = cx[i];
-    sm[nv + i] = cy[i];
+  float2* s_sa = (float2*)stage_base(sm, (uint32_t)(2 * kCols * nx * sizeof(float2)));
+  if (bulk) {
+    if (threadIdx.x == 0) {
+      mbar_init(&bar);
+      mbar_expect_tx(&bar, 16u * nv);
+      bulk_g2s(sm, cx, 8u * nv, &bar);
+      bulk_g2s(sm + nv, cy, 8u * nv, &bar);
+    }
+    __syncthreads();
+    bulk_wait(&bar, 0, ctl);
+    if (threadIdx.x == 0) {
+      mbar_expect_tx(&bar, 8u * nv);
+      bulk_g2s(s_sa, SA + fs + (size_t)ky0 * nx, 8u * nv, &bar);
+    }
+  } else {
+    for (int i = threadIdx.x; i < nv; i += kThreads) {
+      sm[i] = cx[i];
+      sm[nv + i] = cy[i];
+    }
+    __syncthreads();
   }
-  __syncthreads();
   fft_run<-1, PX>(2 * ncol, ax);
+  if (bulk) bulk_wait(&bar, 1, ctl);
   const float inv_N = (float)c->inv_N;
   const float ch_mul = (float)par->ch_mul;
   const float dtD = (float)(par->dt * par->D_s);
   for (int cc = 0; cc < ncol; ++cc) {
     const float ky = (float)kys[ky0 + cc];
-    const float2* xcol = SA + fs + (size_t)(ky0 + cc) * nx;
+    const float2* xcol = bulk ? s_sa + cc * nx : SA + fs + (size_t)(ky0 + cc) * nx;
     float2* z = sm + cc * nx;
     const float2* zy = sm + nv + cc * nx;
     for (int p = threadIdx.x; p < nx; p += kThreads) {
@@ -1032,6 +1083,8 @@ inline size_t row_stage_bytes(int ny, int F) {
 inline size_t rows_a_smem(int ny) { return seq_smem(ny, 3) + row_stage_bytes(ny, 3); }
 inline size_t rows_bc_smem(int ny) { return seq_smem(ny, 3) + row_stage_bytes(ny, 3); }
 inline size_t rows_d_smem(int ny) { return seq_smem(ny, 2) + row_stage_bytes(ny, 2); }
+// column increment passes: m x kCols columns, and kCols staged SA columns
+inline size_t cols_cd_smem(int nx, int m) { return seq_smem(nx, m * kCols) + 128 + seq_smem(nx, kCols); }
 inline int col_blocks(int nyh) { return (nyh + kCols - 1) / kCols; }
 
 template <int PY>
@@ -1067,10 +1120,12 @@ void launch_cols(const KksFftLaunch& L, int stage, cudaStream_t s) {
   const int nb = col_blocks(L.nyh);
   if (stage == 0) {
     kf_cols_AB<PX><<<dim3(nb, 4), kThreads, seq_smem(L.nx, kCols), s>>>(L.dc, L.par, L.fc, RA, SA, RB, L.f->ky,
-                                                                         L.f->partials);
+                                                                         L.f->partials, L.ctl, L.bulk_cols);
   } else {
-    kf_cols_CD_eta<PX><<<nb, kThreads, seq_smem(L.nx, kCols), s>>>(L.dc, L.par, L.fc, RA, SA, RB, L.f->ky);
-    kf_cols_CD_X<PX><<<nb, kThreads, seq_smem(L.nx, 2 * kCols), s>>>(L.dc, L.par, L.fc, RA, SA, RB, L.f->ky);
+    kf_cols_CD_eta<PX><<<nb, kThreads, cols_cd_smem(L.nx, 1), s>>>(L.dc, L.par, L.fc, RA, SA, RB, L.f->ky, L.ctl,
+                                                                    L.bulk_cols);
+    kf_cols_CD_X<PX><<<nb, kThreads, cols_cd_smem(L.nx, 2), s>>>(L.dc, L.par, L.fc, RA, SA, RB, L.f->ky, L.ctl,
+                                                                  L.bulk_cols);
   }
 }
 
@@ -1093,8 +1148,8 @@ int set_row_attrs(int ny) {
 template <int PX>
 int set_col_attrs(int nx) {
   cudaError_t e = set_attr(kf_cols_AB<PX>, seq_smem(nx, kCols));
-  if (e == cudaSuccess) e = set_attr(kf_cols_CD_eta<PX>, seq_smem(nx, kCols));
-  if (e == cudaSuccess) e = set_attr(kf_cols_CD_X<PX>, seq_smem(nx, 2 * kCols));
+  if (e == cudaSuccess) e = set_attr(kf_cols_CD_eta<PX>, cols_cd_smem(nx, 1));
+  if (e == cudaSuccess) e = set_attr(kf_cols_CD_X<PX>, cols_cd_smem(nx, 2));
   return (int)e;
 }
 
@@ -1124,7 +1179,7 @@ void prime_table(std::vector<float2>& t) {
 
 size_t kks_fft_smem_bytes(int nx, int ny) {
   const size_t r = rows_bc_smem(ny) > rows_d_smem(ny) ? rows_bc_smem(ny) : rows_d_smem(ny);
-  const size_t c = seq_smem(nx, 2 * kCols);
+  const size_t c = cols_cd_smem(nx, 2);
   return (r > c ? r : c) + 1024;  // + the reduction scratch
 }
 

@@ -52,6 +52,7 @@ struct KksFftLaunch {
   int PX, PY;
   int bulk_rows;  // 1: row passes move their spectra with tensor copies and stage their state
                   // rows with bulk copies (needs nx % 2 == 0, ny % 4 == 0 and encoded maps)
+  int bulk_cols;  // 1: column passes load their columns with bulk copies (needs nx % 2 == 0)
   // tensor maps (x: nx, ky: nyh, field: F; 8-byte elements; box {2, min(nyh, 256), F})
   CUtensorMap map_RA3;  // RA (also RC), F = 3
   CUtensorMap map_RB3;  // RB, F = 3
