@@ -287,7 +287,6 @@ static int setup_fused(kks_handle* h, const std::vector<double>& kx) {
   int optin = 0;
   CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device));
   if (kks_fft_smem_bytes(c.nx, c.ny) > (size_t)optin) return KKS_OK;
-  if (kks_fft_upload_prime_tables() != 0) return set_error(KKS_ERR_CUDA, "fft prime tables");
   std::vector<float> kx_slot(c.nx);
   for (int k = 0; k < c.nx; ++k) kx_slot[tx.slot[k]] = (float)kx[k];
   // device tables and buffers in one allocation
@@ -296,8 +295,12 @@ static int setup_fused(kks_handle* h, const std::vector<double>& kx) {
   const size_t b_twx = al(tx.tw.size() * sizeof(float2)), b_twy = al(ty.tw.size() * sizeof(float2));
   const size_t b_slx = al(tx.slot.size() * sizeof(int)), b_sly = al(ty.slot.size() * sizeof(int));
   const size_t b_kxs = al(kx_slot.size() * sizeof(float));
+  // prime-stage factor tables of the two axes (at most 35 x 35 pairs each)
+  std::vector<float2> ptx(35 * 35), pty(35 * 35);
+  const int npx = kks_fft_prime_table(fc.ax.P, ptx.data()), npy = kks_fft_prime_table(fc.ay.P, pty.data());
+  const size_t b_ptx = al(std::max(npx, 1) * sizeof(float2)), b_pty = al(std::max(npy, 1) * sizeof(float2));
   const size_t b_spec = al(3 * fs) * 2 + al(2 * fs);
-  const size_t total = b_twx + b_twy + b_slx + b_sly + b_kxs + b_spec;
+  const size_t total = b_twx + b_twy + b_slx + b_sly + b_kxs + b_ptx + b_pty + b_spec;
   CK(cudaMalloc(&h->fft_arena, total));
   char* a = (char*)h->fft_arena;
   cudaError_t put_err = cudaSuccess;
@@ -313,6 +316,8 @@ static int setup_fused(kks_handle* h, const std::vector<double>& kx) {
   fc.ax.slot = (const int*)put(tx.slot.data(), tx.slot.size() * sizeof(int), b_slx);
   fc.ay.slot = (const int*)put(ty.slot.data(), ty.slot.size() * sizeof(int), b_sly);
   fc.kx_slot = (const float*)put(kx_slot.data(), kx_slot.size() * sizeof(float), b_kxs);
+  fc.ax.ptw = (const float2*)put(ptx.data(), std::max(npx, 1) * sizeof(float2), b_ptx);
+  fc.ay.ptw = (const float2*)put(pty.data(), std::max(npy, 1) * sizeof(float2), b_pty);
   CK(put_err);
   void* RA = a; a += al(3 * fs);
   void* RB = a; a += al(3 * fs);

@@ -188,7 +188,11 @@ __device__ __forceinline__ void bfly_small(float2* base, int q, int j, const flo
 // Prime stages. The H = (P-1)/2 output pairs (k, P-k) of a DFT are split into
 // NG groups of G; the table of prime P holds (cos, sin)(2 pi ((n k) mod P) / P)
 // at [(g H + n - 1) G + j] for output k = g G + j + 1 and input n = 1..H
-// (filled from the host in double precision, see kks_fft_upload_prime_tables).
+// (computed on the host in double precision, see kks_fft_prime_table). Every
+// pass kernel copies it into shared memory at entry: the warps of the five
+// groups read different parts of the 9.8 KB table for P = 71, more than the
+// constant cache holds, while a shared-memory read by a whole warp at one
+// address is a single broadcast.
 template <int P>
 struct PrimeShape {
   static constexpr int H = (P - 1) / 2;
@@ -198,15 +202,31 @@ struct PrimeShape {
   static_assert(NG <= kThreads / 32, "a round needs one warp per group");
 };
 
-__constant__ float2 kPrimeTw11[5 * 5];
-__constant__ float2 kPrimeTw19[9 * 9];
-__constant__ float2 kPrimeTw71[35 * 35];
+__shared__ float2 s_ptw11[5 * 5];
+__shared__ float2 s_ptw19[9 * 9];
+__shared__ float2 s_ptw71[35 * 35];
+
+template <int P>
+__device__ __forceinline__ float2* prime_tw_smem() {
+  if constexpr (P == 11) return s_ptw11;
+  else if constexpr (P == 19) return s_ptw19;
+  else return s_ptw71;
+}
 
 template <int P>
 __device__ __forceinline__ float2 prime_tw(int i) {
-  if constexpr (P == 11) return kPrimeTw11[i];
-  else if constexpr (P == 19) return kPrimeTw19[i];
-  else return kPrimeTw71[i];
+  return prime_tw_smem<P>()[i];
+}
+
+// Copy the axis's prime table into shared memory (before the kernel's first
+// barrier; nothing for axes without a prime stage).
+template <int P>
+__device__ __forceinline__ void prime_table_fill(const float2* __restrict__ src) {
+  if constexpr (P > 7) {
+    constexpr int H = (P - 1) / 2;
+    float2* dst = prime_tw_smem<P>();
+    for (int i = threadIdx.x; i < H * H; i += blockDim.x) dst[i] = src[i];
+  }
 }
 
 // The prime stage of nseq sequences of length n at the start of the block's
@@ -532,6 +552,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
               const double* __restrict__ eta, const double* __restrict__ X, float2* __restrict__ RA,
               double* __restrict__ partials, KksCtl* ctl, int bulk, const __grid_constant__ CUtensorMap map_RA) {
   if (!par->active) return;
+  prime_table_fill<PY>(fc->ay.ptw);
   extern __shared__ float2 sm[];
   __shared__ __align__(8) uint64_t bar;
   const KksFftAxis& ay = fc->ay;
@@ -600,6 +621,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
                const float2* __restrict__ RA, float2* __restrict__ SA, float2* __restrict__ RB,
                const double* __restrict__ kys, double* __restrict__ partials, KksCtl* ctl, int bulk) {
   if (!par->active) return;
+  prime_table_fill<PX>(fc->ax.ptw);
   extern __shared__ float2 sm[];
   __shared__ __align__(8) uint64_t bar;
   bulk = bulk && (smem_u32(sm) & 15u) == 0;  // bulk destinations need 16-byte alignment
@@ -692,6 +714,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
                double* __restrict__ partials, KksCtl* ctl, int bulk, const __grid_constant__ CUtensorMap map_RB,
                const __grid_constant__ CUtensorMap map_RC) {
   if (!par->active) return;
+  prime_table_fill<PY>(fc->ay.ptw);
   extern __shared__ float2 sm[];
   __shared__ __align__(8) uint64_t bar;
   const KksFftAxis& ay = fc->ay;
@@ -794,6 +817,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
                    const float2* __restrict__ RC, const float2* __restrict__ SA, float2* __restrict__ RD,
                    const double* __restrict__ kys, KksCtl* ctl, int bulk) {
   if (!par->active) return;
+  prime_table_fill<PX>(fc->ax.ptw);
   extern __shared__ float2 sm[];
   __shared__ __align__(8) uint64_t bar;
   bulk = bulk && (smem_u32(sm) & 15u) == 0;  // bulk destinations need 16-byte alignment
@@ -851,6 +875,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
                  const float2* __restrict__ RC, const float2* __restrict__ SA, float2* __restrict__ RD,
                  const double* __restrict__ kys, KksCtl* ctl, int bulk) {
   if (!par->active) return;
+  prime_table_fill<PX>(fc->ax.ptw);
   extern __shared__ float2 sm[];
   __shared__ __align__(8) uint64_t bar;
   bulk = bulk && (smem_u32(sm) & 15u) == 0;  // bulk destinations need 16-byte alignment
@@ -923,6 +948,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
               float* __restrict__ mu, float* g0, float* g1, float* g2, double* __restrict__ partials, KksCtl* ctl,
               int bulk, const __grid_constant__ CUtensorMap map_RD) {
   if (!par->active) return;
+  prime_table_fill<PY>(fc->ay.ptw);
   extern __shared__ float2 sm[];
   __shared__ __align__(8) uint64_t bar;
   const KksFftAxis& ay = fc->ay;
@@ -1163,9 +1189,8 @@ int set_col_attrs(int nx) {
   }
 
 template <int P>
-void prime_table(std::vector<float2>& t) {
+int prime_table(float2* t) {
   using S = PrimeShape<P>;
-  t.assign(S::H * S::H, make_float2(0.f, 0.f));
   for (int g = 0; g < S::NG; ++g)
     for (int n = 1; n <= S::H; ++n)
       for (int j = 0; j < S::G; ++j) {
@@ -1173,6 +1198,7 @@ void prime_table(std::vector<float2>& t) {
         const double th = 2.0 * M_PI * (double)((n * k) % P) / (double)P;
         t[(g * S::H + n - 1) * S::G + j] = make_float2((float)cos(th), (float)sin(th));
       }
+  return S::H * S::H;
 }
 
 }  // namespace
@@ -1180,7 +1206,7 @@ void prime_table(std::vector<float2>& t) {
 size_t kks_fft_smem_bytes(int nx, int ny) {
   const size_t r = rows_bc_smem(ny) > rows_d_smem(ny) ? rows_bc_smem(ny) : rows_d_smem(ny);
   const size_t c = cols_cd_smem(nx, 2);
-  return (r > c ? r : c) + 1024;  // + the reduction scratch
+  return (r > c ? r : c) + 1024 + 35 * 35 * sizeof(float2);  // + reduction scratch and prime table
 }
 
 int kks_fft_row_blocks(int nx) { return (nx + 1) / 2; }
@@ -1204,19 +1230,13 @@ int kks_fft_set_attributes(const KksFftLaunch& L) {
   return rc != 0 ? rc : rc2;
 }
 
-int kks_fft_upload_prime_tables() {
-  std::vector<float2> t;
-  prime_table<11>(t);
-  cudaError_t e = cudaMemcpyToSymbol(kPrimeTw11, t.data(), t.size() * sizeof(float2));
-  if (e == cudaSuccess) {
-    prime_table<19>(t);
-    e = cudaMemcpyToSymbol(kPrimeTw19, t.data(), t.size() * sizeof(float2));
+int kks_fft_prime_table(int P, float2* out) {
+  switch (P) {
+    case 11: return prime_table<11>(out);
+    case 19: return prime_table<19>(out);
+    case 71: return prime_table<71>(out);
+    default: return 0;
   }
-  if (e == cudaSuccess) {
-    prime_table<71>(t);
-    e = cudaMemcpyToSymbol(kPrimeTw71, t.data(), t.size() * sizeof(float2));
-  }
-  return (int)e;
 }
 
 void kks_fft_launch_attempt(const KksFftLaunch& L, int p, cudaStream_t s) {
