@@ -150,3 +150,17 @@ def test_make_params_scaling():
 def test_golden_logs_present():
     with open(os.path.join(GOLDEN, "reference_small_logs.json")) as f:
         assert set(json.load(f)) == {"fixed40", "accepted30", "enlarged40", "rejected40"}
+
+
+def test_accuracy_history_deviation_skips_shared_nans():
+    from pf_kks_gpu.accuracy import history_deviation
+
+    ref = np.array([1.0, 2.0, np.nan, 4.0])
+    test = np.array([1.0, 2.5, np.nan, 4.0])
+    d = history_deviation(test, ref)
+    assert d["nan_mismatch"] == 0
+    assert d["max_abs_dev"] == pytest.approx(0.5)
+    assert d["max_dev_over_range"] == pytest.approx(0.5 / 3.0)
+    d2 = history_deviation(np.array([1.0, np.nan, 3.0]), np.array([1.0, 2.0, 3.0]))
+    assert d2["nan_mismatch"] == 1 and d2["max_abs_dev"] == 0.0
+    assert "shape_test" in history_deviation(np.zeros(2), np.zeros(3))
