@@ -38,7 +38,8 @@
 // s_n = x_n + x_{P-n}, d_n = x_n - x_{P-n} and forms each output pair (k, P-k)
 // from H = (P-1)/2 real-by-complex products on s and d. It runs as warp tasks:
 // the lanes of a warp take 32 DFTs and one group of G output pairs, the warp's
-// cos / sin factors come from constant memory (uniform across the warp), and
+// cos / sin factors come from a table in shared memory (one broadcast read per
+// factor, uniform across the warp), and
 // the outputs wait in registers for a block barrier before they overwrite the
 // inputs, so the stage is in place and no thread holds the whole folded input.
 // Only the mixed path uses these kernels (FP32 transforms on the increments of
