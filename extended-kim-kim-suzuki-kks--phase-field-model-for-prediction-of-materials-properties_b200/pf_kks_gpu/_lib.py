@@ -17,6 +17,9 @@ KKS_STATUS_OK = 0
 KKS_STATUS_MAX_ITER = 1
 KKS_STATUS_NONFINITE = 2
 KKS_STATUS_TIMEOUT = 3
+KKS_COEF_COUNT = 15
+COEF_NAMES = ("dt", "L_s", "kappa2_s", "D_s", "w_s", "A_alp_s", "B_alp_s", "C_alp_s", "A_thet_s", "B_thet_s",
+              "C_thet_s", "epsX", "C44", "pc_shift", "pc_ratio")
 KKS_PRECISION_FP64 = 0
 KKS_PRECISION_MIXED = 1
 KKS_PRECISION_MIXED_CUFFT = 2
@@ -47,6 +50,7 @@ EXPORTS = (
     "kks_create", "kks_upload", "kks_run", "kks_drain", "kks_get_state", "kks_download", "kks_elastic_fields",
     "kks_checkpoint", "kks_restore", "kks_timing", "kks_destroy", "kks_last_error", "kks_version",
     "kks_state_sums_noalloc", "kks_run_many", "kks_pipeline",
+    "kks_adj_create", "kks_adj_forward", "kks_adj_backward", "kks_adj_destroy",
 )
 
 
@@ -126,6 +130,13 @@ def load(path=LIB_PATH):
     lib.kks_restore.argtypes = [vp, vp, ctypes.c_size_t]
     lib.kks_timing.argtypes = [vp, dp, P(ctypes.c_int64)]
     lib.kks_pipeline.argtypes = [vp, P(ctypes.c_int32), P(ctypes.c_int32)]
+    lib.kks_adj_create.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_double,
+                                   ctypes.c_double, ctypes.c_int, P(vp)]
+    lib.kks_adj_forward.argtypes = [vp, vp, dp, vp]
+    lib.kks_adj_backward.argtypes = [vp, vp, vp, dp, vp, vp, dp]
+    lib.kks_adj_destroy.argtypes = [vp]
+    for name in ("kks_adj_create", "kks_adj_forward", "kks_adj_backward", "kks_adj_destroy"):
+        getattr(lib, name).restype = ctypes.c_int
     lib.kks_destroy.argtypes = [vp]
     lib.kks_run_many.argtypes = [P(vp), ctypes.c_int32, P(ctypes.c_int32), P(ctypes.c_int32)]
     lib.kks_run_many.restype = ctypes.c_int

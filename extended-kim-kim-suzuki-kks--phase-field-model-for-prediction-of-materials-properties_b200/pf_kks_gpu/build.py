@@ -31,6 +31,7 @@ SOURCES = {
     "kks_abi.cu": [],
     "kks_fft.cu": [],
     "kks_noalloc.cu": [],
+    "kks_adjoint.cu": [],
 }
 
 

@@ -196,6 +196,36 @@ int kks_destroy(kks_handle* h);
 #define KKS_NOALLOC_MAX_POINTS (1 << 26)
 int kks_state_sums_noalloc(const double* eta, const double* X, int32_t nx, int32_t ny, double* out, void* stream);
 
+/* Fixed-dt step with explicit coefficients, and its adjoint. No counterpart in
+ * the reference: they make the step differentiable (gradients of history
+ * functionals such as a simulated DSC with respect to the kinetic parameters).
+ * A fixed-dt step is the unarmed branch of the attempt loop
+ * (pf_kks/solver.py:176-290 with flag == 0), all in FP64, with the per-step
+ * coefficients given by the caller instead of the prologue:
+ * coef[KKS_COEF_COUNT] = { dtime_s, L_s, kappa2_s, D_s, w_s, A_alp_s, B_alp_s,
+ * C_alp_s, A_thet_s, B_thet_s, C_thet_s, epsX, C44(T), (B_alp - B_thet) /
+ * (2 A_thet), A_alp / A_thet } (pf_kks/kinetics.py:83-107,
+ * pf_kks/free_energy.py:74-95). State buffers are device float64 arrays of
+ * 4*nx*ny: eta | X | X_al | X_th, each C-order (nx, ny). The stiffness is
+ * frozen at C11_0, C12_0, C44_0 (pf_kks/solver.py:152-154). Calls run on the
+ * handle's own stream and return after it has finished. */
+enum {
+  KKS_COEF_DT = 0, KKS_COEF_LS, KKS_COEF_KAPPA2, KKS_COEF_DS, KKS_COEF_W, KKS_COEF_A_ALP, KKS_COEF_B_ALP,
+  KKS_COEF_C_ALP, KKS_COEF_A_THET, KKS_COEF_B_THET, KKS_COEF_C_THET, KKS_COEF_EPSX, KKS_COEF_C44,
+  KKS_COEF_PC_SHIFT, KKS_COEF_PC_RATIO, KKS_COEF_COUNT
+};
+typedef struct kks_adj kks_adj;
+int kks_adj_create(int32_t nx, int32_t ny, double C11_0, double C12_0, double C44_0, int device, kks_adj** out);
+/* state_out = step(state_in; coef). */
+int kks_adj_forward(kks_adj* h, const double* state_in, const double* coef, double* state_out);
+/* Vector-Jacobian product of one step: given state_in, its step state_out and
+ * the cotangent lam_out of state_out, lam_in receives the cotangent of
+ * state_in and dcoef[KKS_COEF_COUNT] the gradient of <lam_out, state_out>
+ * with respect to coef (host array). */
+int kks_adj_backward(kks_adj* h, const double* state_in, const double* state_out, const double* coef,
+                     const double* lam_out, double* lam_in, double* dcoef);
+int kks_adj_destroy(kks_adj* h);
+
 /* Message of the last error of this thread. */
 const char* kks_last_error(void);
 

@@ -1,0 +1,132 @@
+"""GPU checks of the hand-written adjoint of the fixed-dt step
+(csrc/kks_adjoint.cu through the C ABI): the forward step against the torch
+restatement and against the main FP64 cell, the vector-Jacobian product
+against torch autograd, and the gradient of a history functional with
+respect to the kinetic calibration factors against central differences."""
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+from conftest import rel_l2  # noqa: E402
+from kks_torch_step import TorchStep  # noqa: E402
+from test_adjoint_cpu import fixed_dt_case  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+
+def _setup(nx=48, ny=40, n=6):
+    from pf_kks_gpu import adjoint as A
+
+    cfg, tables, state = fixed_dt_case(nx=nx, ny=ny, n=n)
+    stepper = A.StepAdjoint.for_config(cfg, tables, device=0)
+    T0 = float(np.interp(0.0, cfg.schedule_time, cfg.schedule_temperature))
+    tstep = TorchStep(cfg.nx, cfg.ny, tables.at(T0, "C11"), tables.at(T0, "C12"), tables.at(T0, "C44"), "cuda")
+    s0 = A.initial_state_tensor(*state, device=0)
+    return A, cfg, tables, state, stepper, tstep, s0
+
+
+def test_forward_step_matches_torch_step():
+    A, cfg, tables, state, stepper, tstep, s0 = _setup()
+    coef = A.coefficients(cfg, tables, 1)[0]
+    out = torch.empty_like(s0)
+    stepper.forward(s0, coef.numpy(), out)
+    ref = tstep(s0, coef.to("cuda"))
+    for k in range(4):
+        assert rel_l2(out[k].cpu().numpy(), ref[k].cpu().numpy()) <= 1e-12, k
+
+
+def test_vjp_matches_autograd():
+    A, cfg, tables, state, stepper, tstep, s0 = _setup()
+    coef = A.coefficients(cfg, tables, 1)[0].to("cuda")
+    gen = torch.Generator(device="cuda").manual_seed(7)
+    lam = torch.randn(s0.shape, generator=gen, dtype=torch.float64, device="cuda")
+    out = torch.empty_like(s0)
+    stepper.forward(s0, coef.cpu().numpy(), out)
+    lam_in = torch.empty_like(s0)
+    dcoef = stepper.backward(s0, out, coef.cpu().numpy(), lam.contiguous(), lam_in)
+    x = s0.clone().requires_grad_(True)
+    c = coef.clone().requires_grad_(True)
+    y = tstep(x, c)
+    gx, gc = torch.autograd.grad((y * lam).sum(), (x, c))
+    for k in range(4):
+        assert rel_l2(lam_in[k].cpu().numpy(), gx[k].cpu().numpy()) <= 1e-9, k
+    gc = gc.cpu().numpy()
+    for j in range(len(dcoef)):
+        scale = max(abs(gc[j]), 1e-300)
+        assert abs(dcoef[j] - gc[j]) <= 1e-8 * scale + 1e-12 * np.max(np.abs(gc)), (j, dcoef[j], gc[j])
+
+
+def _loss_fn(n, N):
+    gen = np.random.default_rng(11)
+    w = torch.tensor(gen.normal(size=n), dtype=torch.float64, device="cuda")
+    v = torch.tensor(gen.normal(size=n), dtype=torch.float64, device="cuda")
+
+    def loss(eta_mean, xal_mean, final):
+        # a smooth functional of the histories and the final state
+        return (w * eta_mean).sum() * 10 + (v * xal_mean).sum() * 100 + (final[0] ** 2).mean()
+
+    return loss
+
+
+def test_gradient_matches_finite_differences_and_torch_autograd():
+    n = 12
+    A, cfg, tables, state, stepper, tstep, s0 = _setup(n=n)
+    loss = _loss_fn(n, cfg.nx * cfg.ny)
+    run = A.FixedDtRun
+
+    def objective(lcD, lcM):
+        coef = A.coefficients(cfg, tables, n, lcD, lcM)
+        em, xm, fin = run.apply(coef, s0, stepper, 5)
+        return loss(em, xm, fin)
+
+    lcD = torch.zeros((), dtype=torch.float64, requires_grad=True)
+    lcM = torch.zeros((), dtype=torch.float64, requires_grad=True)
+    objective(lcD, lcM).backward()
+    g = np.array([float(lcD.grad), float(lcM.grad)])
+    # central differences of the GPU forward (h balances truncation, ~h^2, against the
+    # forward's round-off divided by h; the tight check is the autograd one below)
+    h = 1e-4
+    fd = []
+    for k in range(2):
+        vals = []
+        for sgn in (1, -1):
+            p = [torch.zeros((), dtype=torch.float64), torch.zeros((), dtype=torch.float64)]
+            p[k] = torch.tensor(sgn * h, dtype=torch.float64)
+            with torch.no_grad():
+                vals.append(float(objective(*p)))
+        fd.append((vals[0] - vals[1]) / (2 * h))
+    fd = np.array(fd)
+    assert np.all(np.abs(g - fd) <= 1e-4 * np.abs(fd)), (g, fd)
+    # autograd through the pure-torch step on the GPU
+    lcD2 = torch.zeros((), dtype=torch.float64, requires_grad=True)
+    lcM2 = torch.zeros((), dtype=torch.float64, requires_grad=True)
+    coef = A.coefficients(cfg, tables, n, lcD2, lcM2).to("cuda")
+    s = s0.clone()
+    ems, xms = [], []
+    for i in range(n):
+        mask = s[0] < 0.05
+        ems.append(s[0].mean())
+        xms.append((s[1] * mask).sum() / mask.sum())
+        s = tstep(s, coef[i])
+    loss(torch.stack(ems), torch.stack(xms), s).backward()
+    g2 = np.array([float(lcD2.grad), float(lcM2.grad)])
+    assert np.all(np.abs(g - g2) <= 1e-9 * np.abs(g2)), (g, g2)
+
+
+def test_forward_run_matches_main_fp64_cell():
+    from pf_kks_gpu import solver
+
+    n = 8
+    A, cfg, tables, state, stepper, tstep, s0 = _setup(n=n)
+    coef = A.coefficients(cfg, tables, n)
+    with torch.no_grad():
+        _, _, fin = A.FixedDtRun.apply(coef, s0, stepper, 3)
+    cell = solver.Cell(cfg, tables, precision="fp64", device=0)
+    cell.upload(*state)
+    cell.run(n)
+    ref = cell.download()
+    cell.close()
+    for k, r in enumerate(ref):
+        assert rel_l2(fin[k].cpu().numpy(), r.reshape(cfg.nx, cfg.ny)) <= 1e-10, k
