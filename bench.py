@@ -220,6 +220,53 @@ def ensemble_leg(precision, device, steps, warmup):
             "speedup": concurrent / sequential, "timing": "host wall clock around kks_run_many (one sync per batch)"}
 
 
+def adjoint_leg(device, steps=300, checkpoint_every=10):
+    """adjoint256: a fixed-dt FP64 run of 300 steps at 256^2 through the
+    coefficient chain and kks_adj_forward, then the gradient of a
+    finite-difference simulated DSC with respect to (c_D, c_Meta) through the
+    hand-written adjoint (checkpoint every 10 steps, segments recomputed)."""
+    import torch
+
+    from pf_kks_gpu import adjoint as A
+    from pf_kks_gpu import workloads
+    from pf_kks_gpu.materials import MaterialTables
+
+    class Enthalpy:  # smooth stand-ins for the CALPHAD enthalpies (J/mol)
+        def hm_fcc(self, T, x):
+            return -2000.0 + 5.0 * T + 3.0e4 * x
+
+        def hm_dia(self, T):
+            return 1.0e4 + 2.0 * T
+
+        def dhm_fcc_dx(self, T, x):
+            return 3.0e4 + 0 * T + 0 * x
+
+    cfg, spec = workloads.adjoint256(n_steps=steps)
+    tables = MaterialTables.from_npz(cfg.material_tables, cfg.c_gamma, cfg.c_eps0)
+    state = workloads.initial_state(cfg, spec)
+    stepper = A.StepAdjoint.for_config(cfg, tables, device=device)
+    s0 = A.initial_state_tensor(*state, device=device)
+    lcD = torch.zeros((), dtype=torch.float64, requires_grad=True)
+    lcM = torch.zeros((), dtype=torch.float64, requires_grad=True)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    coef, t, T = A.coefficients(cfg, tables, steps, lcD, lcM, return_times=True)
+    em, xm, fin = A.FixedDtRun.apply(coef, s0, stepper, checkpoint_every)
+    q = A.finite_difference_dsc(em, xm, t.to(em.device), T.to(em.device), Enthalpy(), 20 / 60)
+    loss = (q**2).sum()
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    loss.backward()
+    torch.cuda.synchronize()
+    t2 = time.perf_counter()
+    stepper.close()
+    return {"workload": "adjoint256: 256^2, 8 cells, 500->520 K, fixed dt, FP64", "steps": steps,
+            "checkpoint_every": checkpoint_every, "forward_s": t1 - t0, "backward_s": t2 - t1,
+            "forward_steps_per_s": steps / (t1 - t0), "gradient_steps_per_s": steps / (t2 - t1),
+            "grad_log_c_D": float(lcD.grad), "grad_log_c_Meta": float(lcM.grad),
+            "timing": "host wall clock, coefficient chain and histories included"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -229,6 +276,7 @@ def main():
     ap.add_argument("--precision", default="mixed", choices=("mixed", "mixed-cufft", "fp64"))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the 48-cell ensemble leg")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint (gradient) leg")
     ap.add_argument("--only-timed", action="store_true",
                     help="skip the FP64 comparison and end-to-end cells (profiling runs)")
     args = ap.parse_args()
@@ -394,6 +442,8 @@ def main():
     }
     if not args.no_ensemble and args.precision != "fp64":
         line["ensemble"] = ensemble_leg(args.precision, local_rank, steps=20, warmup=3)
+    if not args.no_adjoint and world == 1:
+        line["adjoint"] = adjoint_leg(local_rank)
     if not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline(state, cfg)
     print(json.dumps(line), flush=True)

@@ -63,12 +63,15 @@ def _interp(x, xp, fp):
     return slope * (x - xp[i]) + fp[i]
 
 
-def coefficients(cfg, tables, n_steps, log_c_D=None, log_c_Meta=None):
+def coefficients(cfg, tables, n_steps, log_c_D=None, log_c_Meta=None, return_times=False):
     """Per-step coefficients of a fixed-dt run, shape (n_steps, 15), float64,
     in the order of ``KKS_COEF_*`` (``include/kks.h``).
 
     ``log_c_D`` / ``log_c_Meta`` (0-d float64 tensors, default 0) multiply
     ``cfg.c_D`` / ``cfg.c_Meta`` by their exponential; gradients flow to them.
+    With ``return_times`` the result is (coef, time, T): the time [s] and
+    temperature [K] of each step's input state (the ``time`` / ``T``
+    histories), which also depend on the parameters through D(t = 0).
     """
     torch = _torch()
     f64 = torch.float64
@@ -98,10 +101,12 @@ def coefficients(cfg, tables, n_steps, log_c_D=None, log_c_Meta=None):
         dtime_s = dtime_s_min
     Xv = torch.tensor(float(quenched_vacancy_fraction(cfg.T_quench)), dtype=f64)
     t = zero
-    rows = []
+    rows, times, temps = [], [], []
     D_0 = None
     for n in range(n_steps):
         T = _interp(t, st, sT)
+        times.append(t)
+        temps.append(T)
         Xve = torch.exp(-(_HF1VA - T * _SF1VA) / (_R * T)) * (1 - _Z * 0.01 + _Z * 0.01 * torch.exp(
             (_HB - T * _SB_KB) / (_R * T)))
         factor = torch.abs(1 + (Xv - Xve) / Xve)
@@ -129,6 +134,8 @@ def coefficients(cfg, tables, n_steps, log_c_D=None, log_c_Meta=None):
             at["A_alp"] / s, at["B_alp"] / s, at["C_alp"] / s, at["A_thet"] / s, at["B_thet"] / s, at["C_thet"] / s,
             at["epsX"], C44, (at["B_alp"] - at["B_thet"]) / (2 * at["A_thet"]), at["A_alp"] / at["A_thet"]]))
         t = t + (dx**2 / D_0) * dtime_s
+    if return_times:
+        return torch.stack(rows), torch.stack(times), torch.stack(temps)
     return torch.stack(rows)
 
 
@@ -291,6 +298,37 @@ def __getattr__(name):
             _FN = _make_function()
         return _FN
     raise AttributeError(name)
+
+
+M_AL, M_SI = 26.98154, 28.0855  # molar masses [g/mol] (pf_kks/postprocess/dsc.py:24-25)
+
+
+def finite_difference_dsc(eta_mean, X_al_mean, time, T, enthalpy, heating_rate):
+    """Per-step simulated DSC signal from the histories, differentiable in them.
+
+    The precipitation / desaturation term of the reference's simulated DSC
+    (``pf_kks/postprocess/dsc.py:124-129``) with forward differences of the
+    histories in place of the derivatives of their smoothing splines, divided by
+    the heating rate [K/s] to give an apparent heat capacity [J/(g K)]:
+
+        f = eta_mean, x = X_al_mean (matrix Si), n = 0..len-2
+        q_n = (1 - f_n) dHfcc/dx(T_n, x_n) (x_{n+1} - x_n) / dt_n / M_AL
+              + (f_{n+1} - f_n) / dt_n (Hdia(T_n) / M_SI - Hfcc(T_n, x_n) / M_AL)
+
+    ``enthalpy`` supplies the molar enthalpies as torch functions
+    ``hm_fcc(T, x)``, ``hm_dia(T)`` and ``dhm_fcc_dx(T, x)`` [J/mol] (the
+    reference takes them from its CALPHAD description, ``pf_kks/thermo.py``).
+    ``time`` and ``T`` are the run's time [s] and temperature [K] histories.
+    """
+    torch = _torch()
+    f, x = eta_mean, X_al_mean
+    t = torch.as_tensor(time, dtype=f.dtype, device=f.device)
+    TT = torch.as_tensor(T, dtype=f.dtype, device=f.device)
+    dt = t[1:] - t[:-1]
+    Tn, xn, fn = TT[:-1], x[:-1], f[:-1]
+    q = ((1 - fn) * enthalpy.dhm_fcc_dx(Tn, xn) * (x[1:] - xn) / dt / M_AL
+         + (f[1:] - fn) / dt * (enthalpy.hm_dia(Tn) / M_SI - enthalpy.hm_fcc(Tn, xn) / M_AL))
+    return q / heating_rate
 
 
 def initial_state_tensor(eta, X, X_al, X_th, device=0):

@@ -20,7 +20,8 @@ ramp1420   1420^2, 40 cells, ~1200 particles R~U(3,10); 400->719 K at 20 K/min,
            adaptive, mixed precision
 ensemble   48 cells of side {128,192,256,384,512}, seeds 0-47, particles
            proportional to area, heating U(5,40) K/min from 400 to 600 K
-adjoint256 256^2, 8 cells; 500->520 K ramp, 300 fixed-dt steps
+adjoint256 256^2, 8 cells; 500->520 K ramp, 300 fixed-dt steps; c_D x 1.2, sink distance
+           x 1/sqrt(0.8), c_gamma x 1.1 (the gradient workload)
 =========  ==========================================================================
 """
 
@@ -111,8 +112,12 @@ def ensemble(n_instances=48, n_steps=1000, precision="mixed"):
 
 
 def adjoint256(n_steps=300, precision="fp64", seed=0):
+    """Fixed-dt run for gradients: the diffusivity (c_D x 1.2), sink distance
+    (x 1/sqrt(0.8)) and interface energy (c_gamma x 1.1) perturbed from the
+    demo parameters."""
     cfg = base_config(nx=256, ny=256, n_steps=n_steps, schedule_time=[0, 60.0], schedule_temperature=[500, 520],
-                      x_equilibrium=0.0, n_map_saves=2, n_surface_samples=n_steps)
+                      x_equilibrium=0.0, n_map_saves=2, n_surface_samples=n_steps, c_D=1.2,
+                      vacancy_sink_distance=250e-9 / 0.8**0.5, c_gamma=1.1)
     cfg.gpu = GpuOptions(precision=precision)
     spec = MicrostructureSpec(256, 256, n_cells=8, n_particles=102, r_min=3, r_max=8, seed=seed)
     return cfg, spec

@@ -60,3 +60,36 @@ def test_coefficients_are_differentiable():
     coef[:, 1].sum().backward()  # L_s depends on both D and Meta
     assert torch.isfinite(lcD.grad) and torch.isfinite(lcM.grad)
     assert float(lcM.grad) != 0.0
+
+
+class _ToyEnthalpy:
+    """Smooth stand-ins for the CALPHAD enthalpies (J/mol)."""
+
+    def hm_fcc(self, T, x):
+        return -2000.0 + 5.0 * T + 3.0e4 * x
+
+    def hm_dia(self, T):
+        return 1.0e4 + 2.0 * T
+
+    def dhm_fcc_dx(self, T, x):
+        return 3.0e4 + 0 * T + 0 * x
+
+
+def test_finite_difference_dsc_follows_the_histories():
+    cfg, tables, _ = fixed_dt_case(n=5)
+    coef, t, T = A.coefficients(cfg, tables, 5, return_times=True)
+    assert t[0] == 0 and torch.all(t[1:] > t[:-1])
+    assert float(T[-1]) == pytest.approx(float(np.interp(float(t[-1]), cfg.schedule_time, cfg.schedule_temperature)))
+    f = torch.tensor([0.10, 0.11, 0.13, 0.16, 0.17], dtype=torch.float64, requires_grad=True)
+    x = torch.tensor([0.020, 0.019, 0.017, 0.016, 0.0158], dtype=torch.float64, requires_grad=True)
+    q = A.finite_difference_dsc(f, x, t, T, _ToyEnthalpy(), heating_rate=20 / 60)
+    assert q.shape == (4,)
+    # by hand for the first interval
+    e = _ToyEnthalpy()
+    dt0 = float(t[1] - t[0])
+    T0 = float(T[0])
+    ref0 = ((1 - 0.10) * 3.0e4 * (0.019 - 0.020) / dt0 / A.M_AL
+            + (0.11 - 0.10) / dt0 * (e.hm_dia(T0) / A.M_SI - e.hm_fcc(T0, 0.020) / A.M_AL)) / (20 / 60)
+    assert float(q[0].detach()) == pytest.approx(ref0, rel=1e-12)
+    q.sum().backward()
+    assert torch.all(torch.isfinite(f.grad)) and torch.all(torch.isfinite(x.grad))
