@@ -189,11 +189,12 @@ def test_checkpoint_restore_is_exact(precision):
     b.close()
 
 
-@pytest.mark.parametrize("shape", [(160, 160), (45, 38), (33, 64), (64, 31), (40, 50)])
+@pytest.mark.parametrize("shape", [(160, 160), (45, 38), (33, 64), (64, 31), (40, 50), (100, 80)])
 def test_fused_fft_path_matches_oracle(tmp_path, shape):
     """The mixed step with the hand-written shared-memory FFTs (radices 2, 3,
     4, 5, 7 and the prime stages 11, 19, 71) against the FP64 oracle, and
-    against the same step with cuFFT transforms."""
+    against the same step with cuFFT transforms. (64 x 31 has a prime factor
+    without a direct stage and runs cuFFT.)"""
     from oracle import kks_oracle
     from pf_kks_gpu import workloads
     from pf_kks_gpu.generator import MicrostructureSpec
