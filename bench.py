@@ -220,6 +220,39 @@ def ensemble_leg(precision, device, steps, warmup):
             "speedup": concurrent / sequential, "timing": "host wall clock around kks_run_many (one sync per batch)"}
 
 
+def init_leg(precision, device):
+    """Initial state of the 1420^2 cell and of the 48-cell ensemble: the host
+    generator followed by kks_upload, against the device generator
+    (kks_voronoi_edges + kks_generate_fields, the same arrays)."""
+    from pf_kks_gpu import solver, workloads
+    from pf_kks_gpu.materials import MaterialTables
+
+    out = {}
+    for name, members in (("ramp1420", [workloads.ramp1420(n_steps=10, precision=precision)]),
+                          ("ensemble48", workloads.ensemble(48, 10, precision))):
+        cells = []
+        try:
+            for cfg, spec in members:
+                tables = MaterialTables.from_npz(cfg.material_tables, cfg.c_gamma, cfg.c_eps0)
+                cells.append((cfg, spec, solver.Cell(cfg, tables, precision=precision, device=device)))
+            workloads.initial_state_on_device(cells[0][2], cells[0][0], cells[0][1])  # first-call set-up
+            t0 = time.perf_counter()
+            for cfg, spec, cell in cells:
+                cell.upload(*workloads.initial_state(cfg, spec))
+            host = time.perf_counter() - t0
+            t0 = time.perf_counter()
+            for cfg, spec, cell in cells:
+                workloads.initial_state_on_device(cell, cfg, spec)
+            dev = time.perf_counter() - t0
+        finally:
+            for _, _, cell in cells:
+                cell.close()
+        out[name] = {"cells": len(members), "points": int(sum(c.nx * c.ny for c, _ in members)),
+                     "host_generate_and_upload_s": host, "device_generate_s": dev, "speedup": host / dev}
+    out["timing"] = "host wall clock; each call returns after its cell's stream is idle"
+    return out
+
+
 def adjoint_leg(device, steps=300, checkpoint_every=10):
     """adjoint256: a fixed-dt FP64 run of 300 steps at 256^2 through the
     coefficient chain and kks_adj_forward, then the gradient of a
@@ -277,6 +310,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the 48-cell ensemble leg")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint (gradient) leg")
+    ap.add_argument("--no-init", action="store_true", help="skip the initial-state (generator) leg")
     ap.add_argument("--only-timed", action="store_true",
                     help="skip the FP64 comparison and end-to-end cells (profiling runs)")
     args = ap.parse_args()
@@ -442,6 +476,8 @@ def main():
     }
     if not args.no_ensemble and args.precision != "fp64":
         line["ensemble"] = ensemble_leg(args.precision, local_rank, steps=20, warmup=3)
+    if not args.no_init and world == 1 and args.precision != "fp64":
+        line["init"] = init_leg(args.precision, local_rank)
     if not args.no_adjoint and world == 1:
         line["adjoint"] = adjoint_leg(local_rank)
     if not args.no_cpu_baseline and world == 1:

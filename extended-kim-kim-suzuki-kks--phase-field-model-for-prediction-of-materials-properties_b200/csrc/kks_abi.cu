@@ -92,6 +92,13 @@ struct kks_handle {
   KksFftLaunch fl{};
   double* partials_fused = nullptr;
   int nb_fused = 0;
+  // initial state on the device (kks_init.cu): chunk counts and offsets of the
+  // ordered selection, and a per-call buffer for particles and ranks
+  long long* sel = nullptr;
+  void* init_buf = nullptr;
+  size_t init_bytes = 0;
+  bool edges_ready = false;
+  long long n_edges = 0;
 };
 
 static size_t round_up(size_t v, size_t m) { return (v + m - 1) / m * m; }
@@ -428,6 +435,8 @@ static void free_handle(kks_handle* h) {
   cudaFree(h->d_kx);
   cudaFree(h->d_ky);
   cudaFree(h->d_xfer);
+  cudaFree(h->sel);
+  cudaFree(h->init_buf);
   if (h->h_ctl) cudaFreeHost(h->h_ctl);
   if (h->h_target) cudaFreeHost(h->h_target);
   if (h->ev0) cudaEventDestroy(h->ev0);
@@ -613,6 +622,8 @@ static int get_field(kks_handle* h, double* dst, const void* src, bool is_double
   return KKS_OK;
 }
 
+static int reset_loop(kks_handle* h);
+
 int kks_upload(kks_handle* h, const double* eta, const double* X, const double* X_al, const double* X_th) {
   if (!h || !eta || !X || !X_al || !X_th) return set_error(KKS_ERR_ARG, "null argument");
   CK(cudaSetDevice(h->device));
@@ -622,7 +633,11 @@ int kks_upload(kks_handle* h, const double* eta, const double* X, const double* 
   if ((rc = put_field(h, h->f.X[0], true, X)) != KKS_OK) return rc;
   if ((rc = put_field(h, h->f.X_al[0], d, X_al)) != KKS_OK) return rc;
   if ((rc = put_field(h, h->f.X_th[0], d, X_th)) != KKS_OK) return rc;
-  // initial loop state (pf_kks/solver.py:118-175)
+  return reset_loop(h);
+}
+
+// Initial loop state (pf_kks/solver.py:118-175) once state[0] holds the fields.
+static int reset_loop(kks_handle* h) {
   KksCtl* c = h->h_ctl;
   memset(c, 0, sizeof(KksCtl));
   c->iteration = 1;
@@ -818,6 +833,192 @@ int kks_download(kks_handle* h, double* eta, double* X, double* X_al, double* X_
   if (X && (rc = get_field(h, X, h->f.X[p], true)) != KKS_OK) return rc;
   if (X_al && (rc = get_field(h, X_al, h->f.X_al[p], d)) != KKS_OK) return rc;
   if (X_th && (rc = get_field(h, X_th, h->f.X_th[p], d)) != KKS_OK) return rc;
+  return KKS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Initial state on the device (kks_init.cu).
+
+static int ensure_sel(kks_handle* h) {
+  if (!h->sel) CK(cudaMalloc(&h->sel, (2 * (size_t)kks_init_chunks(h->hc.N) + 1) * sizeof(long long)));
+  return KKS_OK;
+}
+
+static int ensure_init_buf(kks_handle* h, size_t bytes) {
+  if (bytes <= h->init_bytes) return KKS_OK;
+  CK(cudaStreamSynchronize(h->stream));
+  cudaFree(h->init_buf);
+  h->init_buf = nullptr;
+  h->init_bytes = 0;
+  CK(cudaMalloc(&h->init_buf, bytes));
+  h->init_bytes = bytes;
+  return KKS_OK;
+}
+
+// chunk counts at sel[0..nc), offsets at sel[nc..2nc]
+static long long* sel_cnt(kks_handle* h) { return h->sel; }
+static long long* sel_off(kks_handle* h) { return h->sel + kks_init_chunks(h->hc.N); }
+
+static int sel_total(kks_handle* h, long long* total) {
+  CK(cudaMemcpyAsync(total, sel_off(h) + kks_init_chunks(h->hc.N), sizeof(long long), cudaMemcpyDeviceToHost,
+                     h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return KKS_OK;
+}
+
+static size_t align256(size_t v) { return (v + 255) / 256 * 256; }
+
+int kks_voronoi_edges(kks_handle* h, int32_t n_seeds, const double* seeds, int64_t* n_edges) {
+  if (!h || !seeds || !n_edges) return set_error(KKS_ERR_ARG, "null argument");
+  if (n_seeds < 1) return set_error(KKS_ERR_ARG, "kks_voronoi_edges: n_seeds < 1");
+  CK(cudaSetDevice(h->device));
+  int rc;
+  if ((rc = ensure_sel(h)) != KKS_OK) return rc;
+  if ((rc = ensure_init_buf(h, align256(2 * (size_t)n_seeds * sizeof(double)))) != KKS_OK) return rc;
+  h->edges_ready = false;
+  CK(cudaMemcpyAsync(h->init_buf, seeds, 2 * (size_t)n_seeds * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  // labels live in the parity-1 eta buffer until the first attempt overwrites it
+  int32_t* labels = (int32_t*)h->f.eta[1];
+  kks_init_labels((const double*)h->init_buf, n_seeds, h->hc.nx, h->hc.ny, labels, h->stream);
+  kks_init_count_edges(labels, h->hc.nx, h->hc.ny, sel_cnt(h), sel_off(h), h->stream);
+  CK(cudaGetLastError());
+  long long total = 0;
+  if ((rc = sel_total(h, &total)) != KKS_OK) return rc;
+  h->n_edges = total;
+  h->edges_ready = true;
+  *n_edges = total;
+  return KKS_OK;
+}
+
+int kks_generate_fields(kks_handle* h, const kks_gen_args* a) {
+  if (!h || !a) return set_error(KKS_ERR_ARG, "null argument");
+  const int n = a->n_particles;
+  if (n < 0 || (n > 0 && (!a->pick || !a->jitter || !a->radii)))
+    return set_error(KKS_ERR_ARG, "kks_generate_fields: bad particle arrays");
+  if (!(a->w > 0.0)) return set_error(KKS_ERR_ARG, "kks_generate_fields: w <= 0");
+  const long long range = a->picks_are_points ? (long long)h->hc.N : h->n_edges;
+  if (!a->picks_are_points && !h->edges_ready)
+    return set_error(KKS_ERR_STATE, "kks_generate_fields before kks_voronoi_edges");
+  // windows reach ceil(R + 8 w) + 1 cells: keep them within int range
+  if (!(a->w <= 1e6)) return set_error(KKS_ERR_ARG, "kks_generate_fields: w > 1e6");
+  for (int j = 0; j < n; ++j) {
+    if (a->pick[j] < 0 || a->pick[j] >= range) return set_error(KKS_ERR_ARG, "kks_generate_fields: pick out of range");
+    if (!(fabs(a->radii[j]) <= 1e6) || !(fabs(a->jitter[2 * j]) <= 1e6) || !(fabs(a->jitter[2 * j + 1]) <= 1e6))
+      return set_error(KKS_ERR_ARG, "kks_generate_fields: radius or jitter not finite or above 1e6 cells");
+  }
+  CK(cudaSetDevice(h->device));
+  const size_t ids = align256(n * sizeof(long long));
+  const size_t o_rank = 0, o_flat = ids, o_jit = 2 * ids, o_rad = o_jit + align256(2 * (size_t)n * sizeof(double)),
+               o_part = o_rad + align256(n * sizeof(double)),
+               total = o_part + align256(n * kks_init_particle_bytes()) + 256;
+  int rc;
+  if ((rc = ensure_init_buf(h, total)) != KKS_OK) return rc;
+  char* b = (char*)h->init_buf;
+  long long* ranks = (long long*)(b + o_rank);
+  long long* flat = (long long*)(b + o_flat);
+  double* jit = (double*)(b + o_jit);
+  double* rad = (double*)(b + o_rad);
+  if (n > 0) {
+    CK(cudaMemcpyAsync(ranks, a->pick, n * sizeof(long long), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(jit, a->jitter, 2 * (size_t)n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(rad, a->radii, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    if (a->picks_are_points) {
+      CK(cudaMemcpyAsync(flat, ranks, n * sizeof(long long), cudaMemcpyDeviceToDevice, h->stream));
+    } else {
+      kks_init_select_edges((const int32_t*)h->f.eta[1], h->hc.nx, h->hc.ny, sel_off(h), ranks, n, flat, h->stream);
+    }
+  }
+  double* eta = (double*)h->f.eta[0];
+  kks_init_eta(flat, n, h->hc.nx, h->hc.ny, jit, rad, a->w, b + o_part, eta, h->stream);
+  if (h->precision == KKS_PRECISION_FP64) {
+    kks_init_fields<double>(h->hc.N, a->rng_state, a->rng_inc, a->x_matrix, a->noise_low, a->noise_range,
+                            a->x_particle, a->pc_shift, a->pc_ratio, eta, (double*)h->f.X[0],
+                            (double*)h->f.X_al[0], (double*)h->f.X_th[0], h->stream);
+  } else {
+    kks_init_fields<float>(h->hc.N, a->rng_state, a->rng_inc, a->x_matrix, a->noise_low, a->noise_range,
+                           a->x_particle, a->pc_shift, a->pc_ratio, eta, (double*)h->f.X[0], (float*)h->f.X_al[0],
+                           (float*)h->f.X_th[0], h->stream);
+  }
+  CK(cudaGetLastError());
+  h->edges_ready = false;
+  return reset_loop(h);
+}
+
+static int place_impl(kks_handle* h, bool add, double dx, double dy, double x_matrix, double x_precipitate,
+                      int32_t n, const double* r, const double* ox, const double* oy, const double* oz) {
+  if (!h) return set_error(KKS_ERR_ARG, "null handle");
+  if (n < 0 || (n > 0 && (!r || !ox || !oy || !oz))) return set_error(KKS_ERR_ARG, "bad precipitate arrays");
+  if (add && !h->uploaded) return set_error(KKS_ERR_STATE, "kks_add_nuclei before the fields are set");
+  CK(cudaSetDevice(h->device));
+  int rc;
+  if ((rc = ensure_init_buf(h, align256(4 * (size_t)std::max(n, 1) * sizeof(double)))) != KKS_OK) return rc;
+  double* prm = (double*)h->init_buf;
+  const double* src[4] = {r, ox, oy, oz};
+  for (int c = 0; c < 4 && n > 0; ++c)
+    CK(cudaMemcpyAsync(prm + (size_t)c * n, src[c], n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  const int p = add ? h->parity : 0;
+  double* eta = (double*)h->f.eta[p];
+  double* X = (double*)h->f.X[p];
+  if (h->precision == KKS_PRECISION_FP64)
+    kks_init_place<double>(add, h->hc.nx, h->hc.ny, dx, dy, prm, n, x_matrix, x_precipitate, eta, X,
+                           (double*)h->f.X_al[p], (double*)h->f.X_th[p], h->stream);
+  else
+    kks_init_place<float>(add, h->hc.nx, h->hc.ny, dx, dy, prm, n, x_matrix, x_precipitate, eta, X,
+                          (float*)h->f.X_al[p], (float*)h->f.X_th[p], h->stream);
+  CK(cudaGetLastError());
+  if (!add) return reset_loop(h);
+  CK(cudaStreamSynchronize(h->stream));
+  return KKS_OK;
+}
+
+int kks_place_precipitates(kks_handle* h, double dx, double dy, double x_matrix, double x_precipitate, int32_t n,
+                           const double* r, const double* ox, const double* oy, const double* oz) {
+  return place_impl(h, false, dx, dy, x_matrix, x_precipitate, n, r, ox, oy, oz);
+}
+
+int kks_add_nuclei(kks_handle* h, double dx, double dy, int32_t n, const double* r, const double* ox,
+                   const double* oy, const double* oz) {
+  return place_impl(h, true, dx, dy, 0.0, 0.0, n, r, ox, oy, oz);
+}
+
+static int count_below(kks_handle* h, double eta_below, long long* count) {
+  int rc;
+  if ((rc = ensure_sel(h)) != KKS_OK) return rc;
+  kks_init_count_below((const double*)h->f.eta[h->parity], eta_below, h->hc.N, sel_cnt(h), sel_off(h), h->stream);
+  CK(cudaGetLastError());
+  return sel_total(h, count);
+}
+
+int kks_count_below(kks_handle* h, double eta_below, int64_t* count) {
+  if (!h || !count) return set_error(KKS_ERR_ARG, "null argument");
+  if (!h->uploaded) return set_error(KKS_ERR_STATE, "kks_count_below before the fields are set");
+  CK(cudaSetDevice(h->device));
+  long long c = 0;
+  int rc = count_below(h, eta_below, &c);
+  *count = c;
+  return rc;
+}
+
+int kks_insert_nuclei(kks_handle* h, double eta_below, int32_t n, const int64_t* ranks) {
+  if (!h || (n > 0 && !ranks)) return set_error(KKS_ERR_ARG, "null argument");
+  if (n < 0) return set_error(KKS_ERR_ARG, "kks_insert_nuclei: n < 0");
+  if (!h->uploaded) return set_error(KKS_ERR_STATE, "kks_insert_nuclei before the fields are set");
+  if (n == 0) return KKS_OK;
+  CK(cudaSetDevice(h->device));
+  long long c = 0;
+  int rc;
+  if ((rc = count_below(h, eta_below, &c)) != KKS_OK) return rc;
+  for (int j = 0; j < n; ++j)
+    if (ranks[j] < 0 || ranks[j] >= c) return set_error(KKS_ERR_ARG, "kks_insert_nuclei: rank out of range");
+  if ((rc = ensure_init_buf(h, 2 * align256(n * sizeof(long long)))) != KKS_OK) return rc;
+  long long* d_rank = (long long*)h->init_buf;
+  long long* d_flat = (long long*)((char*)h->init_buf + align256(n * sizeof(long long)));
+  CK(cudaMemcpyAsync(d_rank, ranks, n * sizeof(long long), cudaMemcpyHostToDevice, h->stream));
+  double* eta = (double*)h->f.eta[h->parity];
+  kks_init_select_below(eta, eta_below, h->hc.N, sel_off(h), d_rank, n, d_flat, h->stream);
+  kks_init_set_eta(d_flat, n, 1.0, eta, h->stream);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(h->stream));
   return KKS_OK;
 }
 

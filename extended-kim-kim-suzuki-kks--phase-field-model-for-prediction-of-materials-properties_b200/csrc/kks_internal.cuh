@@ -179,3 +179,26 @@ template <typename R>
 void kks_launch_to_real(const double* src, R* dst, int n, cudaStream_t s);
 template <typename R>
 void kks_launch_to_double(const R* src, double* dst, int n, cudaStream_t s);
+
+// Initial state on the device (kks_init.cu). Selection buffers: cnt holds
+// kks_init_chunks(N) counts, off kks_init_chunks(N) + 1 offsets (off[last] =
+// total). parts holds n * kks_init_particle_bytes().
+int kks_init_chunks(int N);
+size_t kks_init_particle_bytes();
+void kks_init_labels(const double* seeds, int ns, int nx, int ny, int32_t* labels, cudaStream_t s);
+void kks_init_count_edges(const int32_t* labels, int nx, int ny, long long* cnt, long long* off, cudaStream_t s);
+void kks_init_count_below(const double* eta, double thr, int N, long long* cnt, long long* off, cudaStream_t s);
+void kks_init_select_edges(const int32_t* labels, int nx, int ny, const long long* off, const long long* ranks,
+                           int n, long long* flat, cudaStream_t s);
+void kks_init_select_below(const double* eta, double thr, int N, const long long* off, const long long* ranks, int n,
+                           long long* flat, cudaStream_t s);
+void kks_init_eta(const long long* flat, int n, int nx, int ny, const double* jitter, const double* radii, double w,
+                  void* parts, double* eta, cudaStream_t s);
+template <typename R>
+void kks_init_fields(int N, const uint64_t state[2], const uint64_t inc[2], double x_matrix, double low, double range,
+                     double x_particle, double pc_shift, double pc_ratio, const double* eta, double* X, R* X_al,
+                     R* X_th, cudaStream_t s);
+template <typename R>
+void kks_init_place(bool add, int nx, int ny, double dx, double dy, const double* prm, int n, double x_matrix,
+                    double x_precipitate, double* eta, double* X, R* X_mat, R* X_pre, cudaStream_t s);
+void kks_init_set_eta(const long long* flat, int n, double value, double* eta, cudaStream_t s);

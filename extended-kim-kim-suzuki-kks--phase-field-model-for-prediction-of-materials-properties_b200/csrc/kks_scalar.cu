@@ -399,6 +399,8 @@ __global__ void __launch_bounds__(32 * kDecideWarps) kks_decide(const KksConst* 
   row.v[KKS_H_TTIME] = ctl->ttime;
   row.v[KKS_H_ISTEP] = (double)istep;
   row.v[KKS_H_SURF_VALID] = (double)(ctl->surf_b_valid + 2 * ctl->surf_valid);
+  row.v[KKS_H_D] = par->D;
+  row.v[KKS_H_XV] = ctl->Xv;
   rows[ctl->n_row % row_cap] = row;
   ctl->n_row += 1;
 

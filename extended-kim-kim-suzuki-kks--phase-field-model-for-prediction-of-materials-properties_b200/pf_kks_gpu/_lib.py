@@ -40,7 +40,7 @@ H = {
             "X_al_mean", "X_th_mean", "X_mean", "dX_al_mean", "dX_th_mean", "deta_mean", "dT", "eta_mean",
             "G_mean", "surf", "dsurf", "T", "dtime", "time", "time_s", "L", "energy_s", "dtime_s",
             "residual_total", "residual_energy_derivative", "residual_diffusion", "residual_allen_cahn",
-            "residual_temperature", "ttime", "istep", "surf_valid",
+            "residual_temperature", "ttime", "istep", "surf_valid", "D", "Xv",
         )
     )
 }
@@ -51,6 +51,8 @@ EXPORTS = (
     "kks_checkpoint", "kks_restore", "kks_timing", "kks_destroy", "kks_last_error", "kks_version",
     "kks_state_sums_noalloc", "kks_run_many", "kks_pipeline",
     "kks_adj_create", "kks_adj_forward", "kks_adj_backward", "kks_adj_destroy",
+    "kks_voronoi_edges", "kks_generate_fields", "kks_place_precipitates", "kks_add_nuclei", "kks_count_below",
+    "kks_insert_nuclei",
 )
 
 
@@ -100,6 +102,18 @@ class KksRunState(ctypes.Structure):
     ]
 
 
+class KksGenArgs(ctypes.Structure):
+    _fields_ = [
+        ("n_particles", ctypes.c_int32), ("picks_are_points", ctypes.c_int32),
+        ("pick", ctypes.POINTER(ctypes.c_int64)), ("jitter", ctypes.POINTER(ctypes.c_double)),
+        ("radii", ctypes.POINTER(ctypes.c_double)),
+        ("w", ctypes.c_double), ("x_matrix", ctypes.c_double), ("noise_low", ctypes.c_double),
+        ("noise_range", ctypes.c_double), ("x_particle", ctypes.c_double),
+        ("rng_state", ctypes.c_uint64 * 2), ("rng_inc", ctypes.c_uint64 * 2),
+        ("pc_shift", ctypes.c_double), ("pc_ratio", ctypes.c_double),
+    ]
+
+
 _lib = None
 
 
@@ -142,6 +156,17 @@ def load(path=LIB_PATH):
     lib.kks_run_many.restype = ctypes.c_int
     lib.kks_state_sums_noalloc.argtypes = [vp, vp, ctypes.c_int32, ctypes.c_int32, vp, vp]
     lib.kks_state_sums_noalloc.restype = ctypes.c_int
+    i64p = P(ctypes.c_int64)
+    lib.kks_voronoi_edges.argtypes = [vp, ctypes.c_int32, dp, i64p]
+    lib.kks_generate_fields.argtypes = [vp, P(KksGenArgs)]
+    lib.kks_place_precipitates.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                           ctypes.c_int32, dp, dp, dp, dp]
+    lib.kks_add_nuclei.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_int32, dp, dp, dp, dp]
+    lib.kks_count_below.argtypes = [vp, ctypes.c_double, i64p]
+    lib.kks_insert_nuclei.argtypes = [vp, ctypes.c_double, ctypes.c_int32, i64p]
+    for name in ("kks_voronoi_edges", "kks_generate_fields", "kks_place_precipitates", "kks_add_nuclei",
+                 "kks_count_below", "kks_insert_nuclei"):
+        getattr(lib, name).restype = ctypes.c_int
     lib.kks_last_error.restype = ctypes.c_char_p
     lib.kks_version.restype = ctypes.c_char_p
     for name in ("kks_create", "kks_upload", "kks_run", "kks_drain", "kks_get_state", "kks_download",

@@ -3,9 +3,9 @@
 Each CUDA source is compiled with ``nvcc -gencode arch=compute_100a,code=sm_100a``
 into an object file under ``csrc/_build/``, and the objects are linked into
 ``pf_kks_gpu/libkks_b200.so`` against cuFFT. ``kks_scalar.cu`` (the single-thread
-prologue / decide kernels) is compiled with ``-fmad=false`` so that its scalar
-arithmetic keeps the reference's float64 rounding; the field kernels keep FMA
-contraction.
+prologue / decide kernels) and ``kks_init.cu`` (initial state) are compiled
+with ``-fmad=false`` so that their arithmetic keeps numpy's float64 rounding;
+the field kernels keep FMA contraction.
 
 Usage: python -m pf_kks_gpu.build [--force] [--verbose]
 """
@@ -32,6 +32,7 @@ SOURCES = {
     "kks_fft.cu": [],
     "kks_noalloc.cu": [],
     "kks_adjoint.cu": [],
+    "kks_init.cu": ["-fmad=false"],
 }
 
 

@@ -90,6 +90,38 @@ def diffuse_eta(nx, ny, centres, radii, width_cells):
     return eta
 
 
+def _phase_constants(A_alp, B_alp, A_thet, B_thet):
+    return (B_alp - B_thet) / (2 * A_thet), A_alp / A_thet
+
+
+def generate_on_device(cell, spec, A_alp, B_alp, A_thet, B_thet):
+    """The state of :func:`generate`, written by the device into ``cell``
+    (a :class:`pf_kks_gpu.solver.Cell` of the spec's size).
+
+    The host draws what is per seed or per particle, in the same order and
+    from the same stream as :func:`generate`; labels, edge pixels, the
+    particles' profiles, the per-point matrix noise (the stream's next nx*ny
+    doubles, drawn on the device from the generator state after the radii) and
+    the phase compositions are computed on the device. Returns the number of
+    edge pixels.
+    """
+    if (cell.nx, cell.ny) != (spec.nx, spec.ny):
+        raise ValueError(f"cell is {cell.nx}x{cell.ny}, spec is {spec.nx}x{spec.ny}")
+    rng = np.random.Generator(np.random.PCG64(spec.seed))
+    nx, ny = spec.nx, spec.ny
+    seeds = rng.uniform(0.0, 1.0, size=(spec.n_cells, 2)) * np.array([nx, ny])
+    n_edges = cell.voronoi_edges(seeds)
+    pick = rng.integers(0, n_edges if n_edges else nx * ny, size=spec.n_particles)
+    jitter = rng.uniform(-0.5, 0.5, size=(spec.n_particles, 2))
+    radii = rng.uniform(spec.r_min, spec.r_max, size=spec.n_particles)
+    w = spec.width_cells / (2.0 * np.arctanh(0.9))
+    low, high = -spec.x_noise, spec.x_noise
+    pc_shift, pc_ratio = _phase_constants(A_alp, B_alp, A_thet, B_thet)
+    cell.generate_fields(pick, jitter, radii, w, spec.x_matrix, low, high - low, spec.x_particle,
+                         rng.bit_generator.state, pc_shift, pc_ratio, picks_are_points=(n_edges == 0))
+    return n_edges
+
+
 def generate(spec, A_alp, B_alp, A_thet, B_thet):
     """Initial (eta, X, X_al, X_th), each (nx, ny, 1) float64.
 

@@ -215,6 +215,71 @@ class Cell:
         L.check(self.lib.kks_pipeline(self.h, ctypes.byref(fused), ctypes.byref(kernels)), "kks_pipeline")
         return bool(fused.value), int(kernels.value)
 
+    # -- initial state written on the device (no nx*ny host arrays) ---------
+
+    def voronoi_edges(self, seeds):
+        """Periodic Voronoi labels of ``seeds`` ((n, 2), in cells) on the
+        device; returns the number of edge pixels."""
+        seeds = np.ascontiguousarray(seeds, dtype=np.float64).reshape(-1, 2)
+        n = ctypes.c_int64(0)
+        L.check(self.lib.kks_voronoi_edges(self.h, seeds.shape[0], L.dptr(seeds), ctypes.byref(n)),
+                "kks_voronoi_edges")
+        return int(n.value)
+
+    def generate_fields(self, pick, jitter, radii, w, x_matrix, noise_low, noise_range, x_particle, rng_state,
+                        pc_shift, pc_ratio, picks_are_points=False):
+        """Diffuse particles, noisy matrix and phase compositions into the
+        state; ``rng_state`` is numpy's PCG64 state dict before the noise."""
+        pick = np.ascontiguousarray(pick, dtype=np.int64)
+        jitter = np.ascontiguousarray(jitter, dtype=np.float64).reshape(-1, 2)
+        radii = np.ascontiguousarray(radii, dtype=np.float64)
+        a = L.KksGenArgs()
+        a.n_particles = pick.size
+        a.picks_are_points = int(bool(picks_are_points))
+        a.pick = pick.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))
+        a.jitter = L.dptr(jitter)
+        a.radii = L.dptr(radii)
+        a.w, a.x_matrix, a.noise_low, a.noise_range, a.x_particle = w, x_matrix, noise_low, noise_range, x_particle
+        st = rng_state["state"]
+        mask = (1 << 64) - 1
+        a.rng_state[0], a.rng_state[1] = st["state"] & mask, st["state"] >> 64
+        a.rng_inc[0], a.rng_inc[1] = st["inc"] & mask, st["inc"] >> 64
+        a.pc_shift, a.pc_ratio = pc_shift, pc_ratio
+        L.check(self.lib.kks_generate_fields(self.h, ctypes.byref(a)), "kks_generate_fields")
+
+    @staticmethod
+    def _circles(r, ox, oy, oz):
+        arrs = [np.ascontiguousarray(v, dtype=np.float64).ravel() for v in (r, ox, oy, oz)]
+        if len({a.size for a in arrs}) != 1:
+            raise ValueError("r, ox, oy, oz must have the same length")
+        return arrs
+
+    def place_precipitates(self, dx, dy, x_matrix, x_precipitate, r, ox, oy, oz):
+        """State = (eta, X, X_matrix, X_precipitate) of sharp circles
+        (pf_kks/microstructure.py:7-52) written on the device."""
+        arrs = self._circles(r, ox, oy, oz)
+        L.check(self.lib.kks_place_precipitates(self.h, dx, dy, x_matrix, x_precipitate, arrs[0].size,
+                                                *(L.dptr(a) for a in arrs)), "kks_place_precipitates")
+
+    def add_nuclei(self, dx, dy, r, ox, oy, oz):
+        """Nuclei into the current state, in place (pf_kks/microstructure.py:55-74)."""
+        arrs = self._circles(r, ox, oy, oz)
+        L.check(self.lib.kks_add_nuclei(self.h, dx, dy, arrs[0].size, *(L.dptr(a) for a in arrs)),
+                "kks_add_nuclei")
+
+    def count_below(self, eta_below):
+        """Number of points of the current state with eta < eta_below."""
+        n = ctypes.c_int64(0)
+        L.check(self.lib.kks_count_below(self.h, float(eta_below), ctypes.byref(n)), "kks_count_below")
+        return int(n.value)
+
+    def insert_nuclei(self, ranks, eta_below):
+        """eta = 1 at the ranks-th points (C order) with eta < eta_below."""
+        ranks = np.ascontiguousarray(np.atleast_1d(ranks), dtype=np.int64)
+        L.check(self.lib.kks_insert_nuclei(self.h, float(eta_below), ranks.size,
+                                           ranks.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))),
+                "kks_insert_nuclei")
+
     def close(self):
         if getattr(self, "h", None):
             self.lib.kks_destroy(self.h)

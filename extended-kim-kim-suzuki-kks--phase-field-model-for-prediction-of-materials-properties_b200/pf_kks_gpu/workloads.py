@@ -28,7 +28,7 @@ adjoint256 256^2, 8 cells; 500->520 K ramp, 300 fixed-dt steps; c_D x 1.2, sink 
 import numpy as np
 
 from .config import GpuOptions, SimulationConfig
-from .generator import MicrostructureSpec, generate
+from .generator import MicrostructureSpec, generate, generate_on_device
 from .materials import DEFAULT_TABLES, MaterialTables
 
 T_QUENCH_XV_1E4 = 816.3448
@@ -121,3 +121,10 @@ def adjoint256(n_steps=300, precision="fp64", seed=0):
     cfg.gpu = GpuOptions(precision=precision)
     spec = MicrostructureSpec(256, 256, n_cells=8, n_particles=102, r_min=3, r_max=8, seed=seed)
     return cfg, spec
+
+
+def initial_state_on_device(cell, cfg, spec):
+    """``initial_state`` written by the device straight into ``cell``."""
+    tables = MaterialTables.from_npz(cfg.material_tables, cfg.c_gamma, cfg.c_eps0)
+    T0 = np.interp(0, np.array(cfg.schedule_time), np.array(cfg.schedule_temperature))
+    return generate_on_device(cell, spec, *(tables.at(T0, n) for n in ("A_alp", "B_alp", "A_thet", "B_thet")))

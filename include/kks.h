@@ -101,7 +101,10 @@ enum {
   KKS_H_DT, KKS_H_ETA_MEAN, KKS_H_G_MEAN, KKS_H_SURF, KKS_H_DSURF, KKS_H_T, KKS_H_DTIME, KKS_H_TIME,
   KKS_H_TIME_S, KKS_H_L, KKS_H_ENERGY_S, KKS_H_DTIME_S, KKS_H_RES_TOTAL, KKS_H_RES_ENERGY_DERIVATIVE,
   KKS_H_RES_DIFFUSION, KKS_H_RES_ALLEN_CAHN, KKS_H_RES_TEMPERATURE, KKS_H_TTIME, KKS_H_ISTEP,
-  KKS_H_SURF_VALID, KKS_H_COUNT
+  KKS_H_SURF_VALID,
+  KKS_H_D,   /* Si diffusivity of the accepted attempt [m^2/s] (pf_kks/kinetics.py:24-37, solver.py:184) */
+  KKS_H_XV,  /* vacancy site fraction after the step (pf_kks/kinetics.py:52-60, solver.py:201) */
+  KKS_H_COUNT
 };
 typedef struct kks_step_row {
   double v[32];
@@ -225,6 +228,64 @@ int kks_adj_forward(kks_adj* h, const double* state_in, const double* coef, doub
 int kks_adj_backward(kks_adj* h, const double* state_in, const double* state_out, const double* coef,
                      const double* lam_out, double* lam_in, double* dcoef);
 int kks_adj_destroy(kks_adj* h);
+
+/* Initial state written on the device. No nx*ny host array crosses the ABI:
+ * the fields go straight into the cell's state, and the functions that set a
+ * whole state reset the loop state as kks_upload does.
+ *
+ * The seeded synthetic microstructure of the benchmark workloads (no
+ * counterpart in the reference, which places sharp circles read from a file,
+ * pf_kks/microstructure.py:7-52) is made in two calls around the host's draws
+ * from numpy.random.Generator(PCG64(seed)), which keep their order:
+ *   1. kks_voronoi_edges: seeds (host, n_seeds x {x, y} in cells, drawn
+ *      uniformly in the box) -> nearest-seed labels under the periodic metric
+ *      and *n_edges = the pixels whose right or lower periodic neighbour has
+ *      another label;
+ *   2. the host draws the particle picks (ranks among the edge pixels in C
+ *      order; flat point indices when n_edges == 0), jitters and radii, then
+ *      kks_generate_fields: eta = max over particles of
+ *      1/2 [1 - tanh((r - R)/w)] in a periodic window of reach ceil(R + 8w) + 1
+ *      around each centre, X = eta x_particle + (1 - eta)(x_matrix + low +
+ *      range u_i) with u_i the i-th double of the PCG64 stream from rng_state
+ *      (the 128-bit LCG jumped ahead on the device), and the KKS phase
+ *      compositions X_al = (X - h pc_shift) / ((1 - h) + h pc_ratio),
+ *      X_th = pc_ratio X_al + pc_shift, h = 3 eta^2 - 2 eta^3
+ *      (pf_kks/free_energy.py:74-95). */
+typedef struct kks_gen_args {
+  int32_t n_particles;
+  int32_t picks_are_points;  /* 1: pick[] are flat point indices, not edge-pixel ranks */
+  const int64_t* pick;       /* host, n_particles */
+  const double* jitter;      /* host, 2 per particle: x, y [cells] */
+  const double* radii;       /* host, n_particles [cells] */
+  double w;                  /* width of the tanh profile [cells] */
+  double x_matrix, noise_low, noise_range, x_particle;
+  uint64_t rng_state[2];     /* PCG64 LCG state before the matrix noise: {low 64 bits, high 64 bits} */
+  uint64_t rng_inc[2];       /* PCG64 increment: {low, high} */
+  double pc_shift;           /* (B_alp - B_thet) / (2 A_thet) at the initial temperature */
+  double pc_ratio;           /* A_alp / A_thet */
+} kks_gen_args;
+int kks_voronoi_edges(kks_handle* h, int32_t n_seeds, const double* seeds, int64_t* n_edges);
+int kks_generate_fields(kks_handle* h, const kks_gen_args* args);
+
+/* Sharp circular precipitates in a uniform matrix: the state becomes
+ * (eta, X, X_matrix, X_precipitate) of pf_kks/microstructure.py:7-52
+ * (`place_precipitates`, the CLI's initial state, pf_kks/cli.py:46-49), with
+ * nz = 1: a point at (i dx, j dy, 0) is inside when
+ * sqrt((ox-x)^2 + (oy-y)^2 + (oz-0)^2) <= r. r, ox, oy, oz: host float64[n] in
+ * metres. */
+int kks_place_precipitates(kks_handle* h, double dx, double dy, double x_matrix, double x_precipitate, int32_t n,
+                           const double* r, const double* ox, const double* oy, const double* oz);
+/* Nuclei into the current state, in place (pf_kks/microstructure.py:55-74,
+ * `add_nuclei`): inside points get eta = 1, X = X_th = 0.99999, X_al = 0. */
+int kks_add_nuclei(kks_handle* h, double dx, double dy, int32_t n, const double* r, const double* ox,
+                   const double* oy, const double* oz);
+/* Random nucleation on the current state (pf_kks/nucleation.py:103-111,
+ * `insert_random_nucleus`, with the candidates of the original put_nucle: the
+ * points with eta < eta_below, in C order). kks_count_below gives their number;
+ * kks_insert_nuclei sets eta = 1 at the ranks[j]-th candidate of each j (ranks
+ * taken before any of the n insertions; a rank out of range is KKS_ERR_ARG). */
+int kks_count_below(kks_handle* h, double eta_below, int64_t* count);
+int kks_insert_nuclei(kks_handle* h, double eta_below, int32_t n, const int64_t* ranks);
 
 /* Message of the last error of this thread. */
 const char* kks_last_error(void);

@@ -13,5 +13,7 @@ int main(void) {
   printf("kks_step_row %zu\n", sizeof(kks_step_row));
   printf("kks_run_state %zu %zu %zu\n", sizeof(kks_run_state), offsetof(kks_run_state, t),
          offsetof(kks_run_state, error_dtime_s));
+  printf("kks_gen_args %zu %zu %zu %zu\n", sizeof(kks_gen_args), offsetof(kks_gen_args, w),
+         offsetof(kks_gen_args, rng_state), offsetof(kks_gen_args, pc_ratio));
   return 0;
 }

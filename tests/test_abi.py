@@ -45,6 +45,8 @@ def test_ctypes_layout_matches_c(tmp_path):
     assert out["kks_step_row"] == [ctypes.sizeof(L.KksStepRow)]
     assert out["kks_run_state"] == [ctypes.sizeof(L.KksRunState), L.KksRunState.t.offset,
                                     L.KksRunState.error_dtime_s.offset]
+    assert out["kks_gen_args"] == [ctypes.sizeof(L.KksGenArgs), L.KksGenArgs.w.offset, L.KksGenArgs.rng_state.offset,
+                                   L.KksGenArgs.pc_ratio.offset]
 
 
 def _gpu_present():
