@@ -302,8 +302,8 @@ static int setup_fused(kks_handle* h, const std::vector<double>& kx) {
   const size_t b_twx = al(tx.tw.size() * sizeof(float2)), b_twy = al(ty.tw.size() * sizeof(float2));
   const size_t b_slx = al(tx.slot.size() * sizeof(int)), b_sly = al(ty.slot.size() * sizeof(int));
   const size_t b_kxs = al(kx_slot.size() * sizeof(float));
-  // prime-stage factor tables of the two axes (at most 35 x 35 pairs each)
-  std::vector<float2> ptx(35 * 35), pty(35 * 35);
+  // prime-stage factor tables of the two axes
+  std::vector<float2> ptx(KKS_FFT_PRIME_TABLE_MAX), pty(KKS_FFT_PRIME_TABLE_MAX);
   const int npx = kks_fft_prime_table(fc.ax.P, ptx.data()), npy = kks_fft_prime_table(fc.ay.P, pty.data());
   const size_t b_ptx = al(std::max(npx, 1) * sizeof(float2)), b_pty = al(std::max(npy, 1) * sizeof(float2));
   const size_t b_spec = al(3 * fs) * 2 + al(2 * fs);

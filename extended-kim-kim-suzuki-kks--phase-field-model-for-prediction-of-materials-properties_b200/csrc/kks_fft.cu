@@ -188,24 +188,31 @@ __device__ __forceinline__ void bfly_small(float2* base, int q, int j, const flo
 // ---------------------------------------------------------------------------
 // Prime stages. The H = (P-1)/2 output pairs (k, P-k) of a DFT are split into
 // NG groups of G; the table of prime P holds (cos, sin)(2 pi ((n k) mod P) / P)
-// at [(g H + n - 1) G + j] for output k = g G + j + 1 and input n = 1..H
-// (computed on the host in double precision, see kks_fft_prime_table). Every
-// pass kernel copies it into shared memory at entry: the warps of the five
-// groups read different parts of the 9.8 KB table for P = 71, more than the
-// constant cache holds, while a shared-memory read by a whole warp at one
+// at [(g H + n - 1) GP + j] for output k = g G + j + 1 and input n = 1..H, rows
+// padded to an even GP so that a warp reads two (cos, sin) pairs per 16-byte
+// load (computed on the host in double precision, see kks_fft_prime_table).
+// Every pass kernel copies it into shared memory at entry: the warps of the
+// five groups read different parts of the 11.2 KB table for P = 71, more than
+// the constant cache holds, while a shared-memory read by a whole warp at one
 // address is a single broadcast.
 template <int P>
 struct PrimeShape {
   static constexpr int H = (P - 1) / 2;
   static constexpr int G = P == 71 ? 7 : (P == 19 ? 3 : H);
   static constexpr int NG = H / G;
+  static constexpr int GP = (G + 1) & ~1;
+  static constexpr int TABLE = NG * H * GP;        // float2 entries
+  static constexpr int FOLD = (H + NG - 1) / NG;   // input pairs each group's warp folds
   static_assert(NG * G == H, "prime group size must divide (P-1)/2");
   static_assert(NG <= kThreads / 32, "a round needs one warp per group");
 };
+static_assert(PrimeShape<71>::TABLE <= KKS_FFT_PRIME_TABLE_MAX && PrimeShape<19>::TABLE <= KKS_FFT_PRIME_TABLE_MAX &&
+                  PrimeShape<11>::TABLE <= KKS_FFT_PRIME_TABLE_MAX,
+              "prime table size");
 
-__shared__ float2 s_ptw11[5 * 5];
-__shared__ float2 s_ptw19[9 * 9];
-__shared__ float2 s_ptw71[35 * 35];
+__shared__ __align__(16) float2 s_ptw11[PrimeShape<11>::TABLE];
+__shared__ __align__(16) float2 s_ptw19[PrimeShape<19>::TABLE];
+__shared__ __align__(16) float2 s_ptw71[PrimeShape<71>::TABLE];
 
 template <int P>
 __device__ __forceinline__ float2* prime_tw_smem() {
@@ -214,32 +221,30 @@ __device__ __forceinline__ float2* prime_tw_smem() {
   else return s_ptw71;
 }
 
-template <int P>
-__device__ __forceinline__ float2 prime_tw(int i) {
-  return prime_tw_smem<P>()[i];
-}
-
 // Copy the axis's prime table into shared memory (before the kernel's first
 // barrier; nothing for axes without a prime stage).
 template <int P>
 __device__ __forceinline__ void prime_table_fill(const float2* __restrict__ src) {
   if constexpr (P > 7) {
-    constexpr int H = (P - 1) / 2;
-    float2* dst = prime_tw_smem<P>();
-    for (int i = threadIdx.x; i < H * H; i += blockDim.x) dst[i] = src[i];
+    float4* dst = reinterpret_cast<float4*>(prime_tw_smem<P>());
+    const float4* s4 = reinterpret_cast<const float4*>(src);
+    for (int i = threadIdx.x; i < PrimeShape<P>::TABLE / 2; i += blockDim.x) dst[i] = __ldg(s4 + i);
   }
 }
 
 // The prime stage of nseq sequences of length n at the start of the block's
 // dynamic shared memory, in place. DFT d = (sequence d / per, block d % per)
 // covers d's P consecutive values. A warp takes 32 DFTs (one per lane) and one
-// group g of output pairs; with W warps a round covers W / NG lane groups. The
-// outputs stay in registers until every warp of the round has read its
-// inputs, then overwrite them.
+// group g of output pairs; with W warps a round covers W / NG lane groups.
+// First the input pairs are folded in place, x[n] <- x[n] + x[P-n] and
+// x[P-n] <- x[n] - x[P-n] (each group's warp folds FOLD of them), so that the
+// products read each folded value once per group; the outputs stay in
+// registers until every warp of the round has read its inputs, then
+// overwrite them.
 template <int P, int DIR>
 __device__ __forceinline__ void prime_stage(int nseq, int n, uint32_t pm) {
   using S = PrimeShape<P>;
-  constexpr int H = S::H, G = S::G, NG = S::NG;
+  constexpr int H = S::H, G = S::G, NG = S::NG, GP = S::GP;
   constexpr int W = kThreads / 32, R = W / NG;
   extern __shared__ float2 sm[];
   const int per = n / P;
@@ -252,10 +257,22 @@ __device__ __forceinline__ void prime_stage(int nseq, int n, uint32_t pm) {
     const int d = (lg << 5) + lane;
     const bool has = warp < R * NG && lg < LG && d < D;
     float2* x = sm;
-    float2 A[G], B[G], x0 = make_float2(0.f, 0.f), sum = make_float2(0.f, 0.f);
     if (has) {
       const int sq = per == 1 ? d : (int)__umulhi((uint32_t)d, pm);
       x = sm + sq * n + (d - sq * per) * P;
+#pragma unroll
+      for (int f = 0; f < S::FOLD; ++f) {
+        const int nn = g * S::FOLD + f + 1;
+        if (nn <= H) {
+          const float2 a = x[nn], c = x[P - nn];
+          x[nn] = cadd(a, c);
+          x[P - nn] = csub(a, c);
+        }
+      }
+    }
+    __syncthreads();
+    float2 A[G], B[G], x0 = make_float2(0.f, 0.f), sum = make_float2(0.f, 0.f);
+    if (has) {
       x0 = x[0];
       sum = x0;
 #pragma unroll
@@ -263,19 +280,24 @@ __device__ __forceinline__ void prime_stage(int nseq, int n, uint32_t pm) {
         A[j] = make_float2(0.f, 0.f);
         B[j] = make_float2(0.f, 0.f);
       }
-      const int tb = g * (H * G);
+      const float4* tw = reinterpret_cast<const float4*>(prime_tw_smem<P>() + g * (H * GP));
 #pragma unroll
       for (int nn = 1; nn <= H; ++nn) {
-        const float2 a = x[nn], c = x[P - nn];
-        const float2 s = cadd(a, c), dd = csub(a, c);
-        sum = cadd(sum, s);
+        const float2 s = x[nn], dd = x[P - nn];
+        if (g == 0) sum = cadd(sum, s);
 #pragma unroll
-        for (int j = 0; j < G; ++j) {
-          const float2 w = prime_tw<P>(tb + (nn - 1) * G + j);
-          A[j].x += s.x * w.x;
-          A[j].y += s.y * w.x;
-          B[j].x += dd.x * w.y;
-          B[j].y += dd.y * w.y;
+        for (int jj = 0; jj < GP / 2; ++jj) {
+          const float4 w = tw[(nn - 1) * (GP / 2) + jj];
+          A[2 * jj].x += s.x * w.x;
+          A[2 * jj].y += s.y * w.x;
+          B[2 * jj].x += dd.x * w.y;
+          B[2 * jj].y += dd.y * w.y;
+          if (2 * jj + 1 < G) {
+            A[2 * jj + 1].x += s.x * w.z;
+            A[2 * jj + 1].y += s.y * w.z;
+            B[2 * jj + 1].x += dd.x * w.w;
+            B[2 * jj + 1].y += dd.y * w.w;
+          }
         }
       }
     }
@@ -1192,14 +1214,15 @@ int set_col_attrs(int nx) {
 template <int P>
 int prime_table(float2* t) {
   using S = PrimeShape<P>;
+  for (int i = 0; i < S::TABLE; ++i) t[i] = make_float2(0.f, 0.f);
   for (int g = 0; g < S::NG; ++g)
     for (int n = 1; n <= S::H; ++n)
       for (int j = 0; j < S::G; ++j) {
         const int k = g * S::G + j + 1;
         const double th = 2.0 * M_PI * (double)((n * k) % P) / (double)P;
-        t[(g * S::H + n - 1) * S::G + j] = make_float2((float)cos(th), (float)sin(th));
+        t[(g * S::H + n - 1) * S::GP + j] = make_float2((float)cos(th), (float)sin(th));
       }
-  return S::H * S::H;
+  return S::TABLE;
 }
 
 }  // namespace
@@ -1207,7 +1230,7 @@ int prime_table(float2* t) {
 size_t kks_fft_smem_bytes(int nx, int ny) {
   const size_t r = rows_bc_smem(ny) > rows_d_smem(ny) ? rows_bc_smem(ny) : rows_d_smem(ny);
   const size_t c = cols_cd_smem(nx, 2);
-  return (r > c ? r : c) + 1024 + 35 * 35 * sizeof(float2);  // + reduction scratch and prime table
+  return (r > c ? r : c) + 1024 + KKS_FFT_PRIME_TABLE_MAX * sizeof(float2);  // + reduction scratch and prime table
 }
 
 int kks_fft_row_blocks(int nx) { return (nx + 1) / 2; }

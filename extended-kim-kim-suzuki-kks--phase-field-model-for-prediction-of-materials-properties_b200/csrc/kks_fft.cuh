@@ -27,7 +27,7 @@ struct KksFftAxis {
   uint32_t qm[KKS_FFT_MAXST], pm[KKS_FFT_MAXST];
   const float2* tw;
   const int* slot;
-  const float2* ptw;  // prime DFT factors, (P-1)^2/4 (cos, sin) pairs (see kks_fft_prime_table); null if P = 0
+  const float2* ptw;  // prime DFT factors, (cos, sin) pairs (see kks_fft_prime_table); null if P = 0
 };
 
 struct KksFftConst {
@@ -70,7 +70,9 @@ size_t kks_fft_smem_bytes(int nx, int ny);
 int kks_fft_row_blocks(int nx);
 int kks_fft_partial_rows(int nx, int ny, int nbx);
 int kks_fft_set_attributes(const KksFftLaunch& L);
-// The prime-stage factor table of prime P (11, 19 or 71): (P-1)^2/4 pairs
-// written to out; returns the count, or 0 for an unsupported P.
+// The prime-stage factor table of prime P (11, 19 or 71), rows padded to an
+// even length: at most KKS_FFT_PRIME_TABLE_MAX pairs written to out; returns
+// the count, or 0 for an unsupported P.
+#define KKS_FFT_PRIME_TABLE_MAX (5 * 35 * 8)
 int kks_fft_prime_table(int P, float2* out);
 void kks_fft_launch_attempt(const KksFftLaunch& L, int parity, cudaStream_t s);
