@@ -458,8 +458,8 @@ def main():
             "unit": "GB/s",
             "frac": achieved / peak,
             "traffic": traffic,
-            "kernel": ("one attempt (captured CUDA graph of 11 kernels: shared-memory FFT passes fused with the "
-                       "pointwise stages)") if fused else
+            "kernel": (f"one attempt (captured CUDA graph of {kernels_per_attempt} kernels: shared-memory FFT passes "
+                       "fused with the pointwise stages)") if fused else
                       "one attempt (captured CUDA graph: 8 own kernels + cuFFT R2C/C2R)",
             "algorithmic_bytes": alg_bytes,
             "peak_kind": peak_kind,

@@ -636,8 +636,8 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
 }
 
 // pass 2: kCols adjacent y-frequency columns of RA. blockIdx.y: 0 eta -> keep
-// FT(eta), i k_x FT(eta); 1 eta -> i k_y FT(eta); 2 eta^2 -> tr eps^
-// (+ Parseval sums); 3 X -> keep FT(X).
+// FT(eta), i k_x FT(eta) and i k_y FT(eta) (one forward, two inverse
+// transforms); 1 eta^2 -> tr eps^ (+ Parseval sums); 2 X -> keep FT(X).
 template <int PX>
 __global__ void __launch_bounds__(kThreads, kMinBlocks)
     kf_cols_AB(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const KksFftConst* __restrict__ fc,
@@ -655,7 +655,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
   const int ky0 = blockIdx.x * kCols;
   const int ncol = min(kCols, nyh - ky0);
   const int nv = ncol * nx;
-  const int src_field = g < 2 ? 0 : (g == 2 ? 2 : 1);
+  const int src_field = g == 0 ? 0 : (g == 1 ? 2 : 1);
   const float2* col = RA + src_field * fs + (size_t)ky0 * nx;
   if (bulk) {  // the block's columns are one contiguous run: one bulk copy
     if (threadIdx.x == 0) {
@@ -670,10 +670,10 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
     __syncthreads();
   }
   fft_run<-1, PX>(ncol, ax);
-  if (g == 3 || g == 0) {
-    float2* dst = SA + (g == 3 ? fs : 0) + (size_t)ky0 * nx;
+  if (g != 1) {
+    float2* dst = SA + (g == 2 ? fs : 0) + (size_t)ky0 * nx;
     for (int i = threadIdx.x; i < nv; i += kThreads) dst[i] = sm[i];
-    if (g == 3) return;
+    if (g == 2) return;
   }
   const float inv_N = (float)c->inv_N;
   const float a = (float)(par->epsX * c->c3) * inv_N;
@@ -686,11 +686,10 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
     float2* z = sm + cc * nx;
     for (int p = threadIdx.x; p < nx; p += kThreads) {
       const float kx = __ldg(fc->kx_slot + p);
-      float2 v = z[p];
+      const float2 v = z[p];
       if (g == 0) {
-        v = make_float2(-kx * inv_N * v.y, kx * inv_N * v.x);
-      } else if (g == 1) {
-        v = make_float2(-ky * inv_N * v.y, ky * inv_N * v.x);
+        z[p] = make_float2(-kx * inv_N * v.y, kx * inv_N * v.x);
+        z[nv + p] = make_float2(-ky * inv_N * v.y, ky * inv_N * v.x);
       } else {
         // strain multipliers of the 2x2 acoustic tensor (stiffness / C44(T0)), 0 at k = 0
         const float Kxx = c11 * kx * kx + ky * ky, Kyy = kx * kx + c11 * ky * ky, Kxy = (c12 + 1.f) * kx * ky;
@@ -713,17 +712,25 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
         acc[4] += pw * (dxx + dyy);
         acc[5] += pw;
         const float st = a * (oxx + oyy);
-        v = make_float2(st * v.x, st * v.y);
+        z[p] = make_float2(st * v.x, st * v.y);
       }
-      z[p] = v;
     }
   }
-  if (g == 2) block_reduce_store<6>(acc, partials + (size_t)blockIdx.x * KKS_NPART + P2_OXX2);
+  if (g == 1) block_reduce_store<6>(acc, partials + (size_t)blockIdx.x * KKS_NPART + P2_OXX2);
   __syncthreads();
-  fft_run<+1, PX>(ncol, ax);
-  const int dst_field = g == 2 ? 0 : (g == 0 ? 1 : 2);
-  float2* dst = RB + dst_field * fs + (size_t)ky0 * nx;
-  for (int i = threadIdx.x; i < nv; i += kThreads) dst[i] = sm[i];
+  // g = 0: the i k_x columns at [0, nv), the i k_y columns at [nv, 2 nv)
+  fft_run<+1, PX>(g == 0 ? 2 * ncol : ncol, ax);
+  if (g == 0) {
+    float2* dx = RB + fs + (size_t)ky0 * nx;
+    float2* dy = RB + 2 * fs + (size_t)ky0 * nx;
+    for (int i = threadIdx.x; i < nv; i += kThreads) {
+      dx[i] = sm[i];
+      dy[i] = sm[nv + i];
+    }
+  } else {
+    float2* dst = RB + (size_t)ky0 * nx;
+    for (int i = threadIdx.x; i < nv; i += kThreads) dst[i] = sm[i];
+  }
 }
 
 // pass 3: one row pair of RB (tr eps, d_x eta, d_y eta) -> inverse FFT ->
@@ -1168,8 +1175,8 @@ void launch_cols(const KksFftLaunch& L, int stage, cudaStream_t s) {
   float2* SA = (float2*)L.SA;
   const int nb = col_blocks(L.nyh);
   if (stage == 0) {
-    kf_cols_AB<PX><<<dim3(nb, 4), kThreads, seq_smem(L.nx, kCols), s>>>(L.dc, L.par, L.fc, RA, SA, RB, L.f->ky,
-                                                                         L.f->partials, L.ctl, L.bulk_cols);
+    kf_cols_AB<PX><<<dim3(nb, 3), kThreads, seq_smem(L.nx, 2 * kCols), s>>>(
+        L.dc, L.par, L.fc, RA, SA, RB, L.f->ky, L.f->partials, L.ctl, L.bulk_cols);
   } else {
     kf_cols_CD_eta<PX><<<nb, kThreads, cols_cd_smem(L.nx, 1), s>>>(L.dc, L.par, L.fc, RA, SA, RB, L.f->ky, L.ctl,
                                                                     L.bulk_cols);
@@ -1196,7 +1203,7 @@ int set_row_attrs(int ny) {
 
 template <int PX>
 int set_col_attrs(int nx) {
-  cudaError_t e = set_attr(kf_cols_AB<PX>, seq_smem(nx, kCols));
+  cudaError_t e = set_attr(kf_cols_AB<PX>, seq_smem(nx, 2 * kCols));
   if (e == cudaSuccess) e = set_attr(kf_cols_CD_eta<PX>, cols_cd_smem(nx, 1));
   if (e == cudaSuccess) e = set_attr(kf_cols_CD_X<PX>, cols_cd_smem(nx, 2));
   return (int)e;
