@@ -1161,7 +1161,7 @@ int kks_pipeline(kks_handle* h, int32_t* fused, int32_t* kernels) {
   // rows D, extras (new state), decide, restore; cuFFT pipeline: prologue,
   // prep, spectral_mid, pre_pointwise, spectral_update, post_pointwise,
   // decide, restore
-  if (kernels) *kernels = h->fused ? 11 : 8;
+  if (kernels) *kernels = h->fused ? 10 : 8;
   return KKS_OK;
 }
 

@@ -568,7 +568,8 @@ __device__ __forceinline__ void stage_store(const CUtensorMap* map, const float2
 
 // ---------------------------------------------------------------------------
 // pass 1: one row pair; the sequences are eta, X, eta^2 -> row spectra RA;
-// old-state history sums.
+// old-state history sums and, at surface steps, the interface cells of rows
+// ix0 and ix0 + 1 (corners in rows ix0 .. ix0 + 2; pf_kks/microstructure.py:117-128).
 template <int PY>
 __global__ void __launch_bounds__(kThreads, kMinBlocks)
     kf_rows_A(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const KksFftConst* __restrict__ fc,
@@ -598,7 +599,8 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
     }
     bulk_wait(&bar, 0, ctl);
   }
-  double acc[5] = {0, 0, 0, 0, 0};
+  const bool surface = par->surface;
+  double acc[6] = {0, 0, 0, 0, 0, 0};
   for (int y = threadIdx.x; y < ny; y += kThreads) {
     double e0, x0, e1, x1;
     if (bulk) {
@@ -606,6 +608,14 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
     } else {
       e0 = eta[i0 + y], x0 = X[i0 + y];
       e1 = has1 ? eta[i0 + ny + y] : 0.0, x1 = has1 ? X[i0 + ny + y] : 0.0;
+    }
+    if (surface && y < ny - 1 && ix0 < nx - 1) {  // ix0 < nx - 1: row ix0 + 1 exists
+      const double e0n = bulk ? s_eta[y + 1] : eta[i0 + y + 1];
+      const double e1n = bulk ? s_eta[ny + y + 1] : eta[i0 + ny + y + 1];
+      const bool m1 = in_iface(e1) && in_iface(e1n);
+      if (m1 && in_iface(e0) && in_iface(e0n)) acc[5] += 1.0;
+      if (m1 && ix0 + 1 < nx - 1 && in_iface(eta[i0 + 2 * ny + y]) && in_iface(eta[i0 + 2 * ny + y + 1]))
+        acc[5] += 1.0;
     }
     sm[y] = make_float2((float)e0, (float)e1);
     sm[ny + y] = make_float2((float)x0, (float)x1);
@@ -632,7 +642,8 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
   } else {
     for (int f = 0; f < 3; ++f) split_store(sm + f * ny, ay, RA + f * fs, ix0, has1, nx, nyh);
   }
-  block_reduce_store<5>(acc, partials + (size_t)blockIdx.x * KKS_NPART + P3_ETA);
+  static_assert(P3_IFACE == P3_ETA + 5, "rows_A writes P3_ETA .. P3_IFACE");
+  block_reduce_store<6>(acc, partials + (size_t)blockIdx.x * KKS_NPART + P3_ETA);
 }
 
 // pass 2: kCols adjacent y-frequency columns of RA. blockIdx.y: 0 eta -> keep
@@ -1272,7 +1283,6 @@ int kks_fft_prime_table(int P, float2* out) {
 
 void kks_fft_launch_attempt(const KksFftLaunch& L, int p, cudaStream_t s) {
   const KksFieldPtrs& f = *L.f;
-  kf_extras<<<L.nbx, kExtrasThreads, 0, s>>>(L.dc, L.par, (const double*)f.eta[p], 2, 0, P3_IFACE, f.partials);
 #define KKS_ROWS(P) launch_rows<P>(L, p, stage, s)
 #define KKS_COLS(P) launch_cols<P>(L, stage, s)
   int stage = 0;
