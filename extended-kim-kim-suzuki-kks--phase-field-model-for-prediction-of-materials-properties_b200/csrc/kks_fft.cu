@@ -1112,22 +1112,42 @@ __global__ void __launch_bounds__(kExtrasThreads)
   if (!do_grad && !do_iface) return;
   const int N = c->N, nx = c->nx, ny = c->ny;
   double acc[2] = {0, 0};
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
-    const int ix = i / ny, iy = i - ix * ny;
-    const double e = eta[i];
-    if (do_grad) {
-      double gx, gy;
-      if (ix == 0) gx = eta[i + ny] - e;
-      else if (ix == nx - 1) gx = e - eta[i - ny];
-      else gx = (eta[i + ny] - eta[i - ny]) / 2.0;
-      if (iy == 0) gy = eta[i + 1] - e;
-      else if (iy == ny - 1) gy = e - eta[i - 1];
-      else gy = (eta[i + 1] - eta[i - 1]) / 2.0;
-      acc[0] += gx * gx + gy * gy;
+  // kU points per thread and iteration, their stencil loads issued together
+  constexpr int kU = 4;
+  const int stride = gridDim.x * blockDim.x;
+  for (int i0 = blockIdx.x * blockDim.x + threadIdx.x; i0 < N; i0 += kU * stride) {
+    double e[kU], xm[kU], xp[kU], ym[kU], yp[kU];
+#pragma unroll
+    for (int u = 0; u < kU; ++u) {
+      const int i = i0 + u * stride;
+      if (i < N) {
+        const int ix = i / ny, iy = i - ix * ny;
+        e[u] = eta[i];
+        xm[u] = ix > 0 ? eta[i - ny] : 0.0;
+        xp[u] = ix < nx - 1 ? eta[i + ny] : 0.0;
+        ym[u] = iy > 0 ? eta[i - 1] : 0.0;
+        yp[u] = iy < ny - 1 ? eta[i + 1] : 0.0;
+      }
     }
-    if (do_iface && ix < nx - 1 && iy < ny - 1 && in_iface(e) && in_iface(eta[i + ny]) &&
-        in_iface(eta[i + ny + 1]) && in_iface(eta[i + 1]))
-      acc[1] += 1.0;
+#pragma unroll
+    for (int u = 0; u < kU; ++u) {
+      const int i = i0 + u * stride;
+      if (i >= N) break;
+      const int ix = i / ny, iy = i - ix * ny;
+      if (do_grad) {
+        double gx, gy;
+        if (ix == 0) gx = xp[u] - e[u];
+        else if (ix == nx - 1) gx = e[u] - xm[u];
+        else gx = (xp[u] - xm[u]) / 2.0;
+        if (iy == 0) gy = yp[u] - e[u];
+        else if (iy == ny - 1) gy = e[u] - ym[u];
+        else gy = (yp[u] - ym[u]) / 2.0;
+        acc[0] += gx * gx + gy * gy;
+      }
+      if (do_iface && ix < nx - 1 && iy < ny - 1 && in_iface(e[u]) && in_iface(xp[u]) &&
+          in_iface(eta[i + ny + 1]) && in_iface(yp[u]))
+        acc[1] += 1.0;
+    }
   }
   double a1[1] = {acc[0]};
   double a2[1] = {acc[1]};

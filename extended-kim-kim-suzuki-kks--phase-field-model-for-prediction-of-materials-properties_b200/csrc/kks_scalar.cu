@@ -84,6 +84,17 @@ __device__ double effective_vacancy_diffusivity(double T, double Xv, double Xve)
   return fabs(1 + (Xv - Xve) / Xve) * (0.03 * D_Si + 0.97 * D_Al);
 }
 
+// Copy a read-only struct into shared memory with all threads of the block
+// (independent 8-byte loads), so that the single-thread chains below read it
+// at shared-memory latency instead of one L2 round trip per cache line.
+template <typename T>
+__device__ __forceinline__ void stage_struct(T* dst, const T* src) {
+  static_assert(sizeof(T) % 8 == 0 && alignof(T) >= 8, "8-byte words");
+  const long long* s = reinterpret_cast<const long long*>(src);
+  long long* d = reinterpret_cast<long long*>(dst);
+  for (int i = threadIdx.x; i < (int)(sizeof(T) / 8); i += blockDim.x) d[i] = s[i];
+}
+
 __device__ void push_record(KksCtl* ctl, kks_record* ring, long long cap, const kks_record& r) {
   ring[ctl->n_rec % cap] = r;
   ctl->n_rec += 1;
@@ -95,7 +106,11 @@ __global__ void kks_prologue(const KksConst* __restrict__ c, KksCtl* ctl, KksPar
   // interpolated at T by one lane each (same expressions, same roundings)
   __shared__ int s_go;
   __shared__ double s_T, s_tab[KKS_NTAB];
-  const kks_params& p = c->p;
+  __shared__ KksConst sc;
+  stage_struct(&sc, c);
+  __syncwarp();
+  c = &sc;
+  const kks_params& p = sc.p;
   const int lane = threadIdx.x;
   if (lane == 0) {
     s_go = ctl->status == KKS_STATUS_OK && ctl->istep < ctl->target_step;
@@ -221,13 +236,28 @@ __global__ void __launch_bounds__(32 * kDecideWarps) kks_decide(const KksConst* 
                            kks_step_row* rows, long long row_cap) {
   __shared__ double S[P_COUNT];
   __shared__ double G[kDecideWarps][KKS_NPART + 1];
+  __shared__ KksConst sc;
+  __shared__ KksPar sp;
   if (!par->active) return;
+  stage_struct(&sc, c);
+  stage_struct(&sp, par);
   // warp w sums rows w, w + W, ...: lane k reads slot k, so a warp reads one
-  // whole row per load; the W row groups are then added in a fixed order
+  // whole row per load, kU rows in flight; the W row groups are then added in
+  // a fixed order
   {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    constexpr int kU = 8;
     double v = 0;
-    for (int b = w; b < nblocks; b += kDecideWarps) v += partials[(size_t)b * KKS_NPART + lane];
+    for (int b0 = w; b0 < nblocks; b0 += kU * kDecideWarps) {
+      double r[kU];
+#pragma unroll
+      for (int u = 0; u < kU; ++u) {
+        const int b = b0 + u * kDecideWarps;
+        r[u] = b < nblocks ? partials[(size_t)b * KKS_NPART + lane] : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < kU; ++u) v += r[u];
+    }
     G[w][lane] = v;
     __syncthreads();
     if (threadIdx.x < P_COUNT) {
@@ -239,7 +269,9 @@ __global__ void __launch_bounds__(32 * kDecideWarps) kks_decide(const KksConst* 
   }
   if (threadIdx.x != 0) return;
 
-  const kks_params& p = c->p;
+  c = &sc;
+  par = &sp;
+  const kks_params& p = sc.p;
   const double Nd = (double)c->N;
   const int istep = par->istep;
   const int iteration = ctl->iteration;
