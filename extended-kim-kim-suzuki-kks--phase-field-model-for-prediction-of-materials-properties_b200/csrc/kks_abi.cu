@@ -713,6 +713,8 @@ int kks_run(kks_handle* h, int32_t n_steps, int32_t* status) {
   h->device_ms += ms;
   h->timed_attempts += launched;
   h->attempts_launched += launched;
+  // attempts launched after a stop did not run: the device's parity is the state's
+  h->parity = c->parity;
   if (status) *status = c->status;
   return KKS_OK;
 }
@@ -768,8 +770,251 @@ int kks_run_many(kks_handle** cells, int32_t n_cells, const int32_t* n_steps, in
     h->device_ms += ms;
     h->timed_attempts += launched[i];
     h->attempts_launched += launched[i];
+    h->parity = h->h_ctl->parity;
     if (status) status[i] = h->h_ctl->status;
   }
+  return KKS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Batches: cells of one device on the fused mixed pipeline, advanced together.
+// One attempt of the batch is one launch per kernel for all cells (block maps
+// built here, largest cells first), captured once as a CUDA graph; each cell's
+// state parity, target step, dt and rejections stay on the device, so cells
+// of different sizes and schedules advance in lockstep without a host
+// decision, and a cell that has reached its target or stopped sits out.
+struct kks_batch {
+  std::vector<kks_handle*> cells;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaGraphExec_t graph = nullptr;
+  KksCellDesc* d_cells = nullptr;
+  int2* d_maps = nullptr;
+  KksBatchLaunch L{};
+  int32_t* h_stage = nullptr;  // pinned: target step per cell
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  double device_ms = 0.0;
+  long long attempts = 0;
+  long long max_batch = 1;
+};
+
+static void free_batch(kks_batch* b) {
+  if (!b) return;
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  cudaFree(b->d_cells);
+  cudaFree(b->d_maps);
+  if (b->h_stage) cudaFreeHost(b->h_stage);
+  if (b->ev0) cudaEventDestroy(b->ev0);
+  if (b->ev1) cudaEventDestroy(b->ev1);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+}
+
+static void fill_desc(KksCellDesc& d, const kks_handle* h) {
+  memset(&d, 0, sizeof(d));
+  const KksFftLaunch& L = h->fl;
+  const KksFieldPtrs& f = h->f;
+  d.map_RA3 = L.map_RA3;
+  d.map_RB3 = L.map_RB3;
+  d.map_RB2 = L.map_RB2;
+  d.dc = h->dc;
+  d.par = h->d_par;
+  d.ctl = h->d_ctl;
+  d.fc = h->d_fc;
+  for (int p = 0; p < 2; ++p) {
+    d.eta[p] = (double*)f.eta[p];
+    d.X[p] = (double*)f.X[p];
+    d.X_al[p] = (float*)f.X_al[p];
+    d.X_th[p] = (float*)f.X_th[p];
+  }
+  d.eta_m = (double*)f.eta_m;
+  d.X_m = (double*)f.X_m;
+  d.mu = (float*)f.mu;
+  for (int k = 0; k < 3; ++k) d.g[k] = (float*)f.g[k];
+  d.RA = (float2*)L.RA;
+  d.RB = (float2*)L.RB;
+  d.SA = (float2*)L.SA;
+  d.partials = h->partials_fused;
+  d.ky = h->d_ky;
+  d.step_flags = h->d_flags;
+  d.ring = h->d_ring;
+  d.ring_cap = h->ring_cap;
+  d.rows = h->d_rows;
+  d.row_cap = h->row_cap;
+  d.N = h->hc.N;
+  d.nbx = h->nblocks;
+  d.part_rows = h->nb_fused;
+  d.bulk_rows = L.bulk_rows;
+  d.bulk_cols = L.bulk_cols;
+}
+
+static int batch_create_impl(kks_batch* b) {
+  const int n = (int)b->cells.size();
+  CK(cudaSetDevice(b->device));
+  CK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+  CK(cudaEventCreate(&b->ev0));
+  CK(cudaEventCreate(&b->ev1));
+  CK(cudaMallocHost(&b->h_stage, n * sizeof(int32_t)));
+  std::vector<KksCellDesc> desc(n);
+  std::vector<int> nx(n), ny(n);
+  for (int i = 0; i < n; ++i) {
+    fill_desc(desc[i], b->cells[i]);
+    nx[i] = b->cells[i]->hc.nx;
+    ny[i] = b->cells[i]->hc.ny;
+  }
+  // largest cells first, so that the small ones fill the last wave of a pass
+  std::vector<int> order(n);
+  for (int i = 0; i < n; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int a, int c) { return b->cells[a]->hc.N > b->cells[c]->hc.N; });
+  std::vector<int2> rows, cols, cols3, extras;
+  for (int i : order) {
+    const int nr = kks_fft_row_blocks(nx[i]), nc = kks_fft_col_blocks(ny[i] / 2 + 1);
+    for (int k = 0; k < nr; ++k) rows.push_back(make_int2(i, k));
+    for (int k = 0; k < nc; ++k) cols.push_back(make_int2(i, k));
+    for (int r = 0; r < 3; ++r)
+      for (int k = 0; k < nc; ++k) cols3.push_back(make_int2(i, (r << 16) | k));
+    for (int k = 0; k < desc[i].nbx; ++k) extras.push_back(make_int2(i, k));
+  }
+  KksBatchLaunch& L = b->L;
+  L.n_cells = n;
+  L.PX = b->cells[0]->fl.PX;
+  L.PY = b->cells[0]->fl.PY;
+  L.n_rows = (int)rows.size();
+  L.n_cols = (int)cols.size();
+  L.n_cols3 = (int)cols3.size();
+  L.n_extras = (int)extras.size();
+  CK(cudaMalloc(&b->d_cells, n * sizeof(KksCellDesc)));
+  CK(cudaMemcpy(b->d_cells, desc.data(), n * sizeof(KksCellDesc), cudaMemcpyHostToDevice));
+  const size_t nm = rows.size() + cols.size() + cols3.size() + extras.size();
+  CK(cudaMalloc(&b->d_maps, nm * sizeof(int2)));
+  int2* m = b->d_maps;
+  for (const std::vector<int2>* v : {&rows, &cols, &cols3, &extras}) {
+    CK(cudaMemcpy(m, v->data(), v->size() * sizeof(int2), cudaMemcpyHostToDevice));
+    if (v == &rows) L.map_rows = m;
+    else if (v == &cols) L.map_cols = m;
+    else if (v == &cols3) L.map_cols3 = m;
+    else L.map_extras = m;
+    m += v->size();
+  }
+  L.cells = b->d_cells;
+  if (kks_fft_batch_prepare(L, nx.data(), ny.data(), n) != 0)
+    return set_error(KKS_ERR_CUDA, "batched fft kernel attributes");
+  b->max_batch = 1LL << 30;
+  for (kks_handle* h : b->cells)
+    b->max_batch = std::min(b->max_batch, std::max(1LL, std::min(h->ring_cap / 2 - 1, h->row_cap - 1)));
+  cudaGraph_t g = nullptr;
+  CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+  kks_fft_launch_attempt_batch(L, b->stream);
+  const cudaError_t le = cudaGetLastError();
+  cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+  if (le != cudaSuccess) e = le;
+  if (e != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    return set_error(KKS_ERR_CUDA, std::string("batch graph capture: ") + cudaGetErrorString(e));
+  }
+  e = cudaGraphInstantiate(&b->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return set_error(KKS_ERR_CUDA, std::string("batch graph instantiate: ") + cudaGetErrorString(e));
+  return KKS_OK;
+}
+
+int kks_batch_create(kks_handle* const* cells, int32_t n_cells, kks_batch** out) {
+  if (!cells || !out || n_cells < 1) return set_error(KKS_ERR_ARG, "bad argument");
+  *out = nullptr;
+  for (int i = 0; i < n_cells; ++i) {
+    const kks_handle* h = cells[i];
+    if (!h) return set_error(KKS_ERR_ARG, "null cell");
+    if (!h->fused)
+      return set_error(KKS_ERR_ARG, "batched cells must use the fused mixed pipeline (KKS_PRECISION_MIXED, supported sizes)");
+    if (h->device != cells[0]->device) return set_error(KKS_ERR_ARG, "cells must share one device");
+    if (h->fl.PX != cells[0]->fl.PX || h->fl.PY != cells[0]->fl.PY)
+      return set_error(KKS_ERR_ARG, "batched cells must share the large prime factor of each axis");
+    for (int j = 0; j < i; ++j)
+      if (cells[j] == h) return set_error(KKS_ERR_ARG, "a cell appears twice in the batch");
+  }
+  kks_batch* b = new (std::nothrow) kks_batch();
+  if (!b) return set_error(KKS_ERR_ARG, "out of host memory");
+  b->cells.assign(cells, cells + n_cells);
+  b->device = cells[0]->device;
+  const int rc = batch_create_impl(b);
+  if (rc != KKS_OK) {
+    std::string msg = g_last_error;
+    free_batch(b);
+    g_last_error = msg;
+    return rc;
+  }
+  *out = b;
+  return KKS_OK;
+}
+
+int kks_batch_run(kks_batch* b, const int32_t* n_steps, int32_t* status) {
+  if (!b || !n_steps) return set_error(KKS_ERR_ARG, "bad argument");
+  const int n = (int)b->cells.size();
+  std::vector<long long> target(n);
+  for (int i = 0; i < n; ++i) {
+    kks_handle* h = b->cells[i];
+    if (n_steps[i] < 0) return set_error(KKS_ERR_ARG, "negative step count");
+    if (!h->uploaded) return set_error(KKS_ERR_STATE, "kks_batch_run before kks_upload of every cell");
+    target[i] = (long long)h->h_ctl->istep + n_steps[i];
+    if (target[i] > h->hc.n_steps) return set_error(KKS_ERR_ARG, "run beyond the scheduled number of steps");
+  }
+  CK(cudaSetDevice(b->device));
+  for (int i = 0; i < n; ++i) {
+    kks_handle* h = b->cells[i];
+    CK(cudaStreamSynchronize(h->stream));  // the cell's own work (uploads, runs) is done
+    b->h_stage[i] = (int32_t)target[i];
+    CK(cudaMemcpyAsync(&h->d_ctl->target_step, &b->h_stage[i], sizeof(int32_t), cudaMemcpyHostToDevice,
+                       b->stream));
+  }
+  CK(cudaEventRecord(b->ev0, b->stream));
+  long long launched = 0;
+  for (;;) {
+    long long todo = 0;
+    for (int i = 0; i < n; ++i) {
+      const KksCtl* c = b->cells[i]->h_ctl;
+      if (c->status == KKS_STATUS_OK && c->istep < target[i]) todo = std::max(todo, target[i] - c->istep);
+    }
+    if (todo == 0) break;
+    todo = std::min(todo, b->max_batch);
+    for (long long a = 0; a < todo; ++a) CK(cudaGraphLaunch(b->graph, b->stream));
+    launched += todo;
+    for (int i = 0; i < n; ++i) {
+      kks_handle* h = b->cells[i];
+      CK(cudaMemcpyAsync(h->h_ctl, h->d_ctl, sizeof(KksCtl), cudaMemcpyDeviceToHost, b->stream));
+    }
+    CK(cudaStreamSynchronize(b->stream));
+    for (int i = 0; i < n; ++i) {
+      int rc = drain_device(b->cells[i]);
+      if (rc != KKS_OK) return rc;
+    }
+  }
+  CK(cudaEventRecord(b->ev1, b->stream));
+  CK(cudaEventSynchronize(b->ev1));
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
+  b->device_ms += ms;
+  b->attempts += launched;
+  for (int i = 0; i < n; ++i) {
+    kks_handle* h = b->cells[i];
+    h->parity = h->h_ctl->parity;
+    if (status) status[i] = h->h_ctl->status;
+  }
+  return KKS_OK;
+}
+
+int kks_batch_timing(const kks_batch* b, double* device_ms, int64_t* attempts) {
+  if (!b) return set_error(KKS_ERR_ARG, "null batch");
+  if (device_ms) *device_ms = b->device_ms;
+  if (attempts) *attempts = b->attempts;
+  return KKS_OK;
+}
+
+int kks_batch_destroy(kks_batch* b) {
+  if (!b) return KKS_OK;
+  CK(cudaSetDevice(b->device));
+  free_batch(b);
   return KKS_OK;
 }
 

@@ -47,6 +47,7 @@
 
 #include <math.h>
 
+#include <algorithm>
 #include <vector>
 
 #include <cuda.h>
@@ -571,17 +572,16 @@ __device__ __forceinline__ void stage_store(const CUtensorMap* map, const float2
 // old-state history sums and, at surface steps, the interface cells of rows
 // ix0 and ix0 + 1 (corners in rows ix0 .. ix0 + 2; pf_kks/microstructure.py:117-128).
 template <int PY>
-__global__ void __launch_bounds__(kThreads, kMinBlocks)
-    kf_rows_A(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const KksFftConst* __restrict__ fc,
+__device__ __forceinline__ void rows_A_body(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const KksFftConst* __restrict__ fc,
               const double* __restrict__ eta, const double* __restrict__ X, float2* __restrict__ RA,
-              double* __restrict__ partials, KksCtl* ctl, int bulk, const __grid_constant__ CUtensorMap map_RA) {
+              double* __restrict__ partials, KksCtl* ctl, int bulk, const CUtensorMap* map_RA, int bx) {
   if (!par->active) return;
   prime_table_fill<PY>(fc->ay.ptw);
   extern __shared__ float2 sm[];
   __shared__ __align__(8) uint64_t bar;
   const KksFftAxis& ay = fc->ay;
   const int nx = c->nx, ny = c->ny, nyh = c->nyh;
-  const int ix0 = 2 * blockIdx.x;
+  const int ix0 = 2 * bx;
   const bool has1 = ix0 + 1 < nx;
   const size_t i0 = (size_t)ix0 * ny;
   // staging after the three sequences: rows ix0, ix0+1 of eta and X, later
@@ -638,22 +638,29 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
     for (int f = 0; f < 3; ++f) split_stage(sm + f * ny, ay, st, f, 3, kb, nyh);
     fence_async_smem();
     __syncthreads();
-    if (threadIdx.x == 0) stage_store(&map_RA, st, ix0, 3, kb, nb);
+    if (threadIdx.x == 0) stage_store(map_RA, st, ix0, 3, kb, nb);
   } else {
     for (int f = 0; f < 3; ++f) split_store(sm + f * ny, ay, RA + f * fs, ix0, has1, nx, nyh);
   }
   static_assert(P3_IFACE == P3_ETA + 5, "rows_A writes P3_ETA .. P3_IFACE");
-  block_reduce_store<6>(acc, partials + (size_t)blockIdx.x * KKS_NPART + P3_ETA);
+  block_reduce_store<6>(acc, partials + (size_t)bx * KKS_NPART + P3_ETA);
 }
 
-// pass 2: kCols adjacent y-frequency columns of RA. blockIdx.y: 0 eta -> keep
+template <int PY>
+__global__ void __launch_bounds__(kThreads, kMinBlocks)
+    kf_rows_A(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const KksFftConst* __restrict__ fc,
+              const double* __restrict__ eta, const double* __restrict__ X, float2* __restrict__ RA,
+              double* __restrict__ partials, KksCtl* ctl, int bulk, const __grid_constant__ CUtensorMap map_RA) {
+  rows_A_body<PY>(c, par, fc, eta, X, RA, partials, ctl, bulk, &map_RA, (int)blockIdx.x);
+}
+
+// pass 2: kCols adjacent y-frequency columns of RA. Role by: 0 eta -> keep
 // FT(eta), i k_x FT(eta) and i k_y FT(eta) (one forward, two inverse
 // transforms); 1 eta^2 -> tr eps^ (+ Parseval sums); 2 X -> keep FT(X).
 template <int PX>
-__global__ void __launch_bounds__(kThreads, kMinBlocks)
-    kf_cols_AB(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const KksFftConst* __restrict__ fc,
+__device__ __forceinline__ void cols_AB_body(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const KksFftConst* __restrict__ fc,
                const float2* __restrict__ RA, float2* __restrict__ SA, float2* __restrict__ RB,
-               const double* __restrict__ kys, double* __restrict__ partials, KksCtl* ctl, int bulk) {
+               const double* __restrict__ kys, double* __restrict__ partials, KksCtl* ctl, int bulk, int bx, int by) {
   if (!par->active) return;
   prime_table_fill<PX>(fc->ax.ptw);
   extern __shared__ float2 sm[];
@@ -662,8 +669,8 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
   const KksFftAxis& ax = fc->ax;
   const int nx = c->nx, ny = c->ny, nyh = c->nyh;
   const size_t fs = (size_t)nx * nyh;
-  const int g = blockIdx.y;
-  const int ky0 = blockIdx.x * kCols;
+  const int g = by;
+  const int ky0 = bx * kCols;
   const int ncol = min(kCols, nyh - ky0);
   const int nv = ncol * nx;
   const int src_field = g == 0 ? 0 : (g == 1 ? 2 : 1);
@@ -727,7 +734,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
       }
     }
   }
-  if (g == 1) block_reduce_store<6>(acc, partials + (size_t)blockIdx.x * KKS_NPART + P2_OXX2);
+  if (g == 1) block_reduce_store<6>(acc, partials + (size_t)bx * KKS_NPART + P2_OXX2);
   __syncthreads();
   // g = 0: the i k_x columns at [0, nv), the i k_y columns at [nv, 2 nv)
   fft_run<+1, PX>(g == 0 ? 2 * ncol : ncol, ax);
@@ -744,16 +751,23 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
   }
 }
 
+template <int PX>
+__global__ void __launch_bounds__(kThreads, kMinBlocks)
+    kf_cols_AB(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const KksFftConst* __restrict__ fc,
+               const float2* __restrict__ RA, float2* __restrict__ SA, float2* __restrict__ RB,
+               const double* __restrict__ kys, double* __restrict__ partials, KksCtl* ctl, int bulk) {
+  cols_AB_body<PX>(c, par, fc, RA, SA, RB, kys, partials, ctl, bulk, (int)blockIdx.x, (int)blockIdx.y);
+}
+
 // pass 3: one row pair of RB (tr eps, d_x eta, d_y eta) -> inverse FFT ->
 // pointwise with the old state: the Allen-Cahn drive (free energy + elastic)
 // and the Cahn-Hilliard fluxes -> forward FFT -> row spectra RC; sum G.
 template <int PY>
-__global__ void __launch_bounds__(kThreads, kMinBlocks)
-    kf_rows_BC(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const KksFftConst* __restrict__ fc,
+__device__ __forceinline__ void rows_BC_body(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const KksFftConst* __restrict__ fc,
                const float2* __restrict__ RB, float2* __restrict__ RC, const double* __restrict__ eta,
                const float* __restrict__ Xal, const float* __restrict__ Xth, float* g0, float* g1, float* g2,
-               double* __restrict__ partials, KksCtl* ctl, int bulk, const __grid_constant__ CUtensorMap map_RB,
-               const __grid_constant__ CUtensorMap map_RC) {
+               double* __restrict__ partials, KksCtl* ctl, int bulk, const CUtensorMap* map_RB,
+               const CUtensorMap* map_RC, int bx) {
   if (!par->active) return;
   prime_table_fill<PY>(fc->ay.ptw);
   extern __shared__ float2 sm[];
@@ -761,7 +775,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
   const KksFftAxis& ay = fc->ay;
   const int nx = c->nx, ny = c->ny, nyh = c->nyh;
   const size_t fs = (size_t)nx * nyh;
-  const int ix0 = 2 * blockIdx.x;
+  const int ix0 = 2 * bx;
   const bool has1 = ix0 + 1 < nx;
   const int kb = nyh < 256 ? nyh : 256, nb = (nyh + kb - 1) / kb;
   // staging after the three sequences: the pair's three half spectra (tensor
@@ -775,7 +789,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
   if (bulk) {
     if (threadIdx.x == 0) {
       mbar_init(&bar);
-      stage_load(st, &map_RB, ix0, 3, kb, nb, &bar);
+      stage_load(st, map_RB, ix0, 3, kb, nb, &bar);
     }
     __syncthreads();
     bulk_wait(&bar, 0, ctl);
@@ -843,20 +857,29 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
     for (int f = 0; f < 3; ++f) split_stage(sm + f * ny, ay, st, f, 3, kb, nyh);
     fence_async_smem();
     __syncthreads();
-    if (threadIdx.x == 0) stage_store(&map_RC, st, ix0, 3, kb, nb);
+    if (threadIdx.x == 0) stage_store(map_RC, st, ix0, 3, kb, nb);
   } else {
     for (int f = 0; f < 3; ++f) split_store(sm + f * ny, ay, RC + f * fs, ix0, has1, nx, nyh);
   }
   double acc[1] = {accG};
-  block_reduce_store<1>(acc, partials + (size_t)blockIdx.x * KKS_NPART + P3_G);
+  block_reduce_store<1>(acc, partials + (size_t)bx * KKS_NPART + P3_G);
+}
+
+template <int PY>
+__global__ void __launch_bounds__(kThreads, kMinBlocks)
+    kf_rows_BC(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const KksFftConst* __restrict__ fc,
+               const float2* __restrict__ RB, float2* __restrict__ RC, const double* __restrict__ eta,
+               const float* __restrict__ Xal, const float* __restrict__ Xth, float* g0, float* g1, float* g2,
+               double* __restrict__ partials, KksCtl* ctl, int bulk, const __grid_constant__ CUtensorMap map_RB,
+               const __grid_constant__ CUtensorMap map_RC) {
+  rows_BC_body<PY>(c, par, fc, RB, RC, eta, Xal, Xth, g0, g1, g2, partials, ctl, bulk, &map_RB, &map_RC, (int)blockIdx.x);
 }
 
 // pass 4a: kCols columns of FT(drive) with FT(eta) -> d_eta^ -> row spectra RD[0]
 template <int PX>
-__global__ void __launch_bounds__(kThreads, kMinBlocks)
-    kf_cols_CD_eta(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const KksFftConst* __restrict__ fc,
+__device__ __forceinline__ void cols_CD_eta_body(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const KksFftConst* __restrict__ fc,
                    const float2* __restrict__ RC, const float2* __restrict__ SA, float2* __restrict__ RD,
-                   const double* __restrict__ kys, KksCtl* ctl, int bulk) {
+                   const double* __restrict__ kys, KksCtl* ctl, int bulk, int bx) {
   if (!par->active) return;
   prime_table_fill<PX>(fc->ax.ptw);
   extern __shared__ float2 sm[];
@@ -864,7 +887,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
   bulk = bulk && (smem_u32(sm) & 15u) == 0;  // bulk destinations need 16-byte alignment
   const KksFftAxis& ax = fc->ax;
   const int nx = c->nx, nyh = c->nyh;
-  const int ky0 = blockIdx.x * kCols;
+  const int ky0 = bx * kCols;
   const int ncol = min(kCols, nyh - ky0);
   const int nv = ncol * nx;
   const float2* col = RC + (size_t)ky0 * nx;
@@ -909,12 +932,19 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
   for (int i = threadIdx.x; i < nv; i += kThreads) dst[i] = sm[i];
 }
 
-// pass 4b: kCols columns of FT(flux_x), FT(flux_y) with FT(X) -> d_X^ -> row spectra RD[1]
 template <int PX>
 __global__ void __launch_bounds__(kThreads, kMinBlocks)
-    kf_cols_CD_X(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const KksFftConst* __restrict__ fc,
+    kf_cols_CD_eta(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const KksFftConst* __restrict__ fc,
+                   const float2* __restrict__ RC, const float2* __restrict__ SA, float2* __restrict__ RD,
+                   const double* __restrict__ kys, KksCtl* ctl, int bulk) {
+  cols_CD_eta_body<PX>(c, par, fc, RC, SA, RD, kys, ctl, bulk, (int)blockIdx.x);
+}
+
+// pass 4b: kCols columns of FT(flux_x), FT(flux_y) with FT(X) -> d_X^ -> row spectra RD[1]
+template <int PX>
+__device__ __forceinline__ void cols_CD_X_body(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const KksFftConst* __restrict__ fc,
                  const float2* __restrict__ RC, const float2* __restrict__ SA, float2* __restrict__ RD,
-                 const double* __restrict__ kys, KksCtl* ctl, int bulk) {
+                 const double* __restrict__ kys, KksCtl* ctl, int bulk, int bx) {
   if (!par->active) return;
   prime_table_fill<PX>(fc->ax.ptw);
   extern __shared__ float2 sm[];
@@ -923,7 +953,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
   const KksFftAxis& ax = fc->ax;
   const int nx = c->nx, nyh = c->nyh;
   const size_t fs = (size_t)nx * nyh;
-  const int ky0 = blockIdx.x * kCols;
+  const int ky0 = bx * kCols;
   const int ncol = min(kCols, nyh - ky0);
   const int nv = ncol * nx;
   // flux_x columns at [0, nv), flux_y columns at [nv, 2 nv); FT(X) of the same
@@ -978,16 +1008,23 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
   for (int i = threadIdx.x; i < nv; i += kThreads) dst[i] = sm[i];
 }
 
+template <int PX>
+__global__ void __launch_bounds__(kThreads, kMinBlocks)
+    kf_cols_CD_X(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const KksFftConst* __restrict__ fc,
+                 const float2* __restrict__ RC, const float2* __restrict__ SA, float2* __restrict__ RD,
+                 const double* __restrict__ kys, KksCtl* ctl, int bulk) {
+  cols_CD_X_body<PX>(c, par, fc, RC, SA, RD, kys, ctl, bulk, (int)blockIdx.x);
+}
+
 // pass 5: one row pair of RD -> d_eta, d_X; new state, phase compositions,
 // new free energy and diffusion potential, residual and history sums
 template <int PY>
-__global__ void __launch_bounds__(kThreads, kMinBlocks)
-    kf_rows_D(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const KksFftConst* __restrict__ fc,
+__device__ __forceinline__ void rows_D_body(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const KksFftConst* __restrict__ fc,
               const float2* __restrict__ RD, const double* __restrict__ eta_o, const double* __restrict__ X_o,
               double* __restrict__ eta_b, double* __restrict__ X_b, float* __restrict__ Xal_b,
               float* __restrict__ Xth_b, const double* __restrict__ eta_m, const double* __restrict__ X_m,
               float* __restrict__ mu, float* g0, float* g1, float* g2, double* __restrict__ partials, KksCtl* ctl,
-              int bulk, const __grid_constant__ CUtensorMap map_RD) {
+              int bulk, const CUtensorMap* map_RD, int bx) {
   if (!par->active) return;
   prime_table_fill<PY>(fc->ay.ptw);
   extern __shared__ float2 sm[];
@@ -995,7 +1032,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
   const KksFftAxis& ay = fc->ay;
   const int nx = c->nx, ny = c->ny, nyh = c->nyh;
   const size_t fs = (size_t)nx * nyh;
-  const int ix0 = 2 * blockIdx.x;
+  const int ix0 = 2 * bx;
   const bool has1 = ix0 + 1 < nx;
   // staging after the two sequences: the pair's two half spectra (tensor
   // load), then rows ix0, ix0+1 of the old eta and X (bulk copies,
@@ -1008,7 +1045,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
     float2* st = (float2*)stage;
     if (threadIdx.x == 0) {
       mbar_init(&bar);
-      stage_load(st, &map_RD, ix0, 2, kb, nb, &bar);
+      stage_load(st, map_RD, ix0, 2, kb, nb, &bar);
     }
     __syncthreads();
     bulk_wait(&bar, 0, ctl);
@@ -1093,19 +1130,30 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
   }
   // slots P5_XLO, NLO, XHI, NHI, ETA are consecutive; DIFF, AC, TEMP, COMB follow P5_IFACE
   double a5[5] = {acc[0], acc[1], acc[2], acc[3], acc[4]};
-  block_reduce_store<5>(a5, partials + (size_t)blockIdx.x * KKS_NPART + P5_XLO);
+  block_reduce_store<5>(a5, partials + (size_t)bx * KKS_NPART + P5_XLO);
   __syncthreads();
   double a4[4] = {acc[5], acc[6], acc[7], acc[8]};
-  block_reduce_store<4>(a4, partials + (size_t)blockIdx.x * KKS_NPART + P5_DIFF);
+  block_reduce_store<4>(a4, partials + (size_t)bx * KKS_NPART + P5_DIFF);
+}
+
+template <int PY>
+__global__ void __launch_bounds__(kThreads, kMinBlocks)
+    kf_rows_D(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const KksFftConst* __restrict__ fc,
+              const float2* __restrict__ RD, const double* __restrict__ eta_o, const double* __restrict__ X_o,
+              double* __restrict__ eta_b, double* __restrict__ X_b, float* __restrict__ Xal_b,
+              float* __restrict__ Xth_b, const double* __restrict__ eta_m, const double* __restrict__ X_m,
+              float* __restrict__ mu, float* g0, float* g1, float* g2, double* __restrict__ partials, KksCtl* ctl,
+              int bulk, const __grid_constant__ CUtensorMap map_RD) {
+  rows_D_body<PY>(c, par, fc, RD, eta_o, X_o, eta_b, X_b, Xal_b, Xth_b, eta_m, X_m, mu, g0, g1, g2, partials, ctl, bulk, &map_RD, (int)blockIdx.x);
 }
 
 // np.gradient energy sum of a state (mode bit 0) and, at surface steps, its
 // interface cell count (mode bit 1) into the given partial slots.
 constexpr int kExtrasThreads = 256;
 
-__global__ void __launch_bounds__(kExtrasThreads)
-    kf_extras(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const double* __restrict__ eta,
-              int mode, int slot_grad, int slot_iface, double* __restrict__ partials) {
+__device__ __forceinline__ void extras_body(const KksConst* __restrict__ c, const KksPar* __restrict__ par,
+                                            const double* __restrict__ eta, int mode, int slot_grad, int slot_iface,
+                                            double* __restrict__ partials, int bx, int nbk) {
   if (!par->active) return;
   const bool do_grad = mode & 1;
   const bool do_iface = (mode & 2) && par->surface;
@@ -1114,8 +1162,8 @@ __global__ void __launch_bounds__(kExtrasThreads)
   double acc[2] = {0, 0};
   // kU points per thread and iteration, their stencil loads issued together
   constexpr int kU = 4;
-  const int stride = gridDim.x * blockDim.x;
-  for (int i0 = blockIdx.x * blockDim.x + threadIdx.x; i0 < N; i0 += kU * stride) {
+  const int stride = nbk * blockDim.x;
+  for (int i0 = bx * blockDim.x + threadIdx.x; i0 < N; i0 += kU * stride) {
     double e[kU], xm[kU], xp[kU], ym[kU], yp[kU];
 #pragma unroll
     for (int u = 0; u < kU; ++u) {
@@ -1151,9 +1199,130 @@ __global__ void __launch_bounds__(kExtrasThreads)
   }
   double a1[1] = {acc[0]};
   double a2[1] = {acc[1]};
-  if (do_grad) block_reduce_store<1, kExtrasThreads>(a1, partials + (size_t)blockIdx.x * KKS_NPART + slot_grad);
+  if (do_grad) block_reduce_store<1, kExtrasThreads>(a1, partials + (size_t)bx * KKS_NPART + slot_grad);
   __syncthreads();
-  if (do_iface) block_reduce_store<1, kExtrasThreads>(a2, partials + (size_t)blockIdx.x * KKS_NPART + slot_iface);
+  if (do_iface) block_reduce_store<1, kExtrasThreads>(a2, partials + (size_t)bx * KKS_NPART + slot_iface);
+}
+
+__global__ void __launch_bounds__(kExtrasThreads)
+    kf_extras(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const double* __restrict__ eta,
+              int mode, int slot_grad, int slot_iface, double* __restrict__ partials) {
+  extras_body(c, par, eta, mode, slot_grad, slot_iface, partials, (int)blockIdx.x, (int)gridDim.x);
+}
+
+// ---------------------------------------------------------------------------
+// Batched passes (KksBatchLaunch): one launch covers every cell of a batch.
+// Block b works on cell map[b].x as block map[b].y of that cell's own grid,
+// with the cell's pointers from its descriptor and its state parity from the
+// attempt's parameters (written by the batched prologue); a cell that takes
+// no part in this attempt (target reached, or stopped) returns at once.
+
+// Orders the host's writes of a tensor map held in global memory (a cell
+// descriptor) before its use by tensor copies.
+__device__ __forceinline__ void tensormap_acquire(const CUtensorMap* map) {
+  asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(map) : "memory");
+}
+
+template <int PY>
+__global__ void __launch_bounds__(kThreads, kMinBlocks)
+    kfb_rows_A(const KksCellDesc* __restrict__ cells, const int2* __restrict__ bmap) {
+  const int2 m = bmap[blockIdx.x];
+  const KksCellDesc* d = cells + m.x;
+  const int p = d->par->parity;
+  if (threadIdx.x == 0 && d->bulk_rows) tensormap_acquire(&d->map_RA3);
+  rows_A_body<PY>(d->dc, d->par, d->fc, d->eta[p], d->X[p], d->RA, d->partials, d->ctl, d->bulk_rows, &d->map_RA3,
+                  m.y);
+}
+
+template <int PX>
+__global__ void __launch_bounds__(kThreads, kMinBlocks)
+    kfb_cols_AB(const KksCellDesc* __restrict__ cells, const int2* __restrict__ bmap) {
+  const int2 m = bmap[blockIdx.x];
+  const KksCellDesc* d = cells + m.x;
+  cols_AB_body<PX>(d->dc, d->par, d->fc, d->RA, d->SA, d->RB, d->ky, d->partials, d->ctl, d->bulk_cols,
+                   m.y & 0xffff, m.y >> 16);
+}
+
+template <int PY>
+__global__ void __launch_bounds__(kThreads, kMinBlocks)
+    kfb_rows_BC(const KksCellDesc* __restrict__ cells, const int2* __restrict__ bmap) {
+  const int2 m = bmap[blockIdx.x];
+  const KksCellDesc* d = cells + m.x;
+  const int p = d->par->parity;
+  if (threadIdx.x == 0 && d->bulk_rows) {
+    tensormap_acquire(&d->map_RB3);
+    tensormap_acquire(&d->map_RA3);
+  }
+  rows_BC_body<PY>(d->dc, d->par, d->fc, d->RB, d->RA, d->eta[p], d->X_al[p], d->X_th[p], d->g[0], d->g[1], d->g[2],
+                   d->partials, d->ctl, d->bulk_rows, &d->map_RB3, &d->map_RA3, m.y);
+}
+
+template <int PX>
+__global__ void __launch_bounds__(kThreads, kMinBlocks)
+    kfb_cols_CD_eta(const KksCellDesc* __restrict__ cells, const int2* __restrict__ bmap) {
+  const int2 m = bmap[blockIdx.x];
+  const KksCellDesc* d = cells + m.x;
+  cols_CD_eta_body<PX>(d->dc, d->par, d->fc, d->RA, d->SA, d->RB, d->ky, d->ctl, d->bulk_cols, m.y);
+}
+
+template <int PX>
+__global__ void __launch_bounds__(kThreads, kMinBlocks)
+    kfb_cols_CD_X(const KksCellDesc* __restrict__ cells, const int2* __restrict__ bmap) {
+  const int2 m = bmap[blockIdx.x];
+  const KksCellDesc* d = cells + m.x;
+  cols_CD_X_body<PX>(d->dc, d->par, d->fc, d->RA, d->SA, d->RB, d->ky, d->ctl, d->bulk_cols, m.y);
+}
+
+template <int PY>
+__global__ void __launch_bounds__(kThreads, kMinBlocks)
+    kfb_rows_D(const KksCellDesc* __restrict__ cells, const int2* __restrict__ bmap) {
+  const int2 m = bmap[blockIdx.x];
+  const KksCellDesc* d = cells + m.x;
+  const int p = d->par->parity, q = p ^ 1;
+  if (threadIdx.x == 0 && d->bulk_rows) tensormap_acquire(&d->map_RB2);
+  rows_D_body<PY>(d->dc, d->par, d->fc, d->RB, d->eta[p], d->X[p], d->eta[q], d->X[q], d->X_al[q], d->X_th[q],
+                  d->eta_m, d->X_m, d->mu, d->g[0], d->g[1], d->g[2], d->partials, d->ctl, d->bulk_rows, &d->map_RB2,
+                  m.y);
+}
+
+// np.gradient energy and interface count of the candidate state
+__global__ void __launch_bounds__(kExtrasThreads)
+    kfb_extras(const KksCellDesc* __restrict__ cells, const int2* __restrict__ bmap) {
+  const int2 m = bmap[blockIdx.x];
+  const KksCellDesc* d = cells + m.x;
+  const int q = d->par->parity ^ 1;
+  extras_body(d->dc, d->par, d->eta[q], 3, P5_GRAD2, P5_IFACE, d->partials, m.y, d->nbx);
+}
+
+// After a rejection (decided by this attempt): the rejected candidate becomes
+// the pair's minus entry and the step's input is copied back into the
+// candidate buffer (k_restore of the single-cell attempt, per cell).
+__global__ void __launch_bounds__(kExtrasThreads)
+    kfb_restore(const KksCellDesc* __restrict__ cells, const int2* __restrict__ bmap) {
+  const int2 m = bmap[blockIdx.x];
+  const KksCellDesc* d = cells + m.x;
+  const KksCtl* ctl = d->ctl;
+  if (!d->par->active || !ctl->restore || ctl->status != KKS_STATUS_OK) return;
+  const int p = d->par->parity, q = p ^ 1;
+  const double* __restrict__ eta_i = d->eta[p];
+  const double* __restrict__ X_i = d->X[p];
+  const float* __restrict__ Xal_i = d->X_al[p];
+  const float* __restrict__ Xth_i = d->X_th[p];
+  double* __restrict__ eta_o = d->eta[q];
+  double* __restrict__ X_o = d->X[q];
+  float* __restrict__ Xal_o = d->X_al[q];
+  float* __restrict__ Xth_o = d->X_th[q];
+  double* __restrict__ eta_m = d->eta_m;
+  double* __restrict__ X_m = d->X_m;
+  const int N = d->N;
+  for (int i = m.y * kExtrasThreads + threadIdx.x; i < N; i += d->nbx * kExtrasThreads) {
+    eta_m[i] = eta_o[i];
+    X_m[i] = X_o[i];
+    eta_o[i] = eta_i[i];
+    X_o[i] = X_i[i];
+    Xal_o[i] = Xal_i[i];
+    Xth_o[i] = Xth_i[i];
+  }
 }
 
 // shared memory of each pass (bytes): its sequences, transformed in place,
@@ -1216,12 +1385,54 @@ void launch_cols(const KksFftLaunch& L, int stage, cudaStream_t s) {
   }
 }
 
+// The dynamic shared-memory limit of a kernel is process-wide: it is only
+// ever raised, so that a smaller cell created later does not lower the limit
+// that the graphs of a larger one rely on.
 template <typename K>
 cudaError_t set_attr(K* kernel, size_t smem) {
-  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaFuncAttributes fa;
+  cudaError_t e = cudaFuncGetAttributes(&fa, kernel);
+  if (e == cudaSuccess && (size_t)fa.maxDynamicSharedSizeBytes < smem)
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
   return e;
+}
+
+template <int PY>
+void launch_rows_batch(const KksBatchLaunch& B, int stage, cudaStream_t s) {
+  if (stage == 0)
+    kfb_rows_A<PY><<<B.n_rows, kThreads, B.smem_rows_a, s>>>(B.cells, B.map_rows);
+  else if (stage == 1)
+    kfb_rows_BC<PY><<<B.n_rows, kThreads, B.smem_rows_bc, s>>>(B.cells, B.map_rows);
+  else
+    kfb_rows_D<PY><<<B.n_rows, kThreads, B.smem_rows_d, s>>>(B.cells, B.map_rows);
+}
+
+template <int PX>
+void launch_cols_batch(const KksBatchLaunch& B, int stage, cudaStream_t s) {
+  if (stage == 0) {
+    kfb_cols_AB<PX><<<B.n_cols3, kThreads, B.smem_cols_ab, s>>>(B.cells, B.map_cols3);
+  } else {
+    kfb_cols_CD_eta<PX><<<B.n_cols, kThreads, B.smem_cols_cd1, s>>>(B.cells, B.map_cols);
+    kfb_cols_CD_X<PX><<<B.n_cols, kThreads, B.smem_cols_cd2, s>>>(B.cells, B.map_cols);
+  }
+}
+
+template <int PY>
+int set_row_batch_attrs(const KksBatchLaunch& B) {
+  cudaError_t e = set_attr(kfb_rows_A<PY>, B.smem_rows_a);
+  if (e == cudaSuccess) e = set_attr(kfb_rows_BC<PY>, B.smem_rows_bc);
+  if (e == cudaSuccess) e = set_attr(kfb_rows_D<PY>, B.smem_rows_d);
+  return (int)e;
+}
+
+template <int PX>
+int set_col_batch_attrs(const KksBatchLaunch& B) {
+  cudaError_t e = set_attr(kfb_cols_AB<PX>, B.smem_cols_ab);
+  if (e == cudaSuccess) e = set_attr(kfb_cols_CD_eta<PX>, B.smem_cols_cd1);
+  if (e == cudaSuccess) e = set_attr(kfb_cols_CD_X<PX>, B.smem_cols_cd2);
+  return (int)e;
 }
 
 template <int PY>
@@ -1317,4 +1528,56 @@ void kks_fft_launch_attempt(const KksFftLaunch& L, int p, cudaStream_t s) {
 #undef KKS_COLS
   kf_extras<<<L.nbx, kExtrasThreads, 0, s>>>(L.dc, L.par, (const double*)f.eta[1 - p], 3, P5_GRAD2, P5_IFACE,
                                        f.partials);
+}
+
+int kks_fft_col_blocks(int nyh) { return col_blocks(nyh); }
+
+int kks_fft_batch_prepare(KksBatchLaunch& B, const int* nx, const int* ny, int n) {
+  size_t ra = 0, rbc = 0, rd = 0, cab = 0, ccd1 = 0, ccd2 = 0;
+  for (int i = 0; i < n; ++i) {
+    ra = std::max(ra, rows_a_smem(ny[i]));
+    rbc = std::max(rbc, rows_bc_smem(ny[i]));
+    rd = std::max(rd, rows_d_smem(ny[i]));
+    cab = std::max(cab, seq_smem(nx[i], 2 * kCols));
+    ccd1 = std::max(ccd1, cols_cd_smem(nx[i], 1));
+    ccd2 = std::max(ccd2, cols_cd_smem(nx[i], 2));
+  }
+  B.smem_rows_a = ra;
+  B.smem_rows_bc = rbc;
+  B.smem_rows_d = rd;
+  B.smem_cols_ab = cab;
+  B.smem_cols_cd1 = ccd1;
+  B.smem_cols_cd2 = ccd2;
+  int rc = -1, rc2 = -1;
+#define KKS_ROWS_ATTR(P) rc = set_row_batch_attrs<P>(B)
+#define KKS_COLS_ATTR(P) rc2 = set_col_batch_attrs<P>(B)
+  KKS_FFT_DISPATCH(B.PY, KKS_ROWS_ATTR)
+  KKS_FFT_DISPATCH(B.PX, KKS_COLS_ATTR)
+#undef KKS_ROWS_ATTR
+#undef KKS_COLS_ATTR
+  if (rc == 0 && rc2 == 0) {
+    cudaError_t e = cudaFuncSetAttribute(kfb_extras, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                         cudaSharedmemCarveoutMaxShared);
+    rc = (int)e;
+  }
+  return rc != 0 ? rc : rc2;
+}
+
+void kks_fft_launch_attempt_batch(const KksBatchLaunch& B, cudaStream_t s) {
+  kks_launch_prologue_batch(B.cells, B.n_cells, s);
+#define KKS_ROWS(P) launch_rows_batch<P>(B, stage, s)
+#define KKS_COLS(P) launch_cols_batch<P>(B, stage, s)
+  int stage = 0;
+  KKS_FFT_DISPATCH(B.PY, KKS_ROWS)
+  KKS_FFT_DISPATCH(B.PX, KKS_COLS)
+  stage = 1;
+  KKS_FFT_DISPATCH(B.PY, KKS_ROWS)
+  KKS_FFT_DISPATCH(B.PX, KKS_COLS)
+  stage = 2;
+  KKS_FFT_DISPATCH(B.PY, KKS_ROWS)
+#undef KKS_ROWS
+#undef KKS_COLS
+  kfb_extras<<<B.n_extras, kExtrasThreads, 0, s>>>(B.cells, B.map_extras);
+  kks_launch_decide_batch(B.cells, B.n_cells, s);
+  kfb_restore<<<B.n_extras, kExtrasThreads, 0, s>>>(B.cells, B.map_extras);
 }

@@ -76,3 +76,65 @@ int kks_fft_set_attributes(const KksFftLaunch& L);
 #define KKS_FFT_PRIME_TABLE_MAX (5 * 35 * 8)
 int kks_fft_prime_table(int P, float2* out);
 void kks_fft_launch_attempt(const KksFftLaunch& L, int parity, cudaStream_t s);
+
+// ---------------------------------------------------------------------------
+// Batched launches: the cells of an ensemble advance together, every kernel of
+// the attempt launched once for all of them. A cell is described in device
+// memory (its tensor maps first, 64-byte aligned as TMA requires); a pass
+// block finds its cell and its block index within the cell in the pass's
+// block map. The state parity of each cell lives on the device (KksCtl::parity,
+// flipped by the prologue of every attempt the cell takes part in), so cells
+// that have reached their target, or stopped, skip attempts without losing
+// track of their buffers.
+struct __align__(64) KksCellDesc {
+  CUtensorMap map_RA3, map_RB3, map_RB2;
+  const KksConst* dc;
+  KksPar* par;
+  KksCtl* ctl;
+  const KksFftConst* fc;
+  double* eta[2];
+  double* X[2];
+  float* X_al[2];
+  float* X_th[2];
+  double* eta_m;
+  double* X_m;
+  float* mu;
+  float* g[3];
+  float2* RA;
+  float2* RB;
+  float2* SA;
+  double* partials;
+  const double* ky;
+  const uint8_t* step_flags;
+  kks_record* ring;
+  long long ring_cap;
+  kks_step_row* rows;
+  long long row_cap;
+  int N, nbx, part_rows, bulk_rows, bulk_cols, pad;
+};
+
+// Block map entry: x = cell, y = block within the cell (for the first column
+// pass: role << 16 | column tile).
+struct KksBatchLaunch {
+  const KksCellDesc* cells;
+  int n_cells;
+  int PX, PY;
+  const int2* map_rows;    // row pairs
+  const int2* map_cols;    // column tiles
+  const int2* map_cols3;   // column tiles x 3 roles (first column pass)
+  const int2* map_extras;  // blocks of the extras and restore kernels (nbx per cell)
+  int n_rows, n_cols, n_cols3, n_extras;
+  size_t smem_rows_a, smem_rows_bc, smem_rows_d, smem_cols_ab, smem_cols_cd1, smem_cols_cd2;
+};
+
+// Fill the block maps' sizes and the passes' shared memory for cells of the
+// given grids (host; the maps themselves are built by the caller in the order
+// of its choice) and raise the kernels' shared-memory limits to match.
+int kks_fft_batch_prepare(KksBatchLaunch& B, const int* nx, const int* ny, int n);
+// Row-pair blocks, column tiles and column-pass roles of one cell.
+int kks_fft_col_blocks(int nyh);
+// prologue, fused passes, extras, decide and restore of one attempt of every cell
+void kks_fft_launch_attempt_batch(const KksBatchLaunch& B, cudaStream_t s);
+// batched scalar kernels (kks_scalar.cu)
+void kks_launch_prologue_batch(const KksCellDesc* cells, int n, cudaStream_t s);
+void kks_launch_decide_batch(const KksCellDesc* cells, int n, cudaStream_t s);

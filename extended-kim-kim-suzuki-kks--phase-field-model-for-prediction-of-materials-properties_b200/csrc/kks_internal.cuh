@@ -76,7 +76,8 @@ struct KksCtl {
   double t, t_s, t_b, ttime, Xv, dtime_s, D_0, Meta_0;
   double surf, surf_b, T_b;
   double E_prev, ts_prev, ed_sum, ed_comp;
-  int32_t ed_n, pad0;
+  int32_t ed_n;
+  int32_t parity;  // state buffer of the next attempt's input (flipped by every attempt that runs)
   double error_dtime_s;
   // residual terms of the last attempt of the current step (history row)
   double res[5];
@@ -87,6 +88,8 @@ struct KksCtl {
 struct KksPar {
   int32_t active, istep, iteration, surface;
   int32_t armed_write, armed_residual, minus_is_state, gm, gs, gb;
+  int32_t parity;  // state buffer of this attempt's input
+  int32_t pad_par;
   double T, D, Meta, L, Vm;
   double dt, L_s, kappa2_s, D_s, w_s;
   double A_alp_s, B_alp_s, C_alp_s, A_thet_s, B_thet_s, C_thet_s;

@@ -20,6 +20,7 @@
 #include <math.h>
 
 #include "kks_internal.cuh"
+#include "kks_fft.cuh"
 
 namespace {
 
@@ -100,8 +101,12 @@ __device__ void push_record(KksCtl* ctl, kks_record* ring, long long cap, const 
   ctl->n_rec += 1;
 }
 
-__global__ void kks_prologue(const KksConst* __restrict__ c, KksCtl* ctl, KksPar* par,
-                             const uint8_t* __restrict__ step_flags, kks_record* ring, long long ring_cap) {
+// An attempt that runs takes KksCtl::parity as its input buffer and flips it,
+// so the device always knows which buffer holds the current state (attempts
+// that do not run, after the target step or a stop, leave it alone).
+__device__ __forceinline__ void prologue_body(const KksConst* __restrict__ c, KksCtl* ctl, KksPar* par,
+                                              const uint8_t* __restrict__ step_flags, kks_record* ring,
+                                              long long ring_cap) {
   // one warp: lane 0 runs the scalar chain; the material tables are
   // interpolated at T by one lane each (same expressions, same roundings)
   __shared__ int s_go;
@@ -193,6 +198,9 @@ __global__ void kks_prologue(const KksConst* __restrict__ c, KksCtl* ctl, KksPar
   q.gm = ctl->gm;
   q.gs = ctl->gs;
   q.gb = ctl->gb;
+  q.parity = ctl->parity;
+  q.pad_par = 0;
+  ctl->parity = q.parity ^ 1;
   q.T = T; q.D = D; q.Meta = Meta; q.L = L; q.Vm = Omega0;
   q.dt = dtime_s;
   q.L_s = (L * C44 * dx2) / D_0;
@@ -227,13 +235,24 @@ __global__ void kks_prologue(const KksConst* __restrict__ c, KksCtl* ctl, KksPar
   ctl->attempts += 1;
 }
 
+__global__ void kks_prologue(const KksConst* __restrict__ c, KksCtl* ctl, KksPar* par,
+                             const uint8_t* __restrict__ step_flags, kks_record* ring, long long ring_cap) {
+  prologue_body(c, ctl, par, step_flags, ring, ring_cap);
+}
+
+// one warp per cell of a batch
+__global__ void kks_prologue_batch(const KksCellDesc* __restrict__ cells) {
+  const KksCellDesc& d = cells[blockIdx.x];
+  prologue_body(d.dc, d.ctl, d.par, d.step_flags, d.ring, d.ring_cap);
+}
+
 // The partial sums of all blocks are finished in a fixed order (deterministic).
 constexpr int kDecideWarps = 16;  // warps of the decide block (one row group each)
 static_assert(KKS_NPART == 32, "one lane per partial-sum slot");
 
-__global__ void __launch_bounds__(32 * kDecideWarps) kks_decide(const KksConst* __restrict__ c, KksCtl* ctl, const KksPar* __restrict__ par,
-                           const double* __restrict__ partials, int nblocks, kks_record* ring, long long ring_cap,
-                           kks_step_row* rows, long long row_cap) {
+__device__ __forceinline__ void decide_body(const KksConst* __restrict__ c, KksCtl* ctl, const KksPar* __restrict__ par,
+                                            const double* __restrict__ partials, int nblocks, kks_record* ring,
+                                            long long ring_cap, kks_step_row* rows, long long row_cap) {
   __shared__ double S[P_COUNT];
   __shared__ double G[kDecideWarps][KKS_NPART + 1];
   __shared__ KksConst sc;
@@ -442,6 +461,19 @@ __global__ void __launch_bounds__(32 * kDecideWarps) kks_decide(const KksConst* 
   ctl->res_valid = 0;
 }
 
+__global__ void __launch_bounds__(32 * kDecideWarps)
+    kks_decide(const KksConst* __restrict__ c, KksCtl* ctl, const KksPar* __restrict__ par,
+               const double* __restrict__ partials, int nblocks, kks_record* ring, long long ring_cap,
+               kks_step_row* rows, long long row_cap) {
+  decide_body(c, ctl, par, partials, nblocks, ring, ring_cap, rows, row_cap);
+}
+
+// one block per cell of a batch
+__global__ void __launch_bounds__(32 * kDecideWarps) kks_decide_batch(const KksCellDesc* __restrict__ cells) {
+  const KksCellDesc& d = cells[blockIdx.x];
+  decide_body(d.dc, d.ctl, d.par, d.partials, d.part_rows, d.ring, d.ring_cap, d.rows, d.row_cap);
+}
+
 }  // namespace
 
 void kks_launch_prologue(const KksConst* c, KksCtl* ctl, KksPar* par, const uint8_t* step_flags, kks_record* ring,
@@ -452,4 +484,12 @@ void kks_launch_prologue(const KksConst* c, KksCtl* ctl, KksPar* par, const uint
 void kks_launch_decide(const KksConst* c, KksCtl* ctl, const KksPar* par, const double* partials, int nblocks,
                        kks_record* ring, long long ring_cap, kks_step_row* rows, long long row_cap, cudaStream_t s) {
   kks_decide<<<1, 32 * kDecideWarps, 0, s>>>(c, ctl, par, partials, nblocks, ring, ring_cap, rows, row_cap);
+}
+
+void kks_launch_prologue_batch(const KksCellDesc* cells, int n, cudaStream_t s) {
+  kks_prologue_batch<<<n, 32, 0, s>>>(cells);
+}
+
+void kks_launch_decide_batch(const KksCellDesc* cells, int n, cudaStream_t s) {
+  kks_decide_batch<<<n, 32 * kDecideWarps, 0, s>>>(cells);
 }

@@ -52,7 +52,7 @@ EXPORTS = (
     "kks_state_sums_noalloc", "kks_run_many", "kks_pipeline",
     "kks_adj_create", "kks_adj_forward", "kks_adj_backward", "kks_adj_destroy",
     "kks_voronoi_edges", "kks_generate_fields", "kks_place_precipitates", "kks_add_nuclei", "kks_count_below",
-    "kks_insert_nuclei",
+    "kks_insert_nuclei", "kks_batch_create", "kks_batch_run", "kks_batch_timing", "kks_batch_destroy",
 )
 
 
@@ -154,6 +154,12 @@ def load(path=LIB_PATH):
     lib.kks_destroy.argtypes = [vp]
     lib.kks_run_many.argtypes = [P(vp), ctypes.c_int32, P(ctypes.c_int32), P(ctypes.c_int32)]
     lib.kks_run_many.restype = ctypes.c_int
+    lib.kks_batch_create.argtypes = [P(vp), ctypes.c_int32, P(vp)]
+    lib.kks_batch_run.argtypes = [vp, P(ctypes.c_int32), P(ctypes.c_int32)]
+    lib.kks_batch_timing.argtypes = [vp, dp, P(ctypes.c_int64)]
+    lib.kks_batch_destroy.argtypes = [vp]
+    for name in ("kks_batch_create", "kks_batch_run", "kks_batch_timing", "kks_batch_destroy"):
+        getattr(lib, name).restype = ctypes.c_int
     lib.kks_state_sums_noalloc.argtypes = [vp, vp, ctypes.c_int32, ctypes.c_int32, vp, vp]
     lib.kks_state_sums_noalloc.restype = ctypes.c_int
     i64p = P(ctypes.c_int64)

@@ -4,9 +4,13 @@ on one GPU.
 Cells of an ensemble (different sizes, seeds, heating rates) share nothing, so
 the multi-GPU layout is a partition of the cells over ranks, one process per
 GPU, with no collective inside the step; per-cell results are gathered on the
-host at the end. On one GPU the cells of a shard run as concurrent attempt
-graphs on their own streams (each cell keeps its own adaptive dt, rejection and
-device loop state), so small grids that cannot fill 148 SMs alone overlap.
+host at the end. On one GPU the cells of a shard advance as one batch
+(``kks_batch_run``): every kernel of an attempt is launched once for all cells
+over their device descriptors, one CUDA graph per batch attempt, while each
+cell keeps its own adaptive dt, rejections, step target and buffer parity on
+the device. Cells that cannot share a batch (the cuFFT or FP64 pipelines, or
+different large prime factors) run as concurrent attempt graphs on their own
+streams (``kks_run_many``).
 """
 
 import math
@@ -60,13 +64,18 @@ def gather_results(local, group=None):
 
 
 class Ensemble:
-    """Cells of one shard resident on one GPU, advanced together by
-    ``kks_run_many`` (each cell on its own stream with its own graphs, one host
-    synchronisation per batch for all of them)."""
+    """Cells of one shard resident on one GPU, advanced together.
 
-    def __init__(self, members, precision="mixed", device=0):
+    ``batched``: None (default) batches the cells when they allow it and
+    otherwise runs them on their own streams; True requires the batch (raises
+    if the cells cannot share one); False always uses the per-cell streams.
+    ``mode`` tells which one is in use ("batch" or "streams").
+    """
+
+    def __init__(self, members, precision="mixed", device=0, batched=None):
         import ctypes
 
+        from . import _lib as L
         from .materials import MaterialTables
         from .solver import Cell
 
@@ -78,20 +87,55 @@ class Ensemble:
             self.cells.append(c)
         self._ptrs = (ctypes.c_void_p * len(self.cells))(*[c.h.value for c in self.cells])
         self.points = [c.N for c in self.cells]
+        self.batch = None
+        self.mode = "streams"
+        if batched is not False and self.cells:
+            b = ctypes.c_void_p()
+            rc = L.load().kks_batch_create(self._ptrs, len(self.cells), ctypes.byref(b))
+            if rc == L.KKS_OK:
+                self.batch = b
+                self.mode = "batch"
+            elif batched:
+                L.check(rc, "kks_batch_create")
 
     def run(self, n_steps):
-        """Advance every cell by ``n_steps`` steps; returns the status per cell."""
+        """Advance every cell by ``n_steps`` steps (an int, or one count per
+        cell); returns the status per cell."""
+        if self.batch is not None:
+            return self._call("kks_batch_run", (self.batch,), n_steps)
+        return self.run_streams(n_steps)
+
+    def run_streams(self, n_steps):
+        """The same steps with every cell on its own stream (``kks_run_many``)."""
+        return self._call("kks_run_many", (self._ptrs, len(self.cells)), n_steps)
+
+    def _call(self, fn, head, n_steps):
         import ctypes
 
         from . import _lib as L
 
         n = len(self.cells)
-        steps = (ctypes.c_int32 * n)(*([int(n_steps)] * n))
+        counts = [int(n_steps)] * n if np.isscalar(n_steps) else [int(k) for k in n_steps]
+        if len(counts) != n:
+            raise ValueError(f"{len(counts)} step counts for {n} cells")
+        steps = (ctypes.c_int32 * n)(*counts)
         status = (ctypes.c_int32 * n)()
-        L.check(L.load().kks_run_many(self._ptrs, n, steps, status), "kks_run_many")
+        L.check(getattr(L.load(), fn)(*head, steps, status), fn)
         for c in self.cells:
             c.drain()
         return list(status)
+
+    def batch_timing(self):
+        """(device ms, batch attempts) of all batched runs so far."""
+        import ctypes
+
+        from . import _lib as L
+
+        if self.batch is None:
+            return 0.0, 0
+        ms, att = ctypes.c_double(), ctypes.c_int64()
+        L.check(L.load().kks_batch_timing(self.batch, ctypes.byref(ms), ctypes.byref(att)), "kks_batch_timing")
+        return ms.value, att.value
 
     def run_sequential(self, n_steps):
         """The same steps, one cell after the other (the comparison baseline)."""
@@ -102,6 +146,11 @@ class Ensemble:
         return out
 
     def close(self):
+        if self.batch is not None:
+            from . import _lib as L
+
+            L.check(L.load().kks_batch_destroy(self.batch), "kks_batch_destroy")
+            self.batch = None
         for c in self.cells:
             c.close()
         self.cells = []

@@ -146,6 +146,24 @@ int kks_run(kks_handle* h, int32_t n_steps, int32_t* status);
  * Replaces running pf_kks.solver.run (pf_kks/solver.py:76-414) once per cell. */
 int kks_run_many(kks_handle** cells, int32_t n_cells, const int32_t* n_steps, int32_t* status);
 
+/* A batch: cells of one device (KKS_PRECISION_MIXED on the shared-memory FFT
+ * pipeline, all with the same large prime factor per axis, e.g. any mix of
+ * 128..512 power-of-two / 3*2^k sides) advanced together. One attempt of the
+ * batch launches every kernel once for all cells over the cells' device
+ * descriptors (one CUDA graph); each cell keeps its own adaptive dt,
+ * rejections, step target and buffer parity on the device, so cells of
+ * different size, seed and schedule advance in lockstep and a cell that has
+ * reached its target sits out. Results equal kks_run of each cell.
+ * The cells must outlive the batch. Replaces running pf_kks.solver.run
+ * (pf_kks/solver.py:76-414) once per instance. */
+typedef struct kks_batch kks_batch;
+int kks_batch_create(kks_handle* const* cells, int32_t n_cells, kks_batch** out);
+/* Advance cell i by n_steps[i] steps; status[i] receives KKS_STATUS_*. */
+int kks_batch_run(kks_batch* b, const int32_t* n_steps, int32_t* status);
+/* Device time of all kks_batch_run calls (CUDA events) and batch attempts launched. */
+int kks_batch_timing(const kks_batch* b, double* device_ms, int64_t* attempts);
+int kks_batch_destroy(kks_batch* b);
+
 /* Copy the log records and history rows produced since the last drain. */
 int kks_drain(kks_handle* h, kks_record* records, int64_t record_cap, int64_t* n_records, kks_step_row* rows,
               int64_t row_cap, int64_t* n_rows);

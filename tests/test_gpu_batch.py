@@ -1,0 +1,171 @@
+"""Batched ensembles (``kks_batch_*``): the cells of a batch advance by one
+launch per kernel for all of them, with each cell's dt, rejections, step
+target and buffer parity on the device. Each cell runs the same kernels on
+the same data in the same order as when it runs alone (``kks_run``), so the
+batch must reproduce the single-cell results bit for bit: fields, history
+rows, log records and status, for cells of different sizes, seeds and
+schedules, step counts that differ per cell, adaptive cells that reject and a
+cell that stops with MAX_ITER.
+"""
+
+import ctypes
+
+import numpy as np
+import pytest
+
+from conftest import copy_state, small_config, three_precipitates
+
+pytestmark = pytest.mark.gpu
+
+
+def _members(relaxed):
+    from pf_kks_gpu import workloads
+    from pf_kks_gpu.generator import MicrostructureSpec
+
+    out = []
+    for k, (nx, ny, n) in enumerate([(128, 96, 30), (64, 64, 30), (96, 80, 30), (40, 50, 30)]):
+        cfg = workloads.base_config(nx=nx, ny=ny, n_steps=n, n_map_saves=2, n_surface_samples=6)
+        spec = MicrostructureSpec(nx, ny, n_cells=3, n_particles=max(3, nx * ny // 600), seed=20 + k)
+        out.append((cfg, workloads.initial_state(cfg, spec)))
+    # adaptive, armed from step 1 (accepts and enlarges; pf_kks tests' relaxed state)
+    cfg = small_config(n_steps=40, x_equilibrium=0.2, dtime_s=60, dtime_max=150, residual_min=7.6e-4)
+    out.append((cfg, relaxed))
+    # adaptive from sharp precipitates: rejects until max_iterations (status MAX_ITER)
+    cfg = small_config(n_steps=40, x_equilibrium=0.2)
+    out.append((cfg, three_precipitates(cfg)))
+    return out
+
+
+def _cell(cfg, state):
+    from pf_kks_gpu import solver
+    from pf_kks_gpu.materials import MaterialTables
+
+    tables = MaterialTables.from_npz(cfg.material_tables, cfg.c_gamma, cfg.c_eps0)
+    c = solver.Cell(cfg, tables, precision="mixed")
+    c.upload(*copy_state(state))
+    return c
+
+
+def _alone(members, plan):
+    """Each cell run alone through kks_run, in the given segments."""
+    out = []
+    for (cfg, state), segs in zip(members, plan):
+        c = _cell(cfg, state)
+        recs, rows, st = [], [], 0
+        for n in segs:
+            st = c.run(n)
+            r, w = c.drain()
+            recs += r
+            rows.append(w)
+        out.append((c.download(), [bytes(r) for r in recs], np.concatenate(rows), st, c.state().istep))
+        c.close()
+    return out
+
+
+def _batched(members, plan, single=None):
+    """All cells in one batch, the same segments as kks_batch_run calls;
+    ``single`` = (segment index, cell, steps): that cell also runs alone by
+    kks_run after that segment (the batch must pick up its new parity)."""
+    from pf_kks_gpu import _lib as L
+
+    cells = [_cell(cfg, state) for cfg, state in members]
+    lib = L.load()
+    ptrs = (ctypes.c_void_p * len(cells))(*[c.h.value for c in cells])
+    b = ctypes.c_void_p()
+    L.check(lib.kks_batch_create(ptrs, len(cells), ctypes.byref(b)), "kks_batch_create")
+    recs = [[] for _ in cells]
+    rows = [[] for _ in cells]
+    status = [0] * len(cells)
+    try:
+        for s in range(max(len(p) for p in plan)):
+            steps = (ctypes.c_int32 * len(cells))(*[p[s] if s < len(p) else 0 for p in plan])
+            st = (ctypes.c_int32 * len(cells))()
+            L.check(lib.kks_batch_run(b, steps, st), "kks_batch_run")
+            for i, c in enumerate(cells):
+                r, w = c.drain()
+                recs[i] += [bytes(x) for x in r]
+                rows[i].append(w)
+                status[i] = st[i]
+            if single is not None and single[0] == s:
+                _, i, n = single
+                status[i] = cells[i].run(n)
+                r, w = cells[i].drain()
+                recs[i] += [bytes(x) for x in r]
+                rows[i].append(w)
+        ms, att = ctypes.c_double(), ctypes.c_int64()
+        L.check(lib.kks_batch_timing(b, ctypes.byref(ms), ctypes.byref(att)), "kks_batch_timing")
+        assert att.value > 0 and ms.value > 0
+        out = [(c.download(), recs[i], np.concatenate(rows[i]), status[i], c.state().istep)
+               for i, c in enumerate(cells)]
+    finally:
+        L.check(lib.kks_batch_destroy(b), "kks_batch_destroy")
+        for c in cells:
+            c.close()
+    return out
+
+
+def _assert_same(got, ref):
+    for i, (g, r) in enumerate(zip(got, ref)):
+        for a, e in zip(g[0], r[0]):
+            np.testing.assert_array_equal(a, e, err_msg=f"cell {i}")
+        assert g[1] == r[1], f"cell {i}: log records differ"
+        np.testing.assert_array_equal(g[2], r[2], err_msg=f"cell {i}: history rows")
+        assert g[3] == r[3], f"cell {i}: status"
+        assert g[4] == r[4], f"cell {i}: step"
+
+
+def test_batch_equals_cells_run_alone(relaxed_state):
+    from pf_kks_gpu import _lib as L
+
+    members = _members(relaxed_state)
+    steps = [[30], [17], [25], [9], [40], [40]]
+    ref = _alone(members, steps)
+    got = _batched(members, steps)
+    _assert_same(got, ref)
+    assert ref[-1][3] == L.KKS_STATUS_MAX_ITER  # the abort case stops on the device
+    assert ref[-2][3] == L.KKS_STATUS_OK and ref[-2][4] == 40
+
+
+def test_batch_segments_and_single_cell_runs_in_between(relaxed_state):
+    """Several kks_batch_run calls, and a kks_run of one cell between two of
+    them (odd step count: the cell's buffer parity changes outside the batch)."""
+    members = _members(relaxed_state)[:5]
+    plan = [[7, 11, 12], [5, 0, 12], [3, 4, 5], [9, 0, 0], [13, 14, 13]]
+    # cell 1 runs 3 more steps alone after the first segment
+    alone_plan = [[7, 11, 12], [5, 3, 0, 12], [3, 4, 5], [9, 0, 0], [13, 14, 13]]
+    ref = _alone(members, alone_plan)
+    got = _batched(members, plan, single=(0, 1, 3))
+    _assert_same(got, ref)
+
+
+def test_batch_rejects_cells_it_cannot_share():
+    from pf_kks_gpu import _lib as L
+    from pf_kks_gpu import solver, workloads
+    from pf_kks_gpu.materials import MaterialTables
+
+    cfg = workloads.base_config(nx=64, ny=64, n_steps=4, n_map_saves=2, n_surface_samples=2)
+    tables = MaterialTables.from_npz(cfg.material_tables, cfg.c_gamma, cfg.c_eps0)
+    a = solver.Cell(cfg, tables, precision="mixed")
+    f = solver.Cell(cfg, tables, precision="fp64")
+    lib = L.load()
+    b = ctypes.c_void_p()
+    for cells in ([a, f], [a, a]):
+        ptrs = (ctypes.c_void_p * 2)(*[c.h.value for c in cells])
+        assert lib.kks_batch_create(ptrs, 2, ctypes.byref(b)) != L.KKS_OK
+    a.close()
+    f.close()
+
+
+def test_ensemble_runs_as_one_batch(relaxed_state):
+    from pf_kks_gpu.ensemble import Ensemble
+
+    ens = Ensemble(_members(relaxed_state)[:3], precision="mixed")
+    try:
+        assert ens.mode == "batch"
+        assert ens.run([4, 2, 3]) == [0, 0, 0]
+        assert [c.state().istep for c in ens.cells] == [4, 2, 3]
+        assert ens.run_streams(2) == [0, 0, 0]
+        assert [c.state().istep for c in ens.cells] == [6, 4, 5]
+        assert ens.batch_timing()[1] == 4
+    finally:
+        ens.close()
