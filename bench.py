@@ -200,7 +200,7 @@ def ensemble_leg(precision, device, steps, warmup):
     from pf_kks_gpu.ensemble import Ensemble
 
     members = [(cfg, workloads.initial_state(cfg, spec)) for cfg, spec in workloads.ensemble(48, 100000, precision)]
-    ens = Ensemble(members, precision=precision, device=device)
+    ens = Ensemble(members, precision=precision, device=device, tune=True)
     try:
         ens.run(warmup)
         ens.run_streams(warmup)
@@ -221,7 +221,8 @@ def ensemble_leg(precision, device, steps, warmup):
     finally:
         ens.close()
     out = {"cells": len(members), "points": int(sum(c.nx * c.ny for c, _ in members)), "steps": steps,
-           "mode": ens.mode, "cell_steps_per_s": batched, "streams_cell_steps_per_s": streams,
+           "mode": ens.mode, "launch_shapes": {f"{k[0]}x{k[1]}": v for k, v in sorted(ens.shapes.items())},
+           "cell_steps_per_s": batched, "streams_cell_steps_per_s": streams,
            "sequential_cell_steps_per_s": sequential, "speedup_vs_streams": batched / streams,
            "speedup_vs_sequential": batched / sequential,
            "timing": "host wall clock around each run call (one host sync per batch of attempts)"}
@@ -317,6 +318,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
     ap.add_argument("--precision", default="mixed", choices=("mixed", "mixed-cufft", "fp64"))
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the default launch shape instead of the autotuner's choice")
+    ap.add_argument("--shape", default=None,
+                    help="explicit launch shape pipeline,cols,field_blocks (skips the autotuner)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the 48-cell ensemble leg")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint (gradient) leg")
@@ -364,8 +369,18 @@ def main():
         return float(t.item())
 
     cell = solver.Cell(cfg, tables, precision=args.precision, device=local_rank)
-    fused, kernels_per_attempt = cell.pipeline()
     cell.upload(*state)
+    # launch shape: the autotuner's choice, timed on this cell's own state
+    # (restored afterwards), outside the timed region
+    tuned = None
+    if args.shape:
+        cell.set_launch_shape(*[int(v) for v in args.shape.split(",")])
+    elif not args.no_autotune and not args.only_timed:
+        from pf_kks_gpu import autotune
+
+        tuned = autotune.tune(cell, attempts=20, device=local_rank, cache=False)
+    shape = cell.launch_shape()
+    fused, kernels_per_attempt = cell.pipeline()
     cell.run(args.warmup)
     cell.drain()
     s0 = cell.state()
@@ -390,6 +405,10 @@ def main():
     if args.precision != "fp64" and not args.only_timed:
         c64 = solver.Cell(cfg, tables, precision="fp64", device=local_rank)
         c64.upload(*state)
+        if not args.no_autotune:
+            from pf_kks_gpu import autotune
+
+            autotune.tune(c64, attempts=10, device=local_rank, cache=False)
         c64.run(args.warmup)
         m0, _ = c64.timing()
         k64 = max(10, args.steps // 4)
@@ -415,6 +434,7 @@ def main():
     for k in range(4):
         pinned[k][:] = state[k].ravel()
     e2e_cell = solver.Cell(cfg, tables, precision=args.precision, device=local_rank)
+    e2e_cell.set_launch_shape(shape["pipeline"], shape["cols"], shape["field_blocks"])
     e2e_cell.upload(*[pinned[k] for k in range(4)])
     e2e_cell.run(args.warmup)
     e2e_cell.drain()
@@ -457,7 +477,10 @@ def main():
         "vs_baseline": None,
         "dtype": "f64" if args.precision == "fp64" else "f32+f64",
         "data": "synthetic",
-        "config": bench_config(args.precision, armed, attempts),
+        "config": dict(bench_config(args.precision, armed, attempts), launch_shape=shape,
+                       autotune=(None if tuned is None else {"ms_per_attempt": tuned["ms_per_attempt"],
+                                                            "note": "fastest of the candidate shapes, "
+                                                                    "timed on the cell before the run"})),
         "cell_updates_per_s": value * N,
         "fp64_steps_per_s": fp64,
         "mixed_over_fp64": (value / world / fp64) if fp64 else None,

@@ -71,7 +71,10 @@ struct kks_handle {
   void* arena = nullptr;
   size_t arena_bytes = 0, state_bytes = 0;
   KksFieldPtrs f{};
-  int nblocks = 0;
+  int nblocks = 0;      // grid of the grid-stride field kernels (a launch shape)
+  int nblocks_cap = 0;  // largest grid the partial-sum buffers hold
+  int nsm = 148;
+  int in_batch = 0;     // batches that hold this cell (its launch shape is then fixed)
   cufftHandle plan_r2c3 = 0, plan_c2r3 = 0, plan_c2r2 = 0;
   bool plans_made = false;
   void* fft_work = nullptr;
@@ -86,12 +89,14 @@ struct kks_handle {
   long long timed_attempts = 0;
   long long attempts_launched = 0;
   // shared-memory FFT pipeline of the mixed path (kks_fft.cu)
-  bool fused = false;
+  bool fused = false;     // the attempt runs the fused passes (KKS_PRECISION_MIXED)
+  bool fused_ok = false;  // the fused passes are set up for this cell
   void* fft_arena = nullptr;
   KksFftConst* d_fc = nullptr;
   KksFftLaunch fl{};
   double* partials_fused = nullptr;
-  int nb_fused = 0;
+  int nb_fused = 0;        // partial-sum rows of the current launch shape
+  int part_cap_fused = 0;  // rows allocated
   // initial state on the device (kks_init.cu): chunk counts and offsets of the
   // ordered selection, and a per-call buffer for particles and ranks
   long long* sel = nullptr;
@@ -285,6 +290,11 @@ static int upload_vec(const std::vector<T>& v, T** dst) {
   return KKS_OK;
 }
 
+// Partial-sum rows the fused attempt writes under the cell's launch shape.
+static int fused_rows(const kks_handle* h) {
+  return std::max(std::max(kks_fft_row_blocks(h->hc.nx), kks_fft_col_blocks(h->hc.nyh, h->fl.cols)), h->nblocks);
+}
+
 static int setup_fused(kks_handle* h, const std::vector<double>& kx) {
   KksConst& c = h->hc;
   KksFftConst fc;
@@ -293,7 +303,8 @@ static int setup_fused(kks_handle* h, const std::vector<double>& kx) {
   if (!build_axis(c.nx, fc.ax, tx) || !build_axis(c.ny, fc.ay, ty)) return KKS_OK;  // not supported: cuFFT
   int optin = 0;
   CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device));
-  if (kks_fft_smem_bytes(c.nx, c.ny) > (size_t)optin) return KKS_OK;
+  if (kks_fft_smem_bytes(c.nx, c.ny, KKS_FFT_COLS) > (size_t)optin) return KKS_OK;
+  fc.cols = KKS_FFT_COLS;
   std::vector<float> kx_slot(c.nx);
   for (int k = 0; k < c.nx; ++k) kx_slot[tx.slot[k]] = (float)kx[k];
   // device tables and buffers in one allocation
@@ -345,6 +356,7 @@ static int setup_fused(kks_handle* h, const std::vector<double>& kx) {
   L.ny = c.ny;
   L.nyh = c.nyh;
   L.nbx = h->nblocks;
+  L.cols = fc.cols;
   L.PX = fc.ax.P;
   L.PY = fc.ay.P;
   // bulk copies of whole row pairs need 16-byte multiples for the f32 rows, the
@@ -358,11 +370,14 @@ static int setup_fused(kks_handle* h, const std::vector<double>& kx) {
   if (kks_fft_set_attributes(L) != 0) return set_error(KKS_ERR_CUDA, "fft kernel attributes");
   // every kernel of the pipeline writes one partial-sum row per block: the
   // buffer holds the largest grid of them (row pairs, column tiles, extras)
-  h->nb_fused = std::max(kks_fft_partial_rows(c.nx, c.ny, L.nbx), h->nblocks);
-  CK(cudaMalloc(&h->partials_fused, (size_t)h->nb_fused * KKS_NPART * sizeof(double)));
-  CK(cudaMemset(h->partials_fused, 0, (size_t)h->nb_fused * KKS_NPART * sizeof(double)));
+  // under any launch shape; the decide kernel reads the rows of the current one
+  h->part_cap_fused = std::max(kks_fft_partial_rows(c.nx, c.ny, h->nblocks_cap), h->nblocks_cap);
+  h->nb_fused = fused_rows(h);
+  CK(cudaMalloc(&h->partials_fused, (size_t)h->part_cap_fused * KKS_NPART * sizeof(double)));
+  CK(cudaMemset(h->partials_fused, 0, (size_t)h->part_cap_fused * KKS_NPART * sizeof(double)));
   h->f.partials = h->partials_fused;
   h->fused = true;
+  h->fused_ok = true;
   return KKS_OK;
 }
 
@@ -474,7 +489,9 @@ static int create_impl(kks_handle* h, const kks_params* prm, int32_t n_steps, co
 
   int nsm = 148;
   CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device));
+  h->nsm = nsm;
   h->nblocks = kks_field_blocks(c.N, nsm);
+  h->nblocks_cap = kks_field_blocks(c.N, 2 * nsm);  // up to 8 blocks per SM
 
   // arena (layout in kks_internal.cuh)
   const bool mixed = h->precision != KKS_PRECISION_FP64;
@@ -484,7 +501,7 @@ static int create_impl(kks_handle* h, const kks_params* prm, int32_t n_steps, co
   const size_t sz_fin = mixed ? 3 * Np * R : 0;
   const size_t sz_spec_a = 3 * NCp * 2 * R, sz_real_b = 3 * Np * R, sz_real_c = 3 * Np * R,
                sz_spec_bcd = 5 * NCp * 2 * R, sz_one = Np * R;
-  const size_t sz_part = round_up((size_t)h->nblocks * KKS_NPART * sizeof(double), 256);
+  const size_t sz_part = round_up((size_t)h->nblocks_cap * KKS_NPART * sizeof(double), 256);
   size_t total = 2 * sz_state + sz_fin + sz_spec_a + sz_real_b + sz_real_c + sz_spec_bcd + 2 * Np * D + 4 * sz_one +
                  sz_part;
   CK(cudaMalloc(&h->arena, total));
@@ -857,11 +874,12 @@ static int batch_create_impl(kks_batch* b) {
   CK(cudaEventCreate(&b->ev1));
   CK(cudaMallocHost(&b->h_stage, n * sizeof(int32_t)));
   std::vector<KksCellDesc> desc(n);
-  std::vector<int> nx(n), ny(n);
+  std::vector<int> nx(n), ny(n), tile(n);
   for (int i = 0; i < n; ++i) {
     fill_desc(desc[i], b->cells[i]);
     nx[i] = b->cells[i]->hc.nx;
     ny[i] = b->cells[i]->hc.ny;
+    tile[i] = b->cells[i]->fl.cols;
   }
   // largest cells first, so that the small ones fill the last wave of a pass
   std::vector<int> order(n);
@@ -870,7 +888,7 @@ static int batch_create_impl(kks_batch* b) {
                    [&](int a, int c) { return b->cells[a]->hc.N > b->cells[c]->hc.N; });
   std::vector<int2> rows, cols, cols3, extras;
   for (int i : order) {
-    const int nr = kks_fft_row_blocks(nx[i]), nc = kks_fft_col_blocks(ny[i] / 2 + 1);
+    const int nr = kks_fft_row_blocks(nx[i]), nc = kks_fft_col_blocks(ny[i] / 2 + 1, tile[i]);
     for (int k = 0; k < nr; ++k) rows.push_back(make_int2(i, k));
     for (int k = 0; k < nc; ++k) cols.push_back(make_int2(i, k));
     for (int r = 0; r < 3; ++r)
@@ -899,7 +917,7 @@ static int batch_create_impl(kks_batch* b) {
     m += v->size();
   }
   L.cells = b->d_cells;
-  if (kks_fft_batch_prepare(L, nx.data(), ny.data(), n) != 0)
+  if (kks_fft_batch_prepare(L, nx.data(), ny.data(), tile.data(), n) != 0)
     return set_error(KKS_ERR_CUDA, "batched fft kernel attributes");
   b->max_batch = 1LL << 30;
   for (kks_handle* h : b->cells)
@@ -945,6 +963,7 @@ int kks_batch_create(kks_handle* const* cells, int32_t n_cells, kks_batch** out)
     g_last_error = msg;
     return rc;
   }
+  for (kks_handle* h : b->cells) h->in_batch += 1;
   *out = b;
   return KKS_OK;
 }
@@ -1014,6 +1033,7 @@ int kks_batch_timing(const kks_batch* b, double* device_ms, int64_t* attempts) {
 int kks_batch_destroy(kks_batch* b) {
   if (!b) return KKS_OK;
   CK(cudaSetDevice(b->device));
+  for (kks_handle* h : b->cells) h->in_batch -= 1;
   free_batch(b);
   return KKS_OK;
 }
@@ -1392,6 +1412,151 @@ int kks_restore(kks_handle* h, const void* buf, size_t size) {
   return KKS_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Launch shapes and the autotuner.
+
+static int apply_shape(kks_handle* h, const kks_launch_shape& s) {
+  if (h->in_batch) return set_error(KKS_ERR_STATE, "the cell belongs to a batch: its launch shape is fixed");
+  if (s.pipeline != 0 && s.pipeline != 1) return set_error(KKS_ERR_ARG, "pipeline must be 0 (cuFFT) or 1 (fused)");
+  if (s.pipeline == 1 && !h->fused_ok)
+    return set_error(KKS_ERR_ARG, "the fused passes are not available for this cell (precision or size)");
+  if (s.field_blocks < 1 || s.field_blocks > h->nblocks_cap)
+    return set_error(KKS_ERR_ARG, "field_blocks out of range (1 .. " + std::to_string(h->nblocks_cap) + ")");
+  if (h->fused_ok) {
+    if (s.cols < 1 || s.cols > KKS_FFT_COLS_MAX) return set_error(KKS_ERR_ARG, "cols out of range (1 .. 4)");
+    int optin = 0;
+    CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device));
+    if (kks_fft_smem_bytes(h->hc.nx, h->hc.ny, s.cols) > (size_t)optin)
+      return set_error(KKS_ERR_CAPACITY, "column tile does not fit shared memory");
+  }
+  CK(cudaSetDevice(h->device));
+  CK(cudaStreamSynchronize(h->stream));
+  for (int p = 0; p < 2; ++p) {
+    if (h->graph[p]) cudaGraphExecDestroy(h->graph[p]);
+    h->graph[p] = nullptr;
+  }
+  h->fused = s.pipeline == 1;
+  h->nblocks = s.field_blocks;
+  size_t rows = (size_t)h->nblocks_cap;
+  if (h->fused_ok) {
+    h->fl.cols = s.cols;
+    h->fl.nbx = h->nblocks;
+    CK(cudaMemcpy(&h->d_fc->cols, &h->fl.cols, sizeof(int), cudaMemcpyHostToDevice));
+    if (kks_fft_set_attributes(h->fl) != 0) return set_error(KKS_ERR_CUDA, "fft kernel attributes");
+    h->nb_fused = fused_rows(h);
+    rows = (size_t)h->part_cap_fused;
+  }
+  // rows that the new shape does not write must read as zero
+  CK(cudaMemset(h->f.partials, 0, rows * KKS_NPART * sizeof(double)));
+  return capture_graphs(h);
+}
+
+static void current_shape(const kks_handle* h, kks_launch_shape* s) {
+  s->pipeline = h->fused ? 1 : 0;
+  s->cols = h->fused_ok ? h->fl.cols : 0;
+  s->field_blocks = h->nblocks;
+  s->pad = 0;
+}
+
+int kks_get_launch_shape(const kks_handle* h, kks_launch_shape* shape) {
+  if (!h || !shape) return set_error(KKS_ERR_ARG, "null argument");
+  current_shape(h, shape);
+  return KKS_OK;
+}
+
+int kks_set_launch_shape(kks_handle* h, const kks_launch_shape* shape) {
+  if (!h || !shape) return set_error(KKS_ERR_ARG, "null argument");
+  return apply_shape(h, *shape);
+}
+
+// Candidates: the field-kernel grid at 1, 2, 4 and 8 blocks per SM (as far as
+// the cell has points for), crossed with the column tiles 1..4 of the fused
+// passes, and the cuFFT passes (unless only batchable shapes are wanted).
+static std::vector<kks_launch_shape> candidate_shapes(const kks_handle* h, bool batchable) {
+  std::vector<int> grids;
+  for (int m : {1, 2, 4, 8}) {
+    const int g = std::min(m * h->nsm, h->nblocks_cap);
+    if (std::find(grids.begin(), grids.end(), g) == grids.end()) grids.push_back(g);
+  }
+  std::vector<kks_launch_shape> out;
+  for (int g : grids) {
+    if (h->fused_ok)
+      for (int cols = 1; cols <= KKS_FFT_COLS_MAX; ++cols) out.push_back({1, cols, g, 0});
+    if (!(batchable && h->fused_ok)) out.push_back({0, h->fused_ok ? h->fl.cols : 0, g, 0});
+  }
+  return out;
+}
+
+int kks_autotune(kks_handle* h, int32_t attempts, int32_t flags, kks_launch_shape* best,
+                 double* best_ms_per_attempt) {
+  if (!h || attempts < 1 || (flags & ~KKS_TUNE_BATCHABLE)) return set_error(KKS_ERR_ARG, "bad argument");
+  if (!h->uploaded) return set_error(KKS_ERR_STATE, "kks_autotune before kks_upload");
+  if (h->in_batch) return set_error(KKS_ERR_STATE, "the cell belongs to a batch: its launch shape is fixed");
+  CK(cudaSetDevice(h->device));
+  CK(cudaStreamSynchronize(h->stream));
+  const KksCtl* c = h->h_ctl;
+  if (c->status != KKS_STATUS_OK) return set_error(KKS_ERR_STATE, "the cell has stopped");
+  const long long left = (long long)h->hc.n_steps - c->istep;
+  const int warm = (int)std::min<long long>(3, left / 4);
+  const int timed = (int)std::min<long long>(attempts, left - warm);
+  if (timed < 1 || left < 2) return set_error(KKS_ERR_STATE, "too few scheduled steps left to time an attempt");
+  // everything an attempt changes, saved and put back after every candidate
+  size_t size = 0;
+  int rc = kks_checkpoint(h, nullptr, 0, &size);
+  if (rc != KKS_OK) return rc;
+  std::vector<char> blob(size);
+  if ((rc = kks_checkpoint(h, blob.data(), size, &size)) != KKS_OK) return rc;
+  const std::vector<kks_record> recs = h->recs;
+  const std::vector<kks_step_row> rows = h->rows;
+  const long long rec_read = h->rec_read, row_read = h->row_read, launched = h->attempts_launched;
+  const long long timed_attempts = h->timed_attempts;
+  const double device_ms = h->device_ms;
+  kks_launch_shape start;
+  current_shape(h, &start);
+  kks_launch_shape win = start;
+  double win_ms = -1.0;
+  const int32_t target = c->istep + warm + timed;
+  for (const kks_launch_shape& cand : candidate_shapes(h, (flags & KKS_TUNE_BATCHABLE) != 0)) {
+    if (apply_shape(h, cand) != KKS_OK) continue;  // e.g. a tile that does not fit
+    if ((rc = kks_restore(h, blob.data(), size)) != KKS_OK) return rc;
+    *h->h_target = target;
+    CK(cudaMemcpyAsync(&h->d_ctl->target_step, h->h_target, sizeof(int32_t), cudaMemcpyHostToDevice, h->stream));
+    for (int a = 0; a < warm; ++a) {
+      CK(cudaGraphLaunch(h->graph[h->parity], h->stream));
+      h->parity ^= 1;
+    }
+    CK(cudaEventRecord(h->ev0, h->stream));
+    for (int a = 0; a < timed; ++a) {
+      CK(cudaGraphLaunch(h->graph[h->parity], h->stream));
+      h->parity ^= 1;
+    }
+    CK(cudaEventRecord(h->ev1, h->stream));
+    CK(cudaMemcpyAsync(h->h_ctl, h->d_ctl, sizeof(KksCtl), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaEventSynchronize(h->ev1));
+    CK(cudaStreamSynchronize(h->stream));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+    if (h->h_ctl->status != KKS_STATUS_OK) continue;  // a stop inside the trial: attempts did not all run
+    const double per = ms / timed;
+    if (win_ms < 0 || per < win_ms) {
+      win_ms = per;
+      win = cand;
+    }
+  }
+  if ((rc = apply_shape(h, win)) != KKS_OK) return rc;
+  if ((rc = kks_restore(h, blob.data(), size)) != KKS_OK) return rc;
+  h->recs = recs;
+  h->rows = rows;
+  h->rec_read = rec_read;
+  h->row_read = row_read;
+  h->attempts_launched = launched;
+  h->timed_attempts = timed_attempts;
+  h->device_ms = device_ms;
+  if (best) *best = win;
+  if (best_ms_per_attempt) *best_ms_per_attempt = win_ms;
+  return win_ms < 0 ? set_error(KKS_ERR_STATE, "no candidate shape completed its trial attempts") : KKS_OK;
+}
+
 int kks_timing(kks_handle* h, double* device_ms, int64_t* attempts) {
   if (!h) return set_error(KKS_ERR_ARG, "null handle");
   if (device_ms) *device_ms = h->device_ms;
@@ -1402,10 +1567,10 @@ int kks_timing(kks_handle* h, double* device_ms, int64_t* attempts) {
 int kks_pipeline(kks_handle* h, int32_t* fused, int32_t* kernels) {
   if (!h) return set_error(KKS_ERR_ARG, "null handle");
   if (fused) *fused = h->fused ? 1 : 0;
-  // fused: prologue, extras (old state), rows A, cols AB, rows BC, cols CD (2),
-  // rows D, extras (new state), decide, restore; cuFFT pipeline: prologue,
-  // prep, spectral_mid, pre_pointwise, spectral_update, post_pointwise,
-  // decide, restore
+  // fused: prologue, rows A, cols AB, rows BC, cols CD (2), rows D, extras
+  // (new state), decide, restore; cuFFT pipeline: prologue, prep,
+  // spectral_mid, pre_pointwise, spectral_update, post_pointwise, decide,
+  // restore
   if (kernels) *kernels = h->fused ? 10 : 8;
   return KKS_OK;
 }

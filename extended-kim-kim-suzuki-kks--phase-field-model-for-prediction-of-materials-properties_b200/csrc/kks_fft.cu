@@ -22,7 +22,8 @@
 // and the operation that consumes it. A row-pass block owns one pair of rows
 // (all fields of the pass), each field's pair transformed as one complex
 // sequence (row a + i row b) and split / merged with the Hermitian symmetry; a
-// column-pass block owns KKS_FFT_COLS adjacent y-frequency columns. A block has
+// column-pass block owns fc->cols adjacent y-frequency columns (a launch shape,
+// KKS_FFT_COLS unless tuned). A block has
 // ten warps for two to six sequences, so that every stage (butterflies, the
 // prime DFTs, loads and stores) has several warps of independent work. Spectra
 // between passes are column-major (x fastest): a column pass moves one
@@ -58,7 +59,6 @@
 namespace {
 
 constexpr int kThreads = KKS_FFT_THREADS;
-constexpr int kCols = KKS_FFT_COLS;
 // blocks per SM the register allocation must allow
 constexpr int kMinBlocks = 2;
 
@@ -654,7 +654,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
   rows_A_body<PY>(c, par, fc, eta, X, RA, partials, ctl, bulk, &map_RA, (int)blockIdx.x);
 }
 
-// pass 2: kCols adjacent y-frequency columns of RA. Role by: 0 eta -> keep
+// pass 2: fc->cols adjacent y-frequency columns of RA. Role by: 0 eta -> keep
 // FT(eta), i k_x FT(eta) and i k_y FT(eta) (one forward, two inverse
 // transforms); 1 eta^2 -> tr eps^ (+ Parseval sums); 2 X -> keep FT(X).
 template <int PX>
@@ -670,8 +670,9 @@ __device__ __forceinline__ void cols_AB_body(const KksConst* __restrict__ c, con
   const int nx = c->nx, ny = c->ny, nyh = c->nyh;
   const size_t fs = (size_t)nx * nyh;
   const int g = by;
-  const int ky0 = bx * kCols;
-  const int ncol = min(kCols, nyh - ky0);
+  const int cols = fc->cols;
+  const int ky0 = bx * cols;
+  const int ncol = min(cols, nyh - ky0);
   const int nv = ncol * nx;
   const int src_field = g == 0 ? 0 : (g == 1 ? 2 : 1);
   const float2* col = RA + src_field * fs + (size_t)ky0 * nx;
@@ -875,7 +876,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
   rows_BC_body<PY>(c, par, fc, RB, RC, eta, Xal, Xth, g0, g1, g2, partials, ctl, bulk, &map_RB, &map_RC, (int)blockIdx.x);
 }
 
-// pass 4a: kCols columns of FT(drive) with FT(eta) -> d_eta^ -> row spectra RD[0]
+// pass 4a: fc->cols columns of FT(drive) with FT(eta) -> d_eta^ -> row spectra RD[0]
 template <int PX>
 __device__ __forceinline__ void cols_CD_eta_body(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const KksFftConst* __restrict__ fc,
                    const float2* __restrict__ RC, const float2* __restrict__ SA, float2* __restrict__ RD,
@@ -887,12 +888,13 @@ __device__ __forceinline__ void cols_CD_eta_body(const KksConst* __restrict__ c,
   bulk = bulk && (smem_u32(sm) & 15u) == 0;  // bulk destinations need 16-byte alignment
   const KksFftAxis& ax = fc->ax;
   const int nx = c->nx, nyh = c->nyh;
-  const int ky0 = bx * kCols;
-  const int ncol = min(kCols, nyh - ky0);
+  const int cols = fc->cols;
+  const int ky0 = bx * cols;
+  const int ncol = min(cols, nyh - ky0);
   const int nv = ncol * nx;
   const float2* col = RC + (size_t)ky0 * nx;
   // FT(eta) of the same columns, staged during the forward FFT
-  float2* s_sa = (float2*)stage_base(sm, (uint32_t)(kCols * nx * sizeof(float2)));
+  float2* s_sa = (float2*)stage_base(sm, (uint32_t)(cols * nx * sizeof(float2)));
   if (bulk) {
     if (threadIdx.x == 0) {
       mbar_init(&bar);
@@ -940,7 +942,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
   cols_CD_eta_body<PX>(c, par, fc, RC, SA, RD, kys, ctl, bulk, (int)blockIdx.x);
 }
 
-// pass 4b: kCols columns of FT(flux_x), FT(flux_y) with FT(X) -> d_X^ -> row spectra RD[1]
+// pass 4b: fc->cols columns of FT(flux_x), FT(flux_y) with FT(X) -> d_X^ -> row spectra RD[1]
 template <int PX>
 __device__ __forceinline__ void cols_CD_X_body(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const KksFftConst* __restrict__ fc,
                  const float2* __restrict__ RC, const float2* __restrict__ SA, float2* __restrict__ RD,
@@ -953,14 +955,15 @@ __device__ __forceinline__ void cols_CD_X_body(const KksConst* __restrict__ c, c
   const KksFftAxis& ax = fc->ax;
   const int nx = c->nx, nyh = c->nyh;
   const size_t fs = (size_t)nx * nyh;
-  const int ky0 = bx * kCols;
-  const int ncol = min(kCols, nyh - ky0);
+  const int cols = fc->cols;
+  const int ky0 = bx * cols;
+  const int ncol = min(cols, nyh - ky0);
   const int nv = ncol * nx;
   // flux_x columns at [0, nv), flux_y columns at [nv, 2 nv); FT(X) of the same
   // columns staged during the forward FFT
   const float2* cx = RC + fs + (size_t)ky0 * nx;
   const float2* cy = RC + 2 * fs + (size_t)ky0 * nx;
-  float2* s_sa = (float2*)stage_base(sm, (uint32_t)(2 * kCols * nx * sizeof(float2)));
+  float2* s_sa = (float2*)stage_base(sm, (uint32_t)(2 * cols * nx * sizeof(float2)));
   if (bulk) {
     if (threadIdx.x == 0) {
       mbar_init(&bar);
@@ -1339,9 +1342,9 @@ inline size_t row_stage_bytes(int ny, int F) {
 inline size_t rows_a_smem(int ny) { return seq_smem(ny, 3) + row_stage_bytes(ny, 3); }
 inline size_t rows_bc_smem(int ny) { return seq_smem(ny, 3) + row_stage_bytes(ny, 3); }
 inline size_t rows_d_smem(int ny) { return seq_smem(ny, 2) + row_stage_bytes(ny, 2); }
-// column increment passes: m x kCols columns, and kCols staged SA columns
-inline size_t cols_cd_smem(int nx, int m) { return seq_smem(nx, m * kCols) + 128 + seq_smem(nx, kCols); }
-inline int col_blocks(int nyh) { return (nyh + kCols - 1) / kCols; }
+// column increment passes: m x cols columns, and cols staged SA columns
+inline size_t cols_cd_smem(int nx, int m, int cols) { return seq_smem(nx, m * cols) + 128 + seq_smem(nx, cols); }
+inline int col_blocks(int nyh, int cols) { return (nyh + cols - 1) / cols; }
 
 template <int PY>
 void launch_rows(const KksFftLaunch& L, int p, int stage, cudaStream_t s) {
@@ -1373,15 +1376,15 @@ void launch_cols(const KksFftLaunch& L, int stage, cudaStream_t s) {
   float2* RA = (float2*)L.RA;
   float2* RB = (float2*)L.RB;
   float2* SA = (float2*)L.SA;
-  const int nb = col_blocks(L.nyh);
+  const int nb = col_blocks(L.nyh, L.cols);
   if (stage == 0) {
-    kf_cols_AB<PX><<<dim3(nb, 3), kThreads, seq_smem(L.nx, 2 * kCols), s>>>(
+    kf_cols_AB<PX><<<dim3(nb, 3), kThreads, seq_smem(L.nx, 2 * L.cols), s>>>(
         L.dc, L.par, L.fc, RA, SA, RB, L.f->ky, L.f->partials, L.ctl, L.bulk_cols);
   } else {
-    kf_cols_CD_eta<PX><<<nb, kThreads, cols_cd_smem(L.nx, 1), s>>>(L.dc, L.par, L.fc, RA, SA, RB, L.f->ky, L.ctl,
-                                                                    L.bulk_cols);
-    kf_cols_CD_X<PX><<<nb, kThreads, cols_cd_smem(L.nx, 2), s>>>(L.dc, L.par, L.fc, RA, SA, RB, L.f->ky, L.ctl,
-                                                                  L.bulk_cols);
+    kf_cols_CD_eta<PX><<<nb, kThreads, cols_cd_smem(L.nx, 1, L.cols), s>>>(L.dc, L.par, L.fc, RA, SA, RB, L.f->ky,
+                                                                            L.ctl, L.bulk_cols);
+    kf_cols_CD_X<PX><<<nb, kThreads, cols_cd_smem(L.nx, 2, L.cols), s>>>(L.dc, L.par, L.fc, RA, SA, RB, L.f->ky,
+                                                                          L.ctl, L.bulk_cols);
   }
 }
 
@@ -1444,10 +1447,10 @@ int set_row_attrs(int ny) {
 }
 
 template <int PX>
-int set_col_attrs(int nx) {
-  cudaError_t e = set_attr(kf_cols_AB<PX>, seq_smem(nx, 2 * kCols));
-  if (e == cudaSuccess) e = set_attr(kf_cols_CD_eta<PX>, cols_cd_smem(nx, 1));
-  if (e == cudaSuccess) e = set_attr(kf_cols_CD_X<PX>, cols_cd_smem(nx, 2));
+int set_col_attrs(int nx, int cols) {
+  cudaError_t e = set_attr(kf_cols_AB<PX>, seq_smem(nx, 2 * cols));
+  if (e == cudaSuccess) e = set_attr(kf_cols_CD_eta<PX>, cols_cd_smem(nx, 1, cols));
+  if (e == cudaSuccess) e = set_attr(kf_cols_CD_X<PX>, cols_cd_smem(nx, 2, cols));
   return (int)e;
 }
 
@@ -1476,9 +1479,9 @@ int prime_table(float2* t) {
 
 }  // namespace
 
-size_t kks_fft_smem_bytes(int nx, int ny) {
+size_t kks_fft_smem_bytes(int nx, int ny, int cols) {
   const size_t r = rows_bc_smem(ny) > rows_d_smem(ny) ? rows_bc_smem(ny) : rows_d_smem(ny);
-  const size_t c = cols_cd_smem(nx, 2);
+  const size_t c = std::max(cols_cd_smem(nx, 2, cols), seq_smem(nx, 2 * cols));
   return (r > c ? r : c) + 1024 + KKS_FFT_PRIME_TABLE_MAX * sizeof(float2);  // + reduction scratch and prime table
 }
 
@@ -1486,7 +1489,7 @@ int kks_fft_row_blocks(int nx) { return (nx + 1) / 2; }
 
 int kks_fft_partial_rows(int nx, int ny, int nbx) {
   int m = kks_fft_row_blocks(nx);
-  const int cb = col_blocks(ny / 2 + 1);  // the column pass that writes sums
+  const int cb = col_blocks(ny / 2 + 1, 1);  // the column pass that writes sums, at its finest tile
   if (cb > m) m = cb;
   return m > nbx ? m : nbx;
 }
@@ -1495,7 +1498,7 @@ int kks_fft_partial_rows(int nx, int ny, int nbx) {
 int kks_fft_set_attributes(const KksFftLaunch& L) {
   int rc = -1, rc2 = -1;
 #define KKS_ROWS_ATTR(P) rc = set_row_attrs<P>(L.ny)
-#define KKS_COLS_ATTR(P) rc2 = set_col_attrs<P>(L.nx)
+#define KKS_COLS_ATTR(P) rc2 = set_col_attrs<P>(L.nx, L.cols)
   KKS_FFT_DISPATCH(L.PY, KKS_ROWS_ATTR)
   KKS_FFT_DISPATCH(L.PX, KKS_COLS_ATTR)
 #undef KKS_ROWS_ATTR
@@ -1530,17 +1533,17 @@ void kks_fft_launch_attempt(const KksFftLaunch& L, int p, cudaStream_t s) {
                                        f.partials);
 }
 
-int kks_fft_col_blocks(int nyh) { return col_blocks(nyh); }
+int kks_fft_col_blocks(int nyh, int cols) { return col_blocks(nyh, cols); }
 
-int kks_fft_batch_prepare(KksBatchLaunch& B, const int* nx, const int* ny, int n) {
+int kks_fft_batch_prepare(KksBatchLaunch& B, const int* nx, const int* ny, const int* cols, int n) {
   size_t ra = 0, rbc = 0, rd = 0, cab = 0, ccd1 = 0, ccd2 = 0;
   for (int i = 0; i < n; ++i) {
     ra = std::max(ra, rows_a_smem(ny[i]));
     rbc = std::max(rbc, rows_bc_smem(ny[i]));
     rd = std::max(rd, rows_d_smem(ny[i]));
-    cab = std::max(cab, seq_smem(nx[i], 2 * kCols));
-    ccd1 = std::max(ccd1, cols_cd_smem(nx[i], 1));
-    ccd2 = std::max(ccd2, cols_cd_smem(nx[i], 2));
+    cab = std::max(cab, seq_smem(nx[i], 2 * cols[i]));
+    ccd1 = std::max(ccd1, cols_cd_smem(nx[i], 1, cols[i]));
+    ccd2 = std::max(ccd2, cols_cd_smem(nx[i], 2, cols[i]));
   }
   B.smem_rows_a = ra;
   B.smem_rows_bc = rbc;

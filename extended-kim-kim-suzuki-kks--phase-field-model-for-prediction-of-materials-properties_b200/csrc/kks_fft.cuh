@@ -10,7 +10,8 @@
 
 #define KKS_FFT_MAXST 16
 #define KKS_FFT_THREADS 320   // threads of every pass block (ten warps)
-#define KKS_FFT_COLS 3        // y-frequency columns per column-pass block
+#define KKS_FFT_COLS 3        // default y-frequency columns per column-pass block (a launch shape)
+#define KKS_FFT_COLS_MAX 4    // largest column tile a launch shape may choose
 #define KKS_FFT_MAXN 8192     // longest axis of the pipeline (shared memory and 32-bit index magic)
 
 // In-place mixed-radix transform of length n along one axis. Stage s has radix
@@ -34,6 +35,7 @@ struct KksFftConst {
   KksFftAxis ax;         // x axis (column passes)
   KksFftAxis ay;         // y axis (row passes)
   const float* kx_slot;  // k_x of the frequency held at each x slot after the DIF
+  int cols;              // y-frequency columns per column-pass block (1..KKS_FFT_COLS_MAX)
 };
 
 // Spectrum buffers are column-major: element (ix, ky) of field f at
@@ -50,6 +52,7 @@ struct KksFftLaunch {
   void* SA;  // 2 full spectra FT(eta), FT(X), x in DIF slot order
   int nx, ny, nyh;
   int nbx;   // grid of the pointwise extras kernel
+  int cols;  // y-frequency columns per column-pass block (the device copy is fc->cols)
   int PX, PY;
   int bulk_rows;  // 1: row passes move their spectra with tensor copies and stage their state
                   // rows with bulk copies (needs nx % 2 == 0, ny % 4 == 0 and encoded maps)
@@ -63,10 +66,11 @@ struct KksFftLaunch {
 // Largest prime factors with a direct DFT stage; other sizes use cuFFT.
 #define KKS_FFT_PRIMES {11, 19, 71}
 
-// Shared memory of the largest pass block for an nx x ny grid (bytes).
-size_t kks_fft_smem_bytes(int nx, int ny);
-// Blocks of a row pass, and the number of partial-sum rows the pipeline
-// writes (the decide kernel reduces them).
+// Shared memory of the largest pass block for an nx x ny grid with column
+// tiles of `cols` (bytes).
+size_t kks_fft_smem_bytes(int nx, int ny, int cols);
+// Blocks of a row pass, and an upper bound of the partial-sum rows the
+// pipeline writes with any column tile (the decide kernel reduces them).
 int kks_fft_row_blocks(int nx);
 int kks_fft_partial_rows(int nx, int ny, int nbx);
 int kks_fft_set_attributes(const KksFftLaunch& L);
@@ -130,9 +134,9 @@ struct KksBatchLaunch {
 // Fill the block maps' sizes and the passes' shared memory for cells of the
 // given grids (host; the maps themselves are built by the caller in the order
 // of its choice) and raise the kernels' shared-memory limits to match.
-int kks_fft_batch_prepare(KksBatchLaunch& B, const int* nx, const int* ny, int n);
-// Row-pair blocks, column tiles and column-pass roles of one cell.
-int kks_fft_col_blocks(int nyh);
+int kks_fft_batch_prepare(KksBatchLaunch& B, const int* nx, const int* ny, const int* cols, int n);
+// Column tiles of a column pass.
+int kks_fft_col_blocks(int nyh, int cols);
 // prologue, fused passes, extras, decide and restore of one attempt of every cell
 void kks_fft_launch_attempt_batch(const KksBatchLaunch& B, cudaStream_t s);
 // batched scalar kernels (kks_scalar.cu)

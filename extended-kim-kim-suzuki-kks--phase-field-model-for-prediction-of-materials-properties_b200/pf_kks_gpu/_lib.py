@@ -23,6 +23,7 @@ COEF_NAMES = ("dt", "L_s", "kappa2_s", "D_s", "w_s", "A_alp_s", "B_alp_s", "C_al
 KKS_PRECISION_FP64 = 0
 KKS_PRECISION_MIXED = 1
 KKS_PRECISION_MIXED_CUFFT = 2
+KKS_TUNE_BATCHABLE = 1
 KKS_MAX_SCHED = 64
 KKS_MAX_TABLE = 32
 KKS_NTAB = 13
@@ -53,7 +54,13 @@ EXPORTS = (
     "kks_adj_create", "kks_adj_forward", "kks_adj_backward", "kks_adj_destroy",
     "kks_voronoi_edges", "kks_generate_fields", "kks_place_precipitates", "kks_add_nuclei", "kks_count_below",
     "kks_insert_nuclei", "kks_batch_create", "kks_batch_run", "kks_batch_timing", "kks_batch_destroy",
+    "kks_get_launch_shape", "kks_set_launch_shape", "kks_autotune",
 )
+
+
+class KksLaunchShape(ctypes.Structure):
+    _fields_ = [("pipeline", ctypes.c_int32), ("cols", ctypes.c_int32), ("field_blocks", ctypes.c_int32),
+                ("pad", ctypes.c_int32)]
 
 
 class KksParams(ctypes.Structure):
@@ -158,7 +165,11 @@ def load(path=LIB_PATH):
     lib.kks_batch_run.argtypes = [vp, P(ctypes.c_int32), P(ctypes.c_int32)]
     lib.kks_batch_timing.argtypes = [vp, dp, P(ctypes.c_int64)]
     lib.kks_batch_destroy.argtypes = [vp]
-    for name in ("kks_batch_create", "kks_batch_run", "kks_batch_timing", "kks_batch_destroy"):
+    lib.kks_get_launch_shape.argtypes = [vp, P(KksLaunchShape)]
+    lib.kks_set_launch_shape.argtypes = [vp, P(KksLaunchShape)]
+    lib.kks_autotune.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, P(KksLaunchShape), dp]
+    for name in ("kks_batch_create", "kks_batch_run", "kks_batch_timing", "kks_batch_destroy",
+                 "kks_get_launch_shape", "kks_set_launch_shape", "kks_autotune"):
         getattr(lib, name).restype = ctypes.c_int
     lib.kks_state_sums_noalloc.argtypes = [vp, vp, ctypes.c_int32, ctypes.c_int32, vp, vp]
     lib.kks_state_sums_noalloc.restype = ctypes.c_int

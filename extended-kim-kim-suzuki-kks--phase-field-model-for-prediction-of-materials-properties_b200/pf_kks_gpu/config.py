@@ -30,11 +30,15 @@ class GpuOptions:
         cuFFT transforms).
     device : CUDA device ordinal.
     records_capacity : size of the device ring of per-attempt log records.
+    autotune : before the run, give the cell the fastest launch shape
+        (timed on the device on the initial state, then cached per GPU, grid
+        and precision; pf_kks_gpu.autotune).
     """
 
     precision: str = "fp64"
     device: int = 0
     records_capacity: int = 1 << 15
+    autotune: bool = False
 
     def __post_init__(self):
         if self.precision not in PRECISIONS:

@@ -70,9 +70,12 @@ class Ensemble:
     otherwise runs them on their own streams; True requires the batch (raises
     if the cells cannot share one); False always uses the per-cell streams.
     ``mode`` tells which one is in use ("batch" or "streams").
+    ``tune``: give the cells the autotuner's launch shape first, timed on the
+    first cell of every grid size (only shapes that can join a batch) and
+    applied to the others of that size; ``shapes`` holds the choices.
     """
 
-    def __init__(self, members, precision="mixed", device=0, batched=None):
+    def __init__(self, members, precision="mixed", device=0, batched=None, tune=False, tune_attempts=10):
         import ctypes
 
         from . import _lib as L
@@ -85,6 +88,17 @@ class Ensemble:
             c = Cell(cfg, tables, precision=precision, device=device)
             c.upload(*state)
             self.cells.append(c)
+        self.shapes = {}
+        if tune:
+            from . import autotune
+
+            for c in self.cells:
+                k = (c.nx, c.ny)
+                if k not in self.shapes:
+                    self.shapes[k] = autotune.tune(c, attempts=tune_attempts, device=device, cache=False,
+                                                   batchable=batched is not False)["shape"]
+                else:
+                    c.set_launch_shape(**self.shapes[k])
         self._ptrs = (ctypes.c_void_p * len(self.cells))(*[c.h.value for c in self.cells])
         self.points = [c.N for c in self.cells]
         self.batch = None

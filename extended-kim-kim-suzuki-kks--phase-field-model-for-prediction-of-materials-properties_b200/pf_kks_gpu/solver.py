@@ -215,6 +215,30 @@ class Cell:
         L.check(self.lib.kks_pipeline(self.h, ctypes.byref(fused), ctypes.byref(kernels)), "kks_pipeline")
         return bool(fused.value), int(kernels.value)
 
+    # -- launch shapes ------------------------------------------------------
+
+    def launch_shape(self):
+        """{"pipeline": 1 fused / 0 cuFFT, "cols": fused column tile,
+        "field_blocks": grid of the grid-stride kernels}."""
+        s = L.KksLaunchShape()
+        L.check(self.lib.kks_get_launch_shape(self.h, ctypes.byref(s)), "kks_get_launch_shape")
+        return {"pipeline": s.pipeline, "cols": s.cols, "field_blocks": s.field_blocks}
+
+    def set_launch_shape(self, pipeline, cols, field_blocks):
+        s = L.KksLaunchShape(int(pipeline), int(cols), int(field_blocks), 0)
+        L.check(self.lib.kks_set_launch_shape(self.h, ctypes.byref(s)), "kks_set_launch_shape")
+
+    def autotune(self, attempts=20, batchable=False):
+        """Time every candidate launch shape on the current state (restored
+        afterwards) and keep the fastest; returns (shape, ms per attempt).
+        ``batchable``: only shapes with which the cell can join a batch."""
+        s = L.KksLaunchShape()
+        ms = ctypes.c_double(0)
+        flags = L.KKS_TUNE_BATCHABLE if batchable else 0
+        L.check(self.lib.kks_autotune(self.h, int(attempts), flags, ctypes.byref(s), ctypes.byref(ms)),
+                "kks_autotune")
+        return {"pipeline": s.pipeline, "cols": s.cols, "field_blocks": s.field_blocks}, ms.value
+
     # -- initial state written on the device (no nx*ny host arrays) ---------
 
     def voronoi_edges(self, seeds):
@@ -409,6 +433,10 @@ def run(cfg, eta, X, X_al, X_th, out_dir=".", base_dir=".", write_logs=True, ver
     map_files = []
     try:
         cell.upload(eta, X, X_al, X_th)
+        if opts.autotune and nstep >= 2:
+            from . import autotune
+
+            autotune.tune(cell, device=device)
         stops = sorted(s for s in schedule.map_steps if 1 <= s <= nstep)
         if not stops or stops[-1] != nstep:
             stops.append(nstep)

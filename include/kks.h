@@ -164,6 +164,31 @@ int kks_batch_run(kks_batch* b, const int32_t* n_steps, int32_t* status);
 int kks_batch_timing(const kks_batch* b, double* device_ms, int64_t* attempts);
 int kks_batch_destroy(kks_batch* b);
 
+/* Launch shape of a cell's attempt. The mixed precision can run the fused
+ * shared-memory FFT passes or the cuFFT passes; the fused column passes take
+ * `cols` y-frequency columns per block; the grid-stride field kernels
+ * (interface / gradient sums, restore, the cuFFT pipeline's pointwise
+ * kernels) run `field_blocks` blocks. kks_create picks a default; the
+ * autotuner below times the candidates. No counterpart in the reference (a
+ * numpy program has no launch shapes). */
+typedef struct kks_launch_shape {
+  int32_t pipeline;     /* 1: fused passes (KKS_PRECISION_MIXED only), 0: cuFFT passes */
+  int32_t cols;         /* fused column tile, 1..4 */
+  int32_t field_blocks; /* 1 .. the cell's maximum (8 blocks per SM) */
+  int32_t pad;
+} kks_launch_shape;
+int kks_get_launch_shape(const kks_handle* h, kks_launch_shape* shape);
+/* Re-captures the attempt graphs; KKS_ERR_STATE while the cell belongs to a batch. */
+int kks_set_launch_shape(kks_handle* h, const kks_launch_shape* shape);
+/* Time every candidate shape on `attempts` attempts of the cell's current
+ * state (which is saved first and restored afterwards: the run continues as if
+ * nothing had happened), keep the fastest and return it with its device time
+ * per attempt. Needs at least 2 scheduled steps left. flags: 0, or
+ * KKS_TUNE_BATCHABLE to consider only shapes that can join a batch. */
+#define KKS_TUNE_BATCHABLE 1
+int kks_autotune(kks_handle* h, int32_t attempts, int32_t flags, kks_launch_shape* best,
+                 double* best_ms_per_attempt);
+
 /* Copy the log records and history rows produced since the last drain. */
 int kks_drain(kks_handle* h, kks_record* records, int64_t record_cap, int64_t* n_records, kks_step_row* rows,
               int64_t row_cap, int64_t* n_rows);
