@@ -61,6 +61,15 @@ namespace {
 constexpr int kThreads = KKS_FFT_THREADS;
 // blocks per SM the register allocation must allow
 constexpr int kMinBlocks = 2;
+// Passes of grids without a large prime factor (small cells, whose blocks are
+// short and latency-bound) ask for three blocks per SM; the prime-stage passes
+// keep two (their warp tasks need 96 registers), and so does rows_D (its FP64
+// pointwise phase would spill). A batched pass and its single-cell twin use
+// the same bound, so that both compile to the same arithmetic.
+template <int P>
+constexpr int pass_min_blocks() {
+  return P > 7 ? kMinBlocks : 3;
+}
 
 __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
@@ -647,7 +656,7 @@ __device__ __forceinline__ void rows_A_body(const KksConst* __restrict__ c, cons
 }
 
 template <int PY>
-__global__ void __launch_bounds__(kThreads, kMinBlocks)
+__global__ void __launch_bounds__(kThreads, pass_min_blocks<PY>())
     kf_rows_A(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const KksFftConst* __restrict__ fc,
               const double* __restrict__ eta, const double* __restrict__ X, float2* __restrict__ RA,
               double* __restrict__ partials, KksCtl* ctl, int bulk, const __grid_constant__ CUtensorMap map_RA) {
@@ -753,7 +762,7 @@ __device__ __forceinline__ void cols_AB_body(const KksConst* __restrict__ c, con
 }
 
 template <int PX>
-__global__ void __launch_bounds__(kThreads, kMinBlocks)
+__global__ void __launch_bounds__(kThreads, pass_min_blocks<PX>())
     kf_cols_AB(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const KksFftConst* __restrict__ fc,
                const float2* __restrict__ RA, float2* __restrict__ SA, float2* __restrict__ RB,
                const double* __restrict__ kys, double* __restrict__ partials, KksCtl* ctl, int bulk) {
@@ -867,7 +876,7 @@ __device__ __forceinline__ void rows_BC_body(const KksConst* __restrict__ c, con
 }
 
 template <int PY>
-__global__ void __launch_bounds__(kThreads, kMinBlocks)
+__global__ void __launch_bounds__(kThreads, pass_min_blocks<PY>())
     kf_rows_BC(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const KksFftConst* __restrict__ fc,
                const float2* __restrict__ RB, float2* __restrict__ RC, const double* __restrict__ eta,
                const float* __restrict__ Xal, const float* __restrict__ Xth, float* g0, float* g1, float* g2,
@@ -935,7 +944,7 @@ __device__ __forceinline__ void cols_CD_eta_body(const KksConst* __restrict__ c,
 }
 
 template <int PX>
-__global__ void __launch_bounds__(kThreads, kMinBlocks)
+__global__ void __launch_bounds__(kThreads, pass_min_blocks<PX>())
     kf_cols_CD_eta(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const KksFftConst* __restrict__ fc,
                    const float2* __restrict__ RC, const float2* __restrict__ SA, float2* __restrict__ RD,
                    const double* __restrict__ kys, KksCtl* ctl, int bulk) {
@@ -1012,7 +1021,7 @@ __device__ __forceinline__ void cols_CD_X_body(const KksConst* __restrict__ c, c
 }
 
 template <int PX>
-__global__ void __launch_bounds__(kThreads, kMinBlocks)
+__global__ void __launch_bounds__(kThreads, pass_min_blocks<PX>())
     kf_cols_CD_X(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const KksFftConst* __restrict__ fc,
                  const float2* __restrict__ RC, const float2* __restrict__ SA, float2* __restrict__ RD,
                  const double* __restrict__ kys, KksCtl* ctl, int bulk) {
@@ -1227,7 +1236,7 @@ __device__ __forceinline__ void tensormap_acquire(const CUtensorMap* map) {
 }
 
 template <int PY>
-__global__ void __launch_bounds__(kThreads, kMinBlocks)
+__global__ void __launch_bounds__(kThreads, pass_min_blocks<PY>())
     kfb_rows_A(const KksCellDesc* __restrict__ cells, const int2* __restrict__ bmap) {
   const int2 m = bmap[blockIdx.x];
   const KksCellDesc* d = cells + m.x;
@@ -1238,7 +1247,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
 }
 
 template <int PX>
-__global__ void __launch_bounds__(kThreads, kMinBlocks)
+__global__ void __launch_bounds__(kThreads, pass_min_blocks<PX>())
     kfb_cols_AB(const KksCellDesc* __restrict__ cells, const int2* __restrict__ bmap) {
   const int2 m = bmap[blockIdx.x];
   const KksCellDesc* d = cells + m.x;
@@ -1247,7 +1256,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
 }
 
 template <int PY>
-__global__ void __launch_bounds__(kThreads, kMinBlocks)
+__global__ void __launch_bounds__(kThreads, pass_min_blocks<PY>())
     kfb_rows_BC(const KksCellDesc* __restrict__ cells, const int2* __restrict__ bmap) {
   const int2 m = bmap[blockIdx.x];
   const KksCellDesc* d = cells + m.x;
@@ -1261,7 +1270,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
 }
 
 template <int PX>
-__global__ void __launch_bounds__(kThreads, kMinBlocks)
+__global__ void __launch_bounds__(kThreads, pass_min_blocks<PX>())
     kfb_cols_CD_eta(const KksCellDesc* __restrict__ cells, const int2* __restrict__ bmap) {
   const int2 m = bmap[blockIdx.x];
   const KksCellDesc* d = cells + m.x;
@@ -1269,7 +1278,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
 }
 
 template <int PX>
-__global__ void __launch_bounds__(kThreads, kMinBlocks)
+__global__ void __launch_bounds__(kThreads, pass_min_blocks<PX>())
     kfb_cols_CD_X(const KksCellDesc* __restrict__ cells, const int2* __restrict__ bmap) {
   const int2 m = bmap[blockIdx.x];
   const KksCellDesc* d = cells + m.x;

@@ -70,9 +70,13 @@ class Ensemble:
     otherwise runs them on their own streams; True requires the batch (raises
     if the cells cannot share one); False always uses the per-cell streams.
     ``mode`` tells which one is in use ("batch" or "streams").
-    ``tune``: give the cells the autotuner's launch shape first, timed on the
-    first cell of every grid size (only shapes that can join a batch) and
-    applied to the others of that size; ``shapes`` holds the choices.
+    ``tune``: choose the launch shapes first. For a batch, the column tile of
+    the fused column passes is timed on the batch itself (one tile for all
+    cells; the cells' states are saved before and restored after every
+    candidate), because a tile that is best for a small cell alone (many small
+    blocks to fill the GPU) wastes SM slots when all cells share the grid.
+    Cells on their own streams get the autotuner's shape of the first cell of
+    each grid size. ``shapes`` holds the choices.
     """
 
     def __init__(self, members, precision="mixed", device=0, batched=None, tune=False, tune_attempts=10):
@@ -89,17 +93,18 @@ class Ensemble:
             c.upload(*state)
             self.cells.append(c)
         self.shapes = {}
-        if tune:
+        self._ptrs = (ctypes.c_void_p * len(self.cells))(*[c.h.value for c in self.cells])
+        self.batch_tile_ms = {}
+        tuned_batch = tune and batched is not False and self.cells and self._tune_batch(tune_attempts)
+        if tune and not tuned_batch:
             from . import autotune
 
             for c in self.cells:
                 k = (c.nx, c.ny)
                 if k not in self.shapes:
-                    self.shapes[k] = autotune.tune(c, attempts=tune_attempts, device=device, cache=False,
-                                                   batchable=batched is not False)["shape"]
+                    self.shapes[k] = autotune.tune(c, attempts=tune_attempts, device=device, cache=False)["shape"]
                 else:
                     c.set_launch_shape(**self.shapes[k])
-        self._ptrs = (ctypes.c_void_p * len(self.cells))(*[c.h.value for c in self.cells])
         self.points = [c.N for c in self.cells]
         self.batch = None
         self.mode = "streams"
@@ -111,6 +116,53 @@ class Ensemble:
                 self.mode = "batch"
             elif batched:
                 L.check(rc, "kks_batch_create")
+
+    def _tune_batch(self, attempts):
+        """Time the batch with every column tile 1..4 (the same for all cells,
+        field grids unchanged) and keep the fastest; False if the cells cannot
+        form a batch."""
+        import ctypes
+
+        from . import _lib as L
+
+        lib = L.load()
+        n = len(self.cells)
+        left = min(c.n_steps - c.state().istep for c in self.cells)
+        k = min(int(attempts), left - 1)
+        if k < 1:
+            return False
+        blobs = [c.checkpoint() for c in self.cells]
+        grids = [c.launch_shape()["field_blocks"] for c in self.cells]
+        for cols in (1, 2, 3, 4):
+            try:
+                for c, g in zip(self.cells, grids):
+                    c.set_launch_shape(1, cols, g)
+            except L.KksError:
+                continue
+            b = ctypes.c_void_p()
+            if lib.kks_batch_create(self._ptrs, n, ctypes.byref(b)) != L.KKS_OK:
+                continue
+            try:
+                st = (ctypes.c_int32 * n)()
+                L.check(lib.kks_batch_run(b, (ctypes.c_int32 * n)(*([1] * n)), st), "kks_batch_run")
+                ms0, a0 = ctypes.c_double(), ctypes.c_int64()
+                L.check(lib.kks_batch_timing(b, ctypes.byref(ms0), ctypes.byref(a0)), "kks_batch_timing")
+                L.check(lib.kks_batch_run(b, (ctypes.c_int32 * n)(*([k] * n)), st), "kks_batch_run")
+                ms1, a1 = ctypes.c_double(), ctypes.c_int64()
+                L.check(lib.kks_batch_timing(b, ctypes.byref(ms1), ctypes.byref(a1)), "kks_batch_timing")
+                if a1.value > a0.value and all(v == L.KKS_STATUS_OK for v in st):
+                    self.batch_tile_ms[cols] = (ms1.value - ms0.value) / (a1.value - a0.value)
+            finally:
+                L.check(lib.kks_batch_destroy(b), "kks_batch_destroy")
+                for c, blob in zip(self.cells, blobs):
+                    c.restore(blob)
+        if not self.batch_tile_ms:
+            return False
+        cols = min(self.batch_tile_ms, key=self.batch_tile_ms.get)
+        for c, g in zip(self.cells, grids):
+            c.set_launch_shape(1, cols, g)
+            self.shapes[(c.nx, c.ny)] = c.launch_shape()
+        return True
 
     def run(self, n_steps):
         """Advance every cell by ``n_steps`` steps (an int, or one count per

@@ -5,7 +5,8 @@ A launch shape only changes how the work of an attempt is cut into blocks: in
 unarmed steps (fixed dt, no residual decision) every shape of the fused passes
 gives the same fields bit for bit, and the cuFFT passes agree to FP32
 round-off. The autotuner leaves the cell's state, step and records as it found
-them, and a batch takes every cell with its own shape.
+them, and a batch takes every cell with its own shape (its results match the
+cells run alone to the mixed path's round-off).
 """
 
 import ctypes
@@ -164,8 +165,9 @@ def test_batch_takes_each_cells_shape():
         L.check(lib.kks_batch_run(b, steps, st), "kks_batch_run")
         assert list(st) == [0, 0, 0]
         for c, r in zip(cells, ref):
-            for x, y in zip(c.download(), r):
-                np.testing.assert_array_equal(x, y)
+            for name, x, y in zip(("eta", "X", "X_al", "X_th"), c.download(), r):
+                # batched kernels: the single-cell run to the mixed path's round-off
+                assert rel_l2(x, y) <= (1e-6 if name in ("eta", "X") else 1e-5), name
     finally:
         L.check(lib.kks_batch_destroy(b), "kks_batch_destroy")
         cells[0].set_launch_shape(1, 3, 7)  # free again once the batch is gone

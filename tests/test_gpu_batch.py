@@ -1,11 +1,19 @@
 """Batched ensembles (``kks_batch_*``): the cells of a batch advance by one
 launch per kernel for all of them, with each cell's dt, rejections, step
-target and buffer parity on the device. Each cell runs the same kernels on
-the same data in the same order as when it runs alone (``kks_run``), so the
-batch must reproduce the single-cell results bit for bit: fields, history
-rows, log records and status, for cells of different sizes, seeds and
-schedules, step counts that differ per cell, adaptive cells that reject and a
-cell that stops with MAX_ITER.
+target and buffer parity on the device.
+
+A batch run is deterministic: run twice it gives the same bits (fields, log
+records, history rows). Against the same cells run alone (``kks_run``) it runs
+the same stages on the same data in the same order, but in kernels compiled
+separately, where the compiler may contract FP32 products differently; such a
+difference in the FP32 increments of a mixed step is as large as the mixed
+step's own rounding (1e-7 relative on X after a few dozen steps), so the bar
+is the mixed path's: eta and X within 1e-6 relative L2, the FP32 phase
+compositions within 1e-5, the same accept / enlarge / reject decisions, steps
+and status, history rows within 1e-4 relative or 2e-7 absolute (the step
+deltas of means of FP32-stored fields are round-off dominated). Covered: cells of different sizes, seeds
+and schedules, step counts that differ per cell, adaptive cells that reject, a
+cell that stops with MAX_ITER, single-cell runs between batch runs.
 """
 
 import ctypes
@@ -13,7 +21,7 @@ import ctypes
 import numpy as np
 import pytest
 
-from conftest import copy_state, small_config, three_precipitates
+from conftest import copy_state, rel_l2, small_config, three_precipitates
 
 pytestmark = pytest.mark.gpu
 
@@ -104,14 +112,40 @@ def _batched(members, plan, single=None):
     return out
 
 
+def _assert_fields_close(got, ref, what):
+    for name, a, e in zip(("eta", "X", "X_al", "X_th"), got, ref):
+        tol = 1e-6 if name in ("eta", "X") else 1e-5
+        assert rel_l2(a, e) <= tol, f"{what}: {name}"
+
+
 def _assert_same(got, ref):
+    """Batch against the cells alone: the mixed path's round-off, same decisions."""
+    from pf_kks_gpu import _lib as L
+
+    for i, (g, r) in enumerate(zip(got, ref)):
+        _assert_fields_close(g[0], r[0], f"cell {i}")
+        assert len(g[1]) == len(r[1]), f"cell {i}: number of log records"
+        for x, y in zip(g[1], r[1]):
+            a, b = L.KksRecord.from_buffer_copy(x), L.KksRecord.from_buffer_copy(y)
+            assert (a.kind, a.istep, a.iteration, a.good_step) == (b.kind, b.istep, b.iteration, b.good_step), \
+                f"cell {i}: decisions differ"
+            np.testing.assert_allclose([a.T, a.D, a.L, a.Meta, a.Vm, a.dtime_s],
+                                       [b.T, b.D, b.L, b.Meta, b.Vm, b.dtime_s], rtol=1e-12)
+        assert g[2].shape == r[2].shape, f"cell {i}: history rows"
+        # the step deltas of means of FP32-stored fields (~1e-7) are round-off dominated
+        np.testing.assert_allclose(g[2], r[2], rtol=1e-4, atol=2e-7, err_msg=f"cell {i}: history rows")
+        assert g[3] == r[3], f"cell {i}: status"
+        assert g[4] == r[4], f"cell {i}: step"
+
+
+def _assert_identical(got, ref):
+    """Two batch runs of the same inputs: bit for bit."""
     for i, (g, r) in enumerate(zip(got, ref)):
         for a, e in zip(g[0], r[0]):
             np.testing.assert_array_equal(a, e, err_msg=f"cell {i}")
-        assert g[1] == r[1], f"cell {i}: log records differ"
+        assert g[1] == r[1], f"cell {i}: log records"
         np.testing.assert_array_equal(g[2], r[2], err_msg=f"cell {i}: history rows")
-        assert g[3] == r[3], f"cell {i}: status"
-        assert g[4] == r[4], f"cell {i}: step"
+        assert g[3:] == r[3:], f"cell {i}: status / step"
 
 
 def test_batch_equals_cells_run_alone(relaxed_state):
@@ -121,6 +155,7 @@ def test_batch_equals_cells_run_alone(relaxed_state):
     steps = [[30], [17], [25], [9], [40], [40]]
     ref = _alone(members, steps)
     got = _batched(members, steps)
+    _assert_identical(_batched(members, steps), got)
     _assert_same(got, ref)
     assert ref[-1][3] == L.KKS_STATUS_MAX_ITER  # the abort case stops on the device
     assert ref[-2][3] == L.KKS_STATUS_OK and ref[-2][4] == 40
@@ -169,3 +204,28 @@ def test_ensemble_runs_as_one_batch(relaxed_state):
         assert ens.batch_timing()[1] == 4
     finally:
         ens.close()
+
+
+def test_ensemble_tunes_the_batch(relaxed_state):
+    """The batch's column tile is timed on the batch itself; the cells start
+    from their initial state afterwards and run exactly as alone with the
+    chosen shape."""
+    from pf_kks_gpu.ensemble import Ensemble
+
+    members = _members(relaxed_state)[:4]
+    ens = Ensemble(members, precision="mixed", tune=True, tune_attempts=3)
+    try:
+        assert ens.mode == "batch" and set(ens.batch_tile_ms) == {1, 2, 3, 4}
+        tiles = {s["cols"] for s in ens.shapes.values()}
+        assert len(tiles) == 1
+        assert [c.state().istep for c in ens.cells] == [0, 0, 0, 0]
+        assert ens.run(5) == [0, 0, 0, 0]
+        got = [c.download() for c in ens.cells]
+    finally:
+        ens.close()
+    for (cfg, state), g in zip(members, got):
+        c = _cell(cfg, state)
+        c.set_launch_shape(1, next(iter(tiles)), c.launch_shape()["field_blocks"])
+        c.run(5)
+        _assert_fields_close(c.download(), g, f"{cfg.nx}x{cfg.ny}")
+        c.close()
