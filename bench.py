@@ -223,6 +223,7 @@ def ensemble_leg(precision, device, steps, warmup):
     out = {"cells": len(members), "points": int(sum(c.nx * c.ny for c, _ in members)), "steps": steps,
            "mode": ens.mode, "launch_shapes": {f"{k[0]}x{k[1]}": v for k, v in sorted(ens.shapes.items())},
            "batch_ms_per_attempt_by_column_tile": ens.batch_tile_ms,
+           "batch_groups": ens.groups, "batch_ms_per_attempt_by_groups": ens.batch_groups_ms,
            "cell_steps_per_s": batched, "streams_cell_steps_per_s": streams,
            "sequential_cell_steps_per_s": sequential, "speedup_vs_streams": batched / streams,
            "speedup_vs_sequential": batched / sequential,

@@ -800,14 +800,23 @@ int kks_run_many(kks_handle** cells, int32_t n_cells, const int32_t* n_steps, in
 // state parity, target step, dt and rejections stay on the device, so cells
 // of different sizes and schedules advance in lockstep without a host
 // decision, and a cell that has reached its target or stopped sits out.
-struct kks_batch {
-  std::vector<kks_handle*> cells;
-  int device = 0;
+// A batch may split its cells into groups of about equal cost, each with its
+// own stream and graph: the groups' passes overlap, so that one group's pass
+// tails and scalar kernels run beside another group's work.
+struct BatchGroup {
+  std::vector<int> idx;  // cells of the batch in this group
   cudaStream_t stream = nullptr;
   cudaGraphExec_t graph = nullptr;
+  cudaEvent_t done = nullptr;
   KksCellDesc* d_cells = nullptr;
   int2* d_maps = nullptr;
   KksBatchLaunch L{};
+};
+
+struct kks_batch {
+  std::vector<kks_handle*> cells;
+  std::vector<BatchGroup> groups;
+  int device = 0;
   int32_t* h_stage = nullptr;  // pinned: target step per cell
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   double device_ms = 0.0;
@@ -817,14 +826,17 @@ struct kks_batch {
 
 static void free_batch(kks_batch* b) {
   if (!b) return;
-  if (b->stream) cudaStreamSynchronize(b->stream);
-  if (b->graph) cudaGraphExecDestroy(b->graph);
-  cudaFree(b->d_cells);
-  cudaFree(b->d_maps);
+  for (BatchGroup& g : b->groups) {
+    if (g.stream) cudaStreamSynchronize(g.stream);
+    if (g.graph) cudaGraphExecDestroy(g.graph);
+    cudaFree(g.d_cells);
+    cudaFree(g.d_maps);
+    if (g.done) cudaEventDestroy(g.done);
+    if (g.stream) cudaStreamDestroy(g.stream);
+  }
   if (b->h_stage) cudaFreeHost(b->h_stage);
   if (b->ev0) cudaEventDestroy(b->ev0);
   if (b->ev1) cudaEventDestroy(b->ev1);
-  if (b->stream) cudaStreamDestroy(b->stream);
   delete b;
 }
 
@@ -866,26 +878,23 @@ static void fill_desc(KksCellDesc& d, const kks_handle* h) {
   d.bulk_cols = L.bulk_cols;
 }
 
-static int batch_create_impl(kks_batch* b) {
-  const int n = (int)b->cells.size();
-  CK(cudaSetDevice(b->device));
-  CK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
-  CK(cudaEventCreate(&b->ev0));
-  CK(cudaEventCreate(&b->ev1));
-  CK(cudaMallocHost(&b->h_stage, n * sizeof(int32_t)));
+static int group_create(kks_batch* b, BatchGroup& G) {
+  const int n = (int)G.idx.size();
+  CK(cudaStreamCreateWithFlags(&G.stream, cudaStreamNonBlocking));
+  CK(cudaEventCreateWithFlags(&G.done, cudaEventDisableTiming));
   std::vector<KksCellDesc> desc(n);
   std::vector<int> nx(n), ny(n), tile(n);
   for (int i = 0; i < n; ++i) {
-    fill_desc(desc[i], b->cells[i]);
-    nx[i] = b->cells[i]->hc.nx;
-    ny[i] = b->cells[i]->hc.ny;
-    tile[i] = b->cells[i]->fl.cols;
+    const kks_handle* h = b->cells[G.idx[i]];
+    fill_desc(desc[i], h);
+    nx[i] = h->hc.nx;
+    ny[i] = h->hc.ny;
+    tile[i] = h->fl.cols;
   }
   // largest cells first, so that the small ones fill the last wave of a pass
   std::vector<int> order(n);
   for (int i = 0; i < n; ++i) order[i] = i;
-  std::stable_sort(order.begin(), order.end(),
-                   [&](int a, int c) { return b->cells[a]->hc.N > b->cells[c]->hc.N; });
+  std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return nx[a] * ny[a] > nx[c] * ny[c]; });
   std::vector<int2> rows, cols, cols3, extras;
   for (int i : order) {
     const int nr = kks_fft_row_blocks(nx[i]), nc = kks_fft_col_blocks(ny[i] / 2 + 1, tile[i]);
@@ -895,7 +904,7 @@ static int batch_create_impl(kks_batch* b) {
       for (int k = 0; k < nc; ++k) cols3.push_back(make_int2(i, (r << 16) | k));
     for (int k = 0; k < desc[i].nbx; ++k) extras.push_back(make_int2(i, k));
   }
-  KksBatchLaunch& L = b->L;
+  KksBatchLaunch& L = G.L;
   L.n_cells = n;
   L.PX = b->cells[0]->fl.PX;
   L.PY = b->cells[0]->fl.PY;
@@ -903,11 +912,11 @@ static int batch_create_impl(kks_batch* b) {
   L.n_cols = (int)cols.size();
   L.n_cols3 = (int)cols3.size();
   L.n_extras = (int)extras.size();
-  CK(cudaMalloc(&b->d_cells, n * sizeof(KksCellDesc)));
-  CK(cudaMemcpy(b->d_cells, desc.data(), n * sizeof(KksCellDesc), cudaMemcpyHostToDevice));
+  CK(cudaMalloc(&G.d_cells, n * sizeof(KksCellDesc)));
+  CK(cudaMemcpy(G.d_cells, desc.data(), n * sizeof(KksCellDesc), cudaMemcpyHostToDevice));
   const size_t nm = rows.size() + cols.size() + cols3.size() + extras.size();
-  CK(cudaMalloc(&b->d_maps, nm * sizeof(int2)));
-  int2* m = b->d_maps;
+  CK(cudaMalloc(&G.d_maps, nm * sizeof(int2)));
+  int2* m = G.d_maps;
   for (const std::vector<int2>* v : {&rows, &cols, &cols3, &extras}) {
     CK(cudaMemcpy(m, v->data(), v->size() * sizeof(int2), cudaMemcpyHostToDevice));
     if (v == &rows) L.map_rows = m;
@@ -916,30 +925,56 @@ static int batch_create_impl(kks_batch* b) {
     else L.map_extras = m;
     m += v->size();
   }
-  L.cells = b->d_cells;
+  L.cells = G.d_cells;
   if (kks_fft_batch_prepare(L, nx.data(), ny.data(), tile.data(), n) != 0)
     return set_error(KKS_ERR_CUDA, "batched fft kernel attributes");
-  b->max_batch = 1LL << 30;
-  for (kks_handle* h : b->cells)
-    b->max_batch = std::min(b->max_batch, std::max(1LL, std::min(h->ring_cap / 2 - 1, h->row_cap - 1)));
   cudaGraph_t g = nullptr;
-  CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-  kks_fft_launch_attempt_batch(L, b->stream);
+  CK(cudaStreamBeginCapture(G.stream, cudaStreamCaptureModeThreadLocal));
+  kks_fft_launch_attempt_batch(L, G.stream);
   const cudaError_t le = cudaGetLastError();
-  cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+  cudaError_t e = cudaStreamEndCapture(G.stream, &g);
   if (le != cudaSuccess) e = le;
   if (e != cudaSuccess) {
     if (g) cudaGraphDestroy(g);
     return set_error(KKS_ERR_CUDA, std::string("batch graph capture: ") + cudaGetErrorString(e));
   }
-  e = cudaGraphInstantiate(&b->graph, g, 0);
+  e = cudaGraphInstantiate(&G.graph, g, 0);
   cudaGraphDestroy(g);
   if (e != cudaSuccess) return set_error(KKS_ERR_CUDA, std::string("batch graph instantiate: ") + cudaGetErrorString(e));
   return KKS_OK;
 }
 
-int kks_batch_create(kks_handle* const* cells, int32_t n_cells, kks_batch** out) {
-  if (!cells || !out || n_cells < 1) return set_error(KKS_ERR_ARG, "bad argument");
+static int batch_create_impl(kks_batch* b, int n_groups) {
+  const int n = (int)b->cells.size();
+  CK(cudaSetDevice(b->device));
+  CK(cudaEventCreate(&b->ev0));
+  CK(cudaEventCreate(&b->ev1));
+  CK(cudaMallocHost(&b->h_stage, n * sizeof(int32_t)));
+  // longest-processing-time split by N log N (the transforms' cost)
+  std::vector<int> order(n);
+  for (int i = 0; i < n; ++i) order[i] = i;
+  auto cost = [&](int i) { const double N = b->cells[i]->hc.N; return N * std::log2(std::max(N, 2.0)); };
+  std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return cost(a) > cost(c); });
+  b->groups.resize(n_groups);
+  std::vector<double> load(n_groups, 0.0);
+  for (int i : order) {
+    const int g = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+    b->groups[g].idx.push_back(i);
+    load[g] += cost(i);
+  }
+  for (BatchGroup& G : b->groups) {
+    std::sort(G.idx.begin(), G.idx.end());
+    const int rc = group_create(b, G);
+    if (rc != KKS_OK) return rc;
+  }
+  b->max_batch = 1LL << 30;
+  for (kks_handle* h : b->cells)
+    b->max_batch = std::min(b->max_batch, std::max(1LL, std::min(h->ring_cap / 2 - 1, h->row_cap - 1)));
+  return KKS_OK;
+}
+
+int kks_batch_create(kks_handle* const* cells, int32_t n_cells, int32_t groups, kks_batch** out) {
+  if (!cells || !out || n_cells < 1 || groups < 1) return set_error(KKS_ERR_ARG, "bad argument");
   *out = nullptr;
   for (int i = 0; i < n_cells; ++i) {
     const kks_handle* h = cells[i];
@@ -956,7 +991,7 @@ int kks_batch_create(kks_handle* const* cells, int32_t n_cells, kks_batch** out)
   if (!b) return set_error(KKS_ERR_ARG, "out of host memory");
   b->cells.assign(cells, cells + n_cells);
   b->device = cells[0]->device;
-  const int rc = batch_create_impl(b);
+  const int rc = batch_create_impl(b, std::min(groups, n_cells));
   if (rc != KKS_OK) {
     std::string msg = g_last_error;
     free_batch(b);
@@ -980,36 +1015,49 @@ int kks_batch_run(kks_batch* b, const int32_t* n_steps, int32_t* status) {
     if (target[i] > h->hc.n_steps) return set_error(KKS_ERR_ARG, "run beyond the scheduled number of steps");
   }
   CK(cudaSetDevice(b->device));
-  for (int i = 0; i < n; ++i) {
-    kks_handle* h = b->cells[i];
-    CK(cudaStreamSynchronize(h->stream));  // the cell's own work (uploads, runs) is done
-    b->h_stage[i] = (int32_t)target[i];
-    CK(cudaMemcpyAsync(&h->d_ctl->target_step, &b->h_stage[i], sizeof(int32_t), cudaMemcpyHostToDevice,
-                       b->stream));
+  cudaStream_t s0 = b->groups[0].stream;
+  for (BatchGroup& G : b->groups) {
+    for (int i : G.idx) {
+      kks_handle* h = b->cells[i];
+      CK(cudaStreamSynchronize(h->stream));  // the cell's own work (uploads, runs) is done
+      b->h_stage[i] = (int32_t)target[i];
+      CK(cudaMemcpyAsync(&h->d_ctl->target_step, &b->h_stage[i], sizeof(int32_t), cudaMemcpyHostToDevice,
+                         G.stream));
+    }
   }
-  CK(cudaEventRecord(b->ev0, b->stream));
+  CK(cudaEventRecord(b->ev0, s0));
+  for (size_t g = 1; g < b->groups.size(); ++g) CK(cudaStreamWaitEvent(b->groups[g].stream, b->ev0, 0));
   long long launched = 0;
   for (;;) {
-    long long todo = 0;
-    for (int i = 0; i < n; ++i) {
-      const KksCtl* c = b->cells[i]->h_ctl;
-      if (c->status == KKS_STATUS_OK && c->istep < target[i]) todo = std::max(todo, target[i] - c->istep);
+    long long most = 0;
+    for (BatchGroup& G : b->groups) {
+      long long todo = 0;
+      for (int i : G.idx) {
+        const KksCtl* c = b->cells[i]->h_ctl;
+        if (c->status == KKS_STATUS_OK && c->istep < target[i]) todo = std::max(todo, target[i] - c->istep);
+      }
+      todo = std::min(todo, b->max_batch);
+      for (long long a = 0; a < todo; ++a) CK(cudaGraphLaunch(G.graph, G.stream));
+      if (todo > 0)
+        for (int i : G.idx) {
+          kks_handle* h = b->cells[i];
+          CK(cudaMemcpyAsync(h->h_ctl, h->d_ctl, sizeof(KksCtl), cudaMemcpyDeviceToHost, G.stream));
+        }
+      most = std::max(most, todo);
     }
-    if (todo == 0) break;
-    todo = std::min(todo, b->max_batch);
-    for (long long a = 0; a < todo; ++a) CK(cudaGraphLaunch(b->graph, b->stream));
-    launched += todo;
-    for (int i = 0; i < n; ++i) {
-      kks_handle* h = b->cells[i];
-      CK(cudaMemcpyAsync(h->h_ctl, h->d_ctl, sizeof(KksCtl), cudaMemcpyDeviceToHost, b->stream));
-    }
-    CK(cudaStreamSynchronize(b->stream));
+    if (most == 0) break;
+    launched += most;
+    for (BatchGroup& G : b->groups) CK(cudaStreamSynchronize(G.stream));
     for (int i = 0; i < n; ++i) {
       int rc = drain_device(b->cells[i]);
       if (rc != KKS_OK) return rc;
     }
   }
-  CK(cudaEventRecord(b->ev1, b->stream));
+  for (size_t g = 1; g < b->groups.size(); ++g) {
+    CK(cudaEventRecord(b->groups[g].done, b->groups[g].stream));
+    CK(cudaStreamWaitEvent(s0, b->groups[g].done, 0));
+  }
+  CK(cudaEventRecord(b->ev1, s0));
   CK(cudaEventSynchronize(b->ev1));
   float ms = 0.f;
   CK(cudaEventElapsedTime(&ms, b->ev0, b->ev1));

@@ -161,7 +161,7 @@ def load(path=LIB_PATH):
     lib.kks_destroy.argtypes = [vp]
     lib.kks_run_many.argtypes = [P(vp), ctypes.c_int32, P(ctypes.c_int32), P(ctypes.c_int32)]
     lib.kks_run_many.restype = ctypes.c_int
-    lib.kks_batch_create.argtypes = [P(vp), ctypes.c_int32, P(vp)]
+    lib.kks_batch_create.argtypes = [P(vp), ctypes.c_int32, ctypes.c_int32, P(vp)]
     lib.kks_batch_run.argtypes = [vp, P(ctypes.c_int32), P(ctypes.c_int32)]
     lib.kks_batch_timing.argtypes = [vp, dp, P(ctypes.c_int64)]
     lib.kks_batch_destroy.argtypes = [vp]

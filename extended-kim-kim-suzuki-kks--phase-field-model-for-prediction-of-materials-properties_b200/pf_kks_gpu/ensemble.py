@@ -70,16 +70,20 @@ class Ensemble:
     otherwise runs them on their own streams; True requires the batch (raises
     if the cells cannot share one); False always uses the per-cell streams.
     ``mode`` tells which one is in use ("batch" or "streams").
+    ``groups``: the batch's cells are split into that many groups of about
+    equal cost, each a graph on its own stream (their passes overlap).
     ``tune``: choose the launch shapes first. For a batch, the column tile of
-    the fused column passes is timed on the batch itself (one tile for all
-    cells; the cells' states are saved before and restored after every
+    the fused column passes and then the number of groups are timed on the
+    batch itself (the cells' states are saved before and restored after every
     candidate), because a tile that is best for a small cell alone (many small
     blocks to fill the GPU) wastes SM slots when all cells share the grid.
     Cells on their own streams get the autotuner's shape of the first cell of
-    each grid size. ``shapes`` holds the choices.
+    each grid size. ``shapes``, ``groups`` and ``batch_tile_ms`` /
+    ``batch_groups_ms`` hold the choices and their device times per attempt.
     """
 
-    def __init__(self, members, precision="mixed", device=0, batched=None, tune=False, tune_attempts=10):
+    def __init__(self, members, precision="mixed", device=0, batched=None, tune=False, tune_attempts=10,
+                 groups=1):
         import ctypes
 
         from . import _lib as L
@@ -95,6 +99,8 @@ class Ensemble:
         self.shapes = {}
         self._ptrs = (ctypes.c_void_p * len(self.cells))(*[c.h.value for c in self.cells])
         self.batch_tile_ms = {}
+        self.batch_groups_ms = {}
+        self.groups = int(groups)
         tuned_batch = tune and batched is not False and self.cells and self._tune_batch(tune_attempts)
         if tune and not tuned_batch:
             from . import autotune
@@ -110,23 +116,49 @@ class Ensemble:
         self.mode = "streams"
         if batched is not False and self.cells:
             b = ctypes.c_void_p()
-            rc = L.load().kks_batch_create(self._ptrs, len(self.cells), ctypes.byref(b))
+            rc = L.load().kks_batch_create(self._ptrs, len(self.cells), self.groups, ctypes.byref(b))
             if rc == L.KKS_OK:
                 self.batch = b
                 self.mode = "batch"
             elif batched:
                 L.check(rc, "kks_batch_create")
 
-    def _tune_batch(self, attempts):
-        """Time the batch with every column tile 1..4 (the same for all cells,
-        field grids unchanged) and keep the fastest; False if the cells cannot
-        form a batch."""
+    def _time_batch(self, groups, k, blobs):
+        """Device ms per batch attempt of the cells' current shapes with the
+        given groups (None if the cells cannot form that batch); the cells'
+        states are restored from ``blobs`` afterwards."""
         import ctypes
 
         from . import _lib as L
 
         lib = L.load()
         n = len(self.cells)
+        b = ctypes.c_void_p()
+        if lib.kks_batch_create(self._ptrs, n, int(groups), ctypes.byref(b)) != L.KKS_OK:
+            return None
+        per = None
+        try:
+            st = (ctypes.c_int32 * n)()
+            L.check(lib.kks_batch_run(b, (ctypes.c_int32 * n)(*([1] * n)), st), "kks_batch_run")
+            ms0, a0 = ctypes.c_double(), ctypes.c_int64()
+            L.check(lib.kks_batch_timing(b, ctypes.byref(ms0), ctypes.byref(a0)), "kks_batch_timing")
+            L.check(lib.kks_batch_run(b, (ctypes.c_int32 * n)(*([k] * n)), st), "kks_batch_run")
+            ms1, a1 = ctypes.c_double(), ctypes.c_int64()
+            L.check(lib.kks_batch_timing(b, ctypes.byref(ms1), ctypes.byref(a1)), "kks_batch_timing")
+            if a1.value > a0.value and all(v == L.KKS_STATUS_OK for v in st):
+                per = (ms1.value - ms0.value) / (a1.value - a0.value)
+        finally:
+            L.check(lib.kks_batch_destroy(b), "kks_batch_destroy")
+            for c, blob in zip(self.cells, blobs):
+                c.restore(blob)
+        return per
+
+    def _tune_batch(self, attempts):
+        """Time the batch with every column tile 1..4 (the same for all cells,
+        field grids unchanged), then with 1, 2, 3 and 4 groups; keep the
+        fastest. False if the cells cannot form a batch."""
+        from . import _lib as L
+
         left = min(c.n_steps - c.state().istep for c in self.cells)
         k = min(int(attempts), left - 1)
         if k < 1:
@@ -139,29 +171,22 @@ class Ensemble:
                     c.set_launch_shape(1, cols, g)
             except L.KksError:
                 continue
-            b = ctypes.c_void_p()
-            if lib.kks_batch_create(self._ptrs, n, ctypes.byref(b)) != L.KKS_OK:
-                continue
-            try:
-                st = (ctypes.c_int32 * n)()
-                L.check(lib.kks_batch_run(b, (ctypes.c_int32 * n)(*([1] * n)), st), "kks_batch_run")
-                ms0, a0 = ctypes.c_double(), ctypes.c_int64()
-                L.check(lib.kks_batch_timing(b, ctypes.byref(ms0), ctypes.byref(a0)), "kks_batch_timing")
-                L.check(lib.kks_batch_run(b, (ctypes.c_int32 * n)(*([k] * n)), st), "kks_batch_run")
-                ms1, a1 = ctypes.c_double(), ctypes.c_int64()
-                L.check(lib.kks_batch_timing(b, ctypes.byref(ms1), ctypes.byref(a1)), "kks_batch_timing")
-                if a1.value > a0.value and all(v == L.KKS_STATUS_OK for v in st):
-                    self.batch_tile_ms[cols] = (ms1.value - ms0.value) / (a1.value - a0.value)
-            finally:
-                L.check(lib.kks_batch_destroy(b), "kks_batch_destroy")
-                for c, blob in zip(self.cells, blobs):
-                    c.restore(blob)
+            per = self._time_batch(1, k, blobs)
+            if per is not None:
+                self.batch_tile_ms[cols] = per
         if not self.batch_tile_ms:
             return False
         cols = min(self.batch_tile_ms, key=self.batch_tile_ms.get)
         for c, g in zip(self.cells, grids):
             c.set_launch_shape(1, cols, g)
             self.shapes[(c.nx, c.ny)] = c.launch_shape()
+        self.batch_groups_ms[1] = self.batch_tile_ms[cols]
+        for groups in (2, 3, 4):
+            if groups <= len(self.cells):
+                per = self._time_batch(groups, k, blobs)
+                if per is not None:
+                    self.batch_groups_ms[groups] = per
+        self.groups = min(self.batch_groups_ms, key=self.batch_groups_ms.get)
         return True
 
     def run(self, n_steps):

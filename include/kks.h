@@ -153,11 +153,14 @@ int kks_run_many(kks_handle** cells, int32_t n_cells, const int32_t* n_steps, in
  * descriptors (one CUDA graph); each cell keeps its own adaptive dt,
  * rejections, step target and buffer parity on the device, so cells of
  * different size, seed and schedule advance in lockstep and a cell that has
- * reached its target sits out. Results equal kks_run of each cell.
- * The cells must outlive the batch. Replaces running pf_kks.solver.run
- * (pf_kks/solver.py:76-414) once per instance. */
+ * reached its target sits out. Results equal kks_run of each cell up to the
+ * rounding of separately compiled FP32 kernels. `groups` (>= 1) splits the
+ * cells into that many groups of about equal cost, each a graph on its own
+ * stream, so that the groups' passes overlap. The cells must outlive the
+ * batch. Replaces running pf_kks.solver.run (pf_kks/solver.py:76-414) once per
+ * instance. */
 typedef struct kks_batch kks_batch;
-int kks_batch_create(kks_handle* const* cells, int32_t n_cells, kks_batch** out);
+int kks_batch_create(kks_handle* const* cells, int32_t n_cells, int32_t groups, kks_batch** out);
 /* Advance cell i by n_steps[i] steps; status[i] receives KKS_STATUS_*. */
 int kks_batch_run(kks_batch* b, const int32_t* n_steps, int32_t* status);
 /* Device time of all kks_batch_run calls (CUDA events) and batch attempts launched. */

@@ -156,7 +156,7 @@ def test_batch_takes_each_cells_shape():
     lib = L.load()
     ptrs = (ctypes.c_void_p * 3)(*[c.h.value for c in cells])
     b = ctypes.c_void_p()
-    L.check(lib.kks_batch_create(ptrs, 3, ctypes.byref(b)), "kks_batch_create")
+    L.check(lib.kks_batch_create(ptrs, 3, 1, ctypes.byref(b)), "kks_batch_create")
     try:
         with pytest.raises(L.KksError):
             cells[0].set_launch_shape(1, 3, 7)  # fixed while the cell is in a batch

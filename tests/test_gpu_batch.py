@@ -70,17 +70,18 @@ def _alone(members, plan):
     return out
 
 
-def _batched(members, plan, single=None):
-    """All cells in one batch, the same segments as kks_batch_run calls;
-    ``single`` = (segment index, cell, steps): that cell also runs alone by
-    kks_run after that segment (the batch must pick up its new parity)."""
+def _batched(members, plan, single=None, groups=1):
+    """All cells in one batch (split into ``groups`` streams), the same
+    segments as kks_batch_run calls; ``single`` = (segment index, cell,
+    steps): that cell also runs alone by kks_run after that segment (the batch
+    must pick up its new parity)."""
     from pf_kks_gpu import _lib as L
 
     cells = [_cell(cfg, state) for cfg, state in members]
     lib = L.load()
     ptrs = (ctypes.c_void_p * len(cells))(*[c.h.value for c in cells])
     b = ctypes.c_void_p()
-    L.check(lib.kks_batch_create(ptrs, len(cells), ctypes.byref(b)), "kks_batch_create")
+    L.check(lib.kks_batch_create(ptrs, len(cells), groups, ctypes.byref(b)), "kks_batch_create")
     recs = [[] for _ in cells]
     rows = [[] for _ in cells]
     status = [0] * len(cells)
@@ -157,6 +158,8 @@ def test_batch_equals_cells_run_alone(relaxed_state):
     got = _batched(members, steps)
     _assert_identical(_batched(members, steps), got)
     _assert_same(got, ref)
+    # cost-balanced groups on their own streams: the same kernels per cell, the same bits
+    _assert_identical(_batched(members, steps, groups=3), got)
     assert ref[-1][3] == L.KKS_STATUS_MAX_ITER  # the abort case stops on the device
     assert ref[-2][3] == L.KKS_STATUS_OK and ref[-2][4] == 40
 
@@ -169,7 +172,7 @@ def test_batch_segments_and_single_cell_runs_in_between(relaxed_state):
     # cell 1 runs 3 more steps alone after the first segment
     alone_plan = [[7, 11, 12], [5, 3, 0, 12], [3, 4, 5], [9, 0, 0], [13, 14, 13]]
     ref = _alone(members, alone_plan)
-    got = _batched(members, plan, single=(0, 1, 3))
+    got = _batched(members, plan, single=(0, 1, 3), groups=2)
     _assert_same(got, ref)
 
 
@@ -186,7 +189,7 @@ def test_batch_rejects_cells_it_cannot_share():
     b = ctypes.c_void_p()
     for cells in ([a, f], [a, a]):
         ptrs = (ctypes.c_void_p * 2)(*[c.h.value for c in cells])
-        assert lib.kks_batch_create(ptrs, 2, ctypes.byref(b)) != L.KKS_OK
+        assert lib.kks_batch_create(ptrs, 2, 1, ctypes.byref(b)) != L.KKS_OK
     a.close()
     f.close()
 
@@ -216,6 +219,7 @@ def test_ensemble_tunes_the_batch(relaxed_state):
     ens = Ensemble(members, precision="mixed", tune=True, tune_attempts=3)
     try:
         assert ens.mode == "batch" and set(ens.batch_tile_ms) == {1, 2, 3, 4}
+        assert set(ens.batch_groups_ms) == {1, 2, 3, 4} and ens.groups in ens.batch_groups_ms
         tiles = {s["cols"] for s in ens.shapes.values()}
         assert len(tiles) == 1
         assert [c.state().istep for c in ens.cells] == [0, 0, 0, 0]
