@@ -70,6 +70,7 @@ class Ensemble:
     otherwise runs them on their own streams; True requires the batch (raises
     if the cells cannot share one); False always uses the per-cell streams.
     ``mode`` tells which one is in use ("batch" or "streams").
+    ``cols``: a fused column tile for every cell (instead of the default).
     ``groups``: the batch's cells are split into that many groups of about
     equal cost, each a graph on its own stream (their passes overlap).
     ``tune``: choose the launch shapes first. For a batch, the column tile of
@@ -80,10 +81,13 @@ class Ensemble:
     Cells on their own streams get the autotuner's shape of the first cell of
     each grid size. ``shapes``, ``groups`` and ``batch_tile_ms`` /
     ``batch_groups_ms`` hold the choices and their device times per attempt.
+    With ``tune`` and a batch, the batch and the per-cell streams are then
+    timed on the same attempts (host wall clock, one synchronisation per
+    call) and ``run`` uses the faster (``mode``; ``mode_ms`` holds the times).
     """
 
     def __init__(self, members, precision="mixed", device=0, batched=None, tune=False, tune_attempts=10,
-                 groups=1):
+                 groups=1, cols=None):
         import ctypes
 
         from . import _lib as L
@@ -97,6 +101,9 @@ class Ensemble:
             c.upload(*state)
             self.cells.append(c)
         self.shapes = {}
+        if cols is not None:
+            for c in self.cells:
+                c.set_launch_shape(1, cols, c.launch_shape()["field_blocks"])
         self._ptrs = (ctypes.c_void_p * len(self.cells))(*[c.h.value for c in self.cells])
         self.batch_tile_ms = {}
         self.batch_groups_ms = {}
@@ -114,6 +121,7 @@ class Ensemble:
         self.points = [c.N for c in self.cells]
         self.batch = None
         self.mode = "streams"
+        self.mode_ms = {}
         if batched is not False and self.cells:
             b = ctypes.c_void_p()
             rc = L.load().kks_batch_create(self._ptrs, len(self.cells), self.groups, ctypes.byref(b))
@@ -122,6 +130,31 @@ class Ensemble:
                 self.mode = "batch"
             elif batched:
                 L.check(rc, "kks_batch_create")
+        if tuned_batch and batched is None:
+            self._choose_mode(tune_attempts)
+
+    def _choose_mode(self, attempts):
+        """Time the batch and the per-cell streams on the same attempts of the
+        current state (restored afterwards) and keep the faster."""
+        import time
+
+        left = min(c.n_steps - c.state().istep for c in self.cells)
+        k = min(int(attempts), left - 1)
+        if k < 1:
+            return
+        blobs = [c.checkpoint() for c in self.cells]
+        for mode, fn in (("batch", lambda m: self._call("kks_batch_run", (self.batch,), m)),
+                         ("streams", self.run_streams)):
+            fn(1)
+            t0 = time.perf_counter()
+            st = fn(k)
+            dt = time.perf_counter() - t0
+            for c, blob in zip(self.cells, blobs):
+                c.restore(blob)
+            if all(v == 0 for v in st):
+                self.mode_ms[mode] = 1000.0 * dt / k
+        if len(self.mode_ms) == 2:
+            self.mode = min(self.mode_ms, key=self.mode_ms.get)
 
     def _time_batch(self, groups, k, blobs):
         """Device ms per batch attempt of the cells' current shapes with the
@@ -192,9 +225,15 @@ class Ensemble:
     def run(self, n_steps):
         """Advance every cell by ``n_steps`` steps (an int, or one count per
         cell); returns the status per cell."""
-        if self.batch is not None:
-            return self._call("kks_batch_run", (self.batch,), n_steps)
+        if self.mode == "batch":
+            return self.run_batch(n_steps)
         return self.run_streams(n_steps)
+
+    def run_batch(self, n_steps):
+        """The same steps as one batch (``kks_batch_run``)."""
+        if self.batch is None:
+            raise RuntimeError("these cells do not form a batch")
+        return self._call("kks_batch_run", (self.batch,), n_steps)
 
     def run_streams(self, n_steps):
         """The same steps with every cell on its own stream (``kks_run_many``)."""
