@@ -228,6 +228,7 @@ def ensemble_leg(precision, device, steps, warmup):
            "mode": ens.mode, "mode_ms_per_attempt": ens.mode_ms,
            "launch_shapes": {f"{k[0]}x{k[1]}": v for k, v in sorted(ens.shapes.items())},
            "batch_ms_per_attempt_by_column_tile": ens.batch_tile_ms,
+           "batch_ms_per_attempt_by_field_grid_divisor": ens.batch_grid_ms,
            "batch_groups": ens.groups, "batch_ms_per_attempt_by_groups": ens.batch_groups_ms,
            "cell_steps_per_s": best, "batch_cell_steps_per_s": batched, "streams_cell_steps_per_s": streams,
            "sequential_cell_steps_per_s": sequential, "speedup_vs_sequential": best / sequential,

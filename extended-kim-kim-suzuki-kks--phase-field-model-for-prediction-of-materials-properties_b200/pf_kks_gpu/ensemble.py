@@ -80,7 +80,8 @@ class Ensemble:
     blocks to fill the GPU) wastes SM slots when all cells share the grid.
     Cells on their own streams get the autotuner's shape of the first cell of
     each grid size. ``shapes``, ``groups`` and ``batch_tile_ms`` /
-    ``batch_groups_ms`` hold the choices and their device times per attempt.
+    ``batch_grid_ms`` / ``batch_groups_ms`` hold the choices and their device
+    times per attempt.
     With ``tune`` and a batch, the batch and the per-cell streams are then
     timed on the same attempts (host wall clock, one synchronisation per
     call) and ``run`` uses the faster (``mode``; ``mode_ms`` holds the times).
@@ -106,6 +107,7 @@ class Ensemble:
                 c.set_launch_shape(1, cols, c.launch_shape()["field_blocks"])
         self._ptrs = (ctypes.c_void_p * len(self.cells))(*[c.h.value for c in self.cells])
         self.batch_tile_ms = {}
+        self.batch_grid_ms = {}
         self.batch_groups_ms = {}
         self.groups = int(groups)
         tuned_batch = tune and batched is not False and self.cells and self._tune_batch(tune_attempts)
@@ -188,8 +190,9 @@ class Ensemble:
 
     def _tune_batch(self, attempts):
         """Time the batch with every column tile 1..4 (the same for all cells,
-        field grids unchanged), then with 1, 2, 3 and 4 groups; keep the
-        fastest. False if the cells cannot form a batch."""
+        field grids unchanged), then the field-kernel grids divided by 1, 4
+        and 16, then 1, 2, 3 and 4 groups; keep the fastest of each. False if
+        the cells cannot form a batch."""
         from . import _lib as L
 
         left = min(c.n_steps - c.state().istep for c in self.cells)
@@ -210,10 +213,20 @@ class Ensemble:
         if not self.batch_tile_ms:
             return False
         cols = min(self.batch_tile_ms, key=self.batch_tile_ms.get)
+        # the grid-stride kernels (gradient energy, interface count, restore):
+        # coarser grids than a cell alone wants, since 48 cells share the GPU
+        self.batch_grid_ms = {1: self.batch_tile_ms[cols]}
+        for d in (4, 16):
+            for c, g in zip(self.cells, grids):
+                c.set_launch_shape(1, cols, max(1, g // d))
+            per = self._time_batch(1, k, blobs)
+            if per is not None:
+                self.batch_grid_ms[d] = per
+        d = min(self.batch_grid_ms, key=self.batch_grid_ms.get)
         for c, g in zip(self.cells, grids):
-            c.set_launch_shape(1, cols, g)
+            c.set_launch_shape(1, cols, max(1, g // d))
             self.shapes[(c.nx, c.ny)] = c.launch_shape()
-        self.batch_groups_ms[1] = self.batch_tile_ms[cols]
+        self.batch_groups_ms[1] = self.batch_grid_ms[d]
         for groups in (2, 3, 4):
             if groups <= len(self.cells):
                 per = self._time_batch(groups, k, blobs)

@@ -219,6 +219,7 @@ def test_ensemble_tunes_the_batch(relaxed_state):
     ens = Ensemble(members, precision="mixed", tune=True, tune_attempts=3)
     try:
         assert set(ens.batch_tile_ms) == {1, 2, 3, 4} and set(ens.mode_ms) == {"batch", "streams"}
+        assert set(ens.batch_grid_ms) == {1, 4, 16}
         assert ens.mode == min(ens.mode_ms, key=ens.mode_ms.get)
         assert set(ens.batch_groups_ms) == {1, 2, 3, 4} and ens.groups in ens.batch_groups_ms
         tiles = {s["cols"] for s in ens.shapes.values()}
@@ -230,7 +231,8 @@ def test_ensemble_tunes_the_batch(relaxed_state):
         ens.close()
     for (cfg, state), g in zip(members, got):
         c = _cell(cfg, state)
-        c.set_launch_shape(1, next(iter(tiles)), c.launch_shape()["field_blocks"])
+        shape = ens.shapes[(cfg.nx, cfg.ny)]
+        c.set_launch_shape(1, shape["cols"], shape["field_blocks"])
         c.run(5)
         _assert_fields_close(c.download(), g, f"{cfg.nx}x{cfg.ny}")
         c.close()
