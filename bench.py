@@ -191,7 +191,36 @@ def cpu_baseline(state, cfg):
             "sample": f"first {k} steps of the same 1420^2 cell, FP64 numpy oracle, scipy.fft with {cores} workers"}
 
 
-def ensemble_leg(precision, device, steps, warmup):
+def _oracle_cell_steps(job):
+    """One CPU process of the ensemble baseline: ``k`` FP64 oracle steps of one
+    cell (numpy, one FFT worker); returns (cell-steps, seconds of the steps)."""
+    from oracle import kks_oracle
+
+    cfg, state, k = job
+    t0 = time.perf_counter()
+    kks_oracle.run(cfg, *state, cfg.material_tables, write_logs=False, save_maps=False, max_steps=k,
+                   fft_workers=1)
+    return cfg.nx * cfg.ny * k, time.perf_counter() - t0
+
+
+def ensemble_cpu_baseline(members, k=3):
+    """The ensemble on the host cores: one independent oracle process per core,
+    each advancing one cell of the ensemble by ``k`` steps (the first ``cores``
+    cells); throughput = all cell-steps / the longest process's step time.
+    Processes are started with ``spawn`` (this process has a CUDA context)."""
+    import multiprocessing as mp
+
+    cores = os.cpu_count() or 1
+    jobs = [(cfg, state, k) for cfg, state in members[:cores]]
+    with mp.get_context("spawn").Pool(len(jobs)) as pool:
+        out = pool.map(_oracle_cell_steps, jobs)
+    work = sum(w for w, _ in out)
+    return {"value": work / max(t for _, t in out), "unit": "cell-steps/s", "cores": len(jobs), "kind": "port",
+            "sample": f"{len(jobs)} concurrent processes (one per core), each {k} FP64 oracle steps of one "
+                      f"ensemble cell (sides {sorted({c.nx for c, _, _ in jobs})}), numpy with one FFT worker"}
+
+
+def ensemble_leg(precision, device, steps, warmup, cpu=True):
     """Batched cell-steps/s of the 48-cell ensemble (sides 128..512, heating
     rates U(5,40) K/min): the batch (kks_batch_run: every kernel of an attempt
     launched once for all cells, one graph per batch attempt), every cell on
@@ -235,6 +264,8 @@ def ensemble_leg(precision, device, steps, warmup):
            "timing": "host wall clock around each run call (one host sync per batch of attempts)"}
     if att1 > att0:
         out["batch_device_ms_per_attempt"] = (ms1 - ms0) / (att1 - att0)
+    if cpu:
+        out["cpu_baseline"] = ensemble_cpu_baseline(members)
     return out
 
 
@@ -544,7 +575,8 @@ def main():
         "gpu_launches": int(kernels_per_attempt * attempts),
     }
     if not args.no_ensemble and args.precision != "fp64":
-        line["ensemble"] = ensemble_leg(args.precision, local_rank, steps=20, warmup=3)
+        line["ensemble"] = ensemble_leg(args.precision, local_rank, steps=20, warmup=3,
+                                        cpu=not args.no_cpu_baseline and world == 1)
     if not args.no_init and world == 1 and args.precision != "fp64":
         line["init"] = init_leg(args.precision, local_rank)
     if not args.no_adjoint and world == 1:
