@@ -292,8 +292,7 @@ static int upload_vec(const std::vector<T>& v, T** dst) {
 
 // Partial-sum rows the fused attempt writes under the cell's launch shape.
 static int fused_rows(const kks_handle* h) {
-  return std::max(std::max(kks_fft_row_blocks(h->hc.nx), kks_fft_col_blocks(h->hc.nyh, h->fl.cols)),
-                  std::max(h->nblocks, kks_fft_extras_blocks(h->hc.nx, h->hc.ny)));
+  return std::max(std::max(kks_fft_row_blocks(h->hc.nx), kks_fft_col_blocks(h->hc.nyh, h->fl.cols)), h->nblocks);
 }
 
 static int setup_fused(kks_handle* h, const std::vector<double>& kx) {
@@ -372,8 +371,7 @@ static int setup_fused(kks_handle* h, const std::vector<double>& kx) {
   // every kernel of the pipeline writes one partial-sum row per block: the
   // buffer holds the largest grid of them (row pairs, column tiles, extras)
   // under any launch shape; the decide kernel reads the rows of the current one
-  h->part_cap_fused = std::max(std::max(kks_fft_partial_rows(c.nx, c.ny, h->nblocks_cap), h->nblocks_cap),
-                               kks_fft_extras_blocks(c.nx, c.ny));
+  h->part_cap_fused = std::max(kks_fft_partial_rows(c.nx, c.ny, h->nblocks_cap), h->nblocks_cap);
   h->nb_fused = fused_rows(h);
   CK(cudaMalloc(&h->partials_fused, (size_t)h->part_cap_fused * KKS_NPART * sizeof(double)));
   CK(cudaMemset(h->partials_fused, 0, (size_t)h->part_cap_fused * KKS_NPART * sizeof(double)));
@@ -897,7 +895,7 @@ static int group_create(kks_batch* b, BatchGroup& G) {
   std::vector<int> order(n);
   for (int i = 0; i < n; ++i) order[i] = i;
   std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return nx[a] * ny[a] > nx[c] * ny[c]; });
-  std::vector<int2> rows, cols, cols3, extras, stencil;
+  std::vector<int2> rows, cols, cols3, extras;
   for (int i : order) {
     const int nr = kks_fft_row_blocks(nx[i]), nc = kks_fft_col_blocks(ny[i] / 2 + 1, tile[i]);
     for (int k = 0; k < nr; ++k) rows.push_back(make_int2(i, k));
@@ -905,7 +903,6 @@ static int group_create(kks_batch* b, BatchGroup& G) {
     for (int r = 0; r < 3; ++r)
       for (int k = 0; k < nc; ++k) cols3.push_back(make_int2(i, (r << 16) | k));
     for (int k = 0; k < desc[i].nbx; ++k) extras.push_back(make_int2(i, k));
-    for (int k = 0, ne = kks_fft_extras_blocks(nx[i], ny[i]); k < ne; ++k) stencil.push_back(make_int2(i, k));
   }
   KksBatchLaunch& L = G.L;
   L.n_cells = n;
@@ -915,19 +912,17 @@ static int group_create(kks_batch* b, BatchGroup& G) {
   L.n_cols = (int)cols.size();
   L.n_cols3 = (int)cols3.size();
   L.n_extras = (int)extras.size();
-  L.n_stencil = (int)stencil.size();
   CK(cudaMalloc(&G.d_cells, n * sizeof(KksCellDesc)));
   CK(cudaMemcpy(G.d_cells, desc.data(), n * sizeof(KksCellDesc), cudaMemcpyHostToDevice));
-  const size_t nm = rows.size() + cols.size() + cols3.size() + extras.size() + stencil.size();
+  const size_t nm = rows.size() + cols.size() + cols3.size() + extras.size();
   CK(cudaMalloc(&G.d_maps, nm * sizeof(int2)));
   int2* m = G.d_maps;
-  for (const std::vector<int2>* v : {&rows, &cols, &cols3, &extras, &stencil}) {
+  for (const std::vector<int2>* v : {&rows, &cols, &cols3, &extras}) {
     CK(cudaMemcpy(m, v->data(), v->size() * sizeof(int2), cudaMemcpyHostToDevice));
     if (v == &rows) L.map_rows = m;
     else if (v == &cols) L.map_cols = m;
     else if (v == &cols3) L.map_cols3 = m;
-    else if (v == &extras) L.map_extras = m;
-    else L.map_stencil = m;
+    else L.map_extras = m;
     m += v->size();
   }
   L.cells = G.d_cells;

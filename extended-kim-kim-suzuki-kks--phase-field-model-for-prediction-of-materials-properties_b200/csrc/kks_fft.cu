@@ -1159,99 +1159,67 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
   rows_D_body<PY>(c, par, fc, RD, eta_o, X_o, eta_b, X_b, Xal_b, Xth_b, eta_m, X_m, mu, g0, g1, g2, partials, ctl, bulk, &map_RD, (int)blockIdx.x);
 }
 
+// np.gradient energy sum of a state (mode bit 0) and, at surface steps, its
+// interface cell count (mode bit 1) into the given partial slots.
 constexpr int kExtrasThreads = 256;
 
-// The np.gradient energy and, at surface steps, the interface count of a
-// cell's candidate state, as a streaming stencil: a warp owns 32
-// consecutive y of a chunk of kExtRows rows and walks down the rows, each lane
-// keeping rows ix - 1, ix, ix + 1 of its column in registers (kExtU rows
-// loaded ahead); the y neighbours come from the adjacent lanes by shuffles,
-// the warp's two edge lanes load theirs. One coalesced load per point instead
-// of five scattered ones. Per point: np.gradient's central differences inside
-// and one-sided ones at the edges (pf_kks/free_energy.py:98-110), and the
-// cells whose four corners lie in [0.1, 0.9] (pf_kks/microstructure.py:117-128).
-constexpr int kExtRows = 16;
-constexpr int kExtU = 8;
-constexpr int kExtWarps = kExtrasThreads / 32;
-
-__host__ __device__ inline int extras_warps(int nx, int ny) {
-  return ((ny + 31) / 32) * ((nx + kExtRows - 1) / kExtRows);
-}
-
-__device__ __forceinline__ void extras_stream_body(const KksConst* __restrict__ c, const KksPar* __restrict__ par,
-                                                   const double* __restrict__ eta, double* __restrict__ partials,
-                                                   int bx) {
+__device__ __forceinline__ void extras_body(const KksConst* __restrict__ c, const KksPar* __restrict__ par,
+                                            const double* __restrict__ eta, int mode, int slot_grad, int slot_iface,
+                                            double* __restrict__ partials, int bx, int nbk) {
   if (!par->active) return;
-  const int nx = c->nx, ny = c->ny;
-  const bool do_iface = par->surface;
-  const int lane = threadIdx.x & 31;
-  const int nsy = (ny + 31) >> 5;
-  const int w = bx * kExtWarps + (threadIdx.x >> 5);
-  double acc[2] = {0.0, 0.0};
-  if (w < extras_warps(nx, ny)) {  // uniform over the warp
-    const int sx = w / nsy, sy = w - sx * nsy;
-    const int y = (sy << 5) + lane;
-    const bool vy = y < ny;
-    const int x0 = sx * kExtRows, x1 = min(x0 + kExtRows, nx);
-    const double* col = eta + y;  // element (ix, y) at col[ix * ny]; dereferenced only for y < ny
-    const bool l0 = lane == 0 && vy && y > 0;  // loads (ix, y - 1)
-    const bool l31 = lane == 31 && y + 1 < ny;  // loads (ix, y + 1)
-    double em = (vy && x0 > 0) ? col[(size_t)(x0 - 1) * ny] : 0.0;
-    double ec = vy ? col[(size_t)x0 * ny] : 0.0;
-    double side = l0 ? col[(size_t)x0 * ny - 1] : (l31 ? col[(size_t)x0 * ny + 1] : 0.0);
-    for (int g = x0; g < x1; g += kExtU) {
-      double nv[kExtU], ns[kExtU];  // row ix + 1 of the column, and of the edge lane's neighbour
+  const bool do_grad = mode & 1;
+  const bool do_iface = (mode & 2) && par->surface;
+  if (!do_grad && !do_iface) return;
+  const int N = c->N, nx = c->nx, ny = c->ny;
+  double acc[2] = {0, 0};
+  // kU points per thread and iteration, their stencil loads issued together
+  constexpr int kU = 4;
+  const int stride = nbk * blockDim.x;
+  for (int i0 = bx * blockDim.x + threadIdx.x; i0 < N; i0 += kU * stride) {
+    double e[kU], xm[kU], xp[kU], ym[kU], yp[kU];
 #pragma unroll
-      for (int u = 0; u < kExtU; ++u) {
-        const int r = g + u + 1;
-        const bool ok = g + u < x1 && r < nx;
-        nv[u] = (ok && vy) ? col[(size_t)r * ny] : 0.0;
-        ns[u] = (ok && l0) ? col[(size_t)r * ny - 1] : ((ok && l31) ? col[(size_t)r * ny + 1] : 0.0);
+    for (int u = 0; u < kU; ++u) {
+      const int i = i0 + u * stride;
+      if (i < N) {
+        const int ix = i / ny, iy = i - ix * ny;
+        e[u] = eta[i];
+        xm[u] = ix > 0 ? eta[i - ny] : 0.0;
+        xp[u] = ix < nx - 1 ? eta[i + ny] : 0.0;
+        ym[u] = iy > 0 ? eta[i - 1] : 0.0;
+        yp[u] = iy < ny - 1 ? eta[i + 1] : 0.0;
       }
+    }
 #pragma unroll
-      for (int u = 0; u < kExtU; ++u) {
-        const int ix = g + u;
-        if (ix < x1) {  // uniform over the warp
-          const double en = nv[u];
-          double ym = __shfl_up_sync(0xffffffffu, ec, 1);
-          double yp = __shfl_down_sync(0xffffffffu, ec, 1);
-          double enp = __shfl_down_sync(0xffffffffu, en, 1);
-          if (lane == 0) ym = side;
-          if (lane == 31) {
-            yp = side;
-            enp = ns[u];
-          }
-          if (vy) {
-            double gx, gy;
-            if (ix == 0) gx = en - ec;
-            else if (ix == nx - 1) gx = ec - em;
-            else gx = (en - em) / 2.0;
-            if (y == 0) gy = yp - ec;
-            else if (y == ny - 1) gy = ec - ym;
-            else gy = (yp - ym) / 2.0;
-            acc[0] += gx * gx + gy * gy;
-            if (do_iface && ix < nx - 1 && y < ny - 1 && in_iface(ec) && in_iface(en) && in_iface(enp) &&
-                in_iface(yp))
-              acc[1] += 1.0;
-          }
-          em = ec;
-          ec = en;
-          side = ns[u];
-        }
+    for (int u = 0; u < kU; ++u) {
+      const int i = i0 + u * stride;
+      if (i >= N) break;
+      const int ix = i / ny, iy = i - ix * ny;
+      if (do_grad) {
+        double gx, gy;
+        if (ix == 0) gx = xp[u] - e[u];
+        else if (ix == nx - 1) gx = e[u] - xm[u];
+        else gx = (xp[u] - xm[u]) / 2.0;
+        if (iy == 0) gy = yp[u] - e[u];
+        else if (iy == ny - 1) gy = e[u] - ym[u];
+        else gy = (yp[u] - ym[u]) / 2.0;
+        acc[0] += gx * gx + gy * gy;
       }
+      if (do_iface && ix < nx - 1 && iy < ny - 1 && in_iface(e[u]) && in_iface(xp[u]) &&
+          in_iface(eta[i + ny + 1]) && in_iface(yp[u]))
+        acc[1] += 1.0;
     }
   }
   double a1[1] = {acc[0]};
   double a2[1] = {acc[1]};
-  block_reduce_store<1, kExtrasThreads>(a1, partials + (size_t)bx * KKS_NPART + P5_GRAD2);
+  if (do_grad) block_reduce_store<1, kExtrasThreads>(a1, partials + (size_t)bx * KKS_NPART + slot_grad);
   __syncthreads();
-  if (do_iface) block_reduce_store<1, kExtrasThreads>(a2, partials + (size_t)bx * KKS_NPART + P5_IFACE);
+  if (do_iface) block_reduce_store<1, kExtrasThreads>(a2, partials + (size_t)bx * KKS_NPART + slot_iface);
 }
 
 __global__ void __launch_bounds__(kExtrasThreads)
-    kf_extras_stream(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const double* __restrict__ eta,
-                     double* __restrict__ partials) {
-  extras_stream_body(c, par, eta, partials, (int)blockIdx.x);
+    kf_extras(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const double* __restrict__ eta,
+              int mode, int slot_grad, int slot_iface, double* __restrict__ partials) {
+  extras_body(c, par, eta, mode, slot_grad, slot_iface, partials, (int)blockIdx.x, (int)gridDim.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -1329,15 +1297,13 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
                   m.y);
 }
 
-// np.gradient energy and interface count of the candidate state (the same
-// streaming stencil and grid per cell as the single-cell attempt, so that both
-// write the same partial-sum rows)
+// np.gradient energy and interface count of the candidate state
 __global__ void __launch_bounds__(kExtrasThreads)
     kfb_extras(const KksCellDesc* __restrict__ cells, const int2* __restrict__ bmap) {
   const int2 m = bmap[blockIdx.x];
   const KksCellDesc* d = cells + m.x;
   const int q = d->par->parity ^ 1;
-  extras_stream_body(d->dc, d->par, d->eta[q], d->partials, m.y);
+  extras_body(d->dc, d->par, d->eta[q], 3, P5_GRAD2, P5_IFACE, d->partials, m.y, d->nbx);
 }
 
 // After a rejection (decided by this attempt): the rejected candidate becomes
@@ -1530,8 +1496,6 @@ size_t kks_fft_smem_bytes(int nx, int ny, int cols) {
 
 int kks_fft_row_blocks(int nx) { return (nx + 1) / 2; }
 
-int kks_fft_extras_blocks(int nx, int ny) { return (extras_warps(nx, ny) + kExtWarps - 1) / kExtWarps; }
-
 int kks_fft_partial_rows(int nx, int ny, int nbx) {
   int m = kks_fft_row_blocks(nx);
   const int cb = col_blocks(ny / 2 + 1, 1);  // the column pass that writes sums, at its finest tile
@@ -1574,9 +1538,8 @@ void kks_fft_launch_attempt(const KksFftLaunch& L, int p, cudaStream_t s) {
   KKS_FFT_DISPATCH(L.PY, KKS_ROWS)
 #undef KKS_ROWS
 #undef KKS_COLS
-  kf_extras_stream<<<kks_fft_extras_blocks(L.nx, L.ny), kExtrasThreads, 0, s>>>(L.dc, L.par,
-                                                                                 (const double*)f.eta[1 - p],
-                                                                                 f.partials);
+  kf_extras<<<L.nbx, kExtrasThreads, 0, s>>>(L.dc, L.par, (const double*)f.eta[1 - p], 3, P5_GRAD2, P5_IFACE,
+                                       f.partials);
 }
 
 int kks_fft_col_blocks(int nyh, int cols) { return col_blocks(nyh, cols); }
@@ -1626,7 +1589,7 @@ void kks_fft_launch_attempt_batch(const KksBatchLaunch& B, cudaStream_t s) {
   KKS_FFT_DISPATCH(B.PY, KKS_ROWS)
 #undef KKS_ROWS
 #undef KKS_COLS
-  kfb_extras<<<B.n_stencil, kExtrasThreads, 0, s>>>(B.cells, B.map_stencil);
+  kfb_extras<<<B.n_extras, kExtrasThreads, 0, s>>>(B.cells, B.map_extras);
   kks_launch_decide_batch(B.cells, B.n_cells, s);
   kfb_restore<<<B.n_extras, kExtrasThreads, 0, s>>>(B.cells, B.map_extras);
 }

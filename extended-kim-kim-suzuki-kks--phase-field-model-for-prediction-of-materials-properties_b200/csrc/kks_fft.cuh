@@ -72,8 +72,6 @@ size_t kks_fft_smem_bytes(int nx, int ny, int cols);
 // Blocks of a row pass, and an upper bound of the partial-sum rows the
 // pipeline writes with any column tile (the decide kernel reduces them).
 int kks_fft_row_blocks(int nx);
-// Blocks of the single-cell gradient / interface pass (one partial-sum row each).
-int kks_fft_extras_blocks(int nx, int ny);
 int kks_fft_partial_rows(int nx, int ny, int nbx);
 int kks_fft_set_attributes(const KksFftLaunch& L);
 // The prime-stage factor table of prime P (11, 19 or 71), rows padded to an
@@ -128,9 +126,8 @@ struct KksBatchLaunch {
   const int2* map_rows;    // row pairs
   const int2* map_cols;    // column tiles
   const int2* map_cols3;   // column tiles x 3 roles (first column pass)
-  const int2* map_extras;   // blocks of the restore kernel (nbx per cell)
-  const int2* map_stencil;  // blocks of the gradient / interface stencil (kks_fft_extras_blocks per cell)
-  int n_rows, n_cols, n_cols3, n_extras, n_stencil;
+  const int2* map_extras;  // blocks of the extras and restore kernels (nbx per cell)
+  int n_rows, n_cols, n_cols3, n_extras;
   size_t smem_rows_a, smem_rows_bc, smem_rows_d, smem_cols_ab, smem_cols_cd1, smem_cols_cd2;
 };
 
