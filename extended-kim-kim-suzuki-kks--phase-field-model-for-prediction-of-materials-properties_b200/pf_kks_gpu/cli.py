@@ -1,9 +1,9 @@
 """Command-line entry point, drop-in for ``pf-kks-run`` (``pf_kks/cli.py:25-56``).
 
 Same arguments and outputs: ``saved_maps/map*.npz``, ``history.npz``,
-``log.txt``, ``dtime.txt`` and ``config.json`` in ``--out``. Two additions:
-``--precision {fp64,mixed}`` and ``--device N`` (else taken from the ``[gpu]``
-section of the configuration).
+``log.txt``, ``dtime.txt`` and ``config.json`` in ``--out``. Additions:
+``--precision {fp64,mixed}``, ``--device N`` and ``--autotune`` (else taken
+from the ``[gpu]`` section of the configuration).
 
 Usage: python -m pf_kks_gpu.cli CONFIG --out DIR [--n-steps N] [--precision mixed]
 """
@@ -40,6 +40,8 @@ def main(argv=None):
     parser.add_argument("--quiet", action="store_true", help="do not print progress")
     parser.add_argument("--precision", choices=("fp64", "mixed"), help="GPU step precision")
     parser.add_argument("--device", type=int, help="CUDA device ordinal")
+    parser.add_argument("--autotune", action="store_true",
+                        help="time the launch shapes on the initial state first (cached per GPU and grid)")
     args = parser.parse_args(argv)
 
     cfg = load_config(args.config, n_steps=args.n_steps, fft_threads=args.fft_threads)
@@ -48,6 +50,10 @@ def main(argv=None):
         print(json.dumps(cfg.to_dict(), indent=2))
         return 0
 
+    if args.autotune:
+        opts = cfg.gpu_options
+        opts.autotune = True
+        cfg.gpu = opts
     os.makedirs(args.out, exist_ok=True)
     with open(os.path.join(args.out, "config.json"), "w") as f:
         json.dump(cfg.to_dict(), f, indent=2)

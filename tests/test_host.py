@@ -39,7 +39,10 @@ def test_gpu_section_and_overrides(tmp_path):
     cfg = C.load_config(p, n_steps=9, fft_threads=None)
     assert (cfg.nx, cfg.ny, cfg.n_steps) == (64, 32, 9)
     assert cfg.gpu_options.precision == "mixed" and cfg.gpu_options.device == 1
+    assert cfg.gpu_options.autotune is False
     assert "gpu" not in cfg.to_dict()
+    p.write_text("[gpu]\nprecision = \"mixed\"\nautotune = true\n")
+    assert C.load_config(p).gpu_options.autotune is True
     p.write_text("[gpu]\nprecision = \"fp16\"\n")
     with pytest.raises(ValueError):
         C.load_config(p)
