@@ -173,3 +173,21 @@ def test_batch_takes_each_cells_shape():
         cells[0].set_launch_shape(1, 3, 7)  # free again once the batch is gone
         for c in cells:
             c.close()
+
+
+def test_solver_run_with_autotune(tmp_path, monkeypatch):
+    """``[gpu] autotune = true``: solver.run tunes the cell on its initial
+    state (cached), and the run itself is the untuned run to the mixed bar."""
+    from pf_kks_gpu import solver
+
+    monkeypatch.setenv("KKS_AUTOTUNE_CACHE", str(tmp_path / "shapes.json"))
+    cfg, state = _member(96, 80, n_steps=12)
+    ref = solver.run(cfg, *copy_state(state), out_dir=str(tmp_path / "plain"), verbose=False, precision="mixed")
+    opts = cfg.gpu_options
+    opts.autotune = True
+    cfg.gpu = opts
+    got = solver.run(cfg, *copy_state(state), out_dir=str(tmp_path / "tuned"), verbose=False, precision="mixed")
+    for name in ("eta", "X"):
+        assert rel_l2(getattr(got, name), getattr(ref, name)) <= 1e-6, name
+    assert len(got.history["time"]) == len(ref.history["time"])
+    assert (tmp_path / "shapes.json").exists()
