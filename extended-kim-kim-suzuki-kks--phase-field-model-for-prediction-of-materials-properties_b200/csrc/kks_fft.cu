@@ -62,13 +62,27 @@ constexpr int kThreads = KKS_FFT_THREADS;
 // blocks per SM the register allocation must allow
 constexpr int kMinBlocks = 2;
 // Passes of grids without a large prime factor (small cells, whose blocks are
-// short and latency-bound) ask for three blocks per SM; the prime-stage passes
-// keep two (their warp tasks need 96 registers), and so does rows_D (its FP64
-// pointwise phase would spill). A batched pass and its single-cell twin use
+// short and latency-bound) ask for six blocks of five warps per SM (64
+// registers); the prime-stage passes keep two blocks of ten warps (their warp
+// tasks need 96 registers), and rows_D keeps 96 registers (its FP64 pointwise
+// phase would spill). A batched pass and its single-cell twin use
 // the same bound, so that both compile to the same arithmetic.
 template <int P>
-constexpr int pass_min_blocks() {
-  return P > 7 ? kMinBlocks : 3;
+__host__ __device__ constexpr int pass_min_blocks() {
+  return P > 7 ? kMinBlocks : 6;
+}
+// Threads of a pass block: ten warps where a prime stage needs one warp per
+// output group; five for grids without a large prime factor, whose rows and
+// columns are short (a radix-4 stage of three 128-point sequences has 96
+// butterflies), so that twice as many smaller blocks share an SM.
+template <int P>
+__host__ __device__ constexpr int pass_threads() {
+  return P > 7 ? kThreads : kThreads / 2;
+}
+// rows_D (96 registers: its FP64 pointwise phase) keeps 20 warps per SM.
+template <int P>
+__host__ __device__ constexpr int rows_d_min_blocks() {
+  return P > 7 ? kMinBlocks : 4;
 }
 
 __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
@@ -450,7 +464,7 @@ __device__ __forceinline__ void fft_run(int nseq, const KksFftAxis& ax) {
     const uint32_t qm = ax.qm[s], pm = ax.pm[s];
     const float2* tw = ax.tw + ax.tw_off[s];
     const int total = nseq * per;
-    for (int t = threadIdx.x; t < total; t += kThreads) {
+    for (int t = threadIdx.x; t < total; t += pass_threads<P>()) {
       const int sq = nseq == 1 ? 0 : fdiv(t, per, pm);
       const int bt = t - sq * per;
       const int b = fdiv(bt, q, qm);
@@ -497,10 +511,11 @@ __device__ __forceinline__ bool in_iface(double e) { return e >= 0.1 && e <= 0.9
 
 // Split the transform of (row a + i row b) (digit-reversed) into the half
 // spectra of rows ix0 (a) and ix0+1 (b) of a column-major row-spectrum field.
+template <int NT>
 __device__ __forceinline__ void split_store(const float2* z, const KksFftAxis& ay, float2* __restrict__ dst, int ix0,
                                             bool has1, int nx, int nyh) {
   const int ny = ay.n;
-  for (int k = threadIdx.x; k < nyh; k += kThreads) {
+  for (int k = threadIdx.x; k < nyh; k += NT) {
     const float2 Zk = z[__ldg(ay.slot + k)];
     const float2 Zm = z[__ldg(ay.slot + (k == 0 ? 0 : ny - k))];
     // A = (Z_k + conj Z_{-k}) / 2, B = (Z_k - conj Z_{-k}) / (2i)
@@ -514,10 +529,11 @@ __device__ __forceinline__ void split_store(const float2* z, const KksFftAxis& a
 // frequencies, the negative ones from the Hermitian extension. The y = 0 and
 // Nyquist bins of a real row are real: their imaginary round-off is dropped
 // (as a C2R transform does), so that it cannot leak into the other row.
+template <int NT>
 __device__ __forceinline__ void merge_load(float2* z, const KksFftAxis& ay, const float2* __restrict__ src, int ix0,
                                            bool has1, int nx, int nyh) {
   const int ny = ay.n;
-  for (int k = threadIdx.x; k < nyh; k += kThreads) {
+  for (int k = threadIdx.x; k < nyh; k += NT) {
     const float2* s = src + (size_t)k * nx + ix0;
     float2 A = s[0];
     float2 B = has1 ? s[1] : make_float2(0.f, 0.f);
@@ -534,10 +550,11 @@ __device__ __forceinline__ void merge_load(float2* z, const KksFftAxis& ay, cons
 
 // split_store / merge_load against a staged box set (field f of F) instead of
 // global memory; the tensor copies move the boxes.
+template <int NT>
 __device__ __forceinline__ void split_stage(const float2* z, const KksFftAxis& ay, float2* stage, int f, int F,
                                             int kb, int nyh) {
   const int ny = ay.n;
-  for (int k = threadIdx.x; k < nyh; k += kThreads) {
+  for (int k = threadIdx.x; k < nyh; k += NT) {
     const float2 Zk = z[__ldg(ay.slot + k)];
     const float2 Zm = z[__ldg(ay.slot + (k == 0 ? 0 : ny - k))];
     const int i = stage_at(k, f, F, kb, 0);
@@ -546,10 +563,11 @@ __device__ __forceinline__ void split_stage(const float2* z, const KksFftAxis& a
   }
 }
 
+template <int NT>
 __device__ __forceinline__ void merge_stage(float2* z, const KksFftAxis& ay, const float2* stage, int f, int F, int kb,
                                             int nyh) {
   const int ny = ay.n;
-  for (int k = threadIdx.x; k < nyh; k += kThreads) {
+  for (int k = threadIdx.x; k < nyh; k += NT) {
     const int i = stage_at(k, f, F, kb, 0);
     float2 A = stage[i], B = stage[i + 1];
     const bool self = k == 0 || 2 * k == ny;
@@ -584,6 +602,7 @@ template <int PY>
 __device__ __forceinline__ void rows_A_body(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const KksFftConst* __restrict__ fc,
               const double* __restrict__ eta, const double* __restrict__ X, float2* __restrict__ RA,
               double* __restrict__ partials, KksCtl* ctl, int bulk, const CUtensorMap* map_RA, int bx) {
+  constexpr int NT = pass_threads<PY>();
   if (!par->active) return;
   prime_table_fill<PY>(fc->ay.ptw);
   extern __shared__ float2 sm[];
@@ -610,7 +629,7 @@ __device__ __forceinline__ void rows_A_body(const KksConst* __restrict__ c, cons
   }
   const bool surface = par->surface;
   double acc[6] = {0, 0, 0, 0, 0, 0};
-  for (int y = threadIdx.x; y < ny; y += kThreads) {
+  for (int y = threadIdx.x; y < ny; y += NT) {
     double e0, x0, e1, x1;
     if (bulk) {
       e0 = s_eta[y], x0 = s_X[y], e1 = s_eta[ny + y], x1 = s_X[ny + y];
@@ -644,19 +663,19 @@ __device__ __forceinline__ void rows_A_body(const KksConst* __restrict__ c, cons
   if (bulk) {
     const int kb = nyh < 256 ? nyh : 256, nb = (nyh + kb - 1) / kb;
     float2* st = (float2*)stage;
-    for (int f = 0; f < 3; ++f) split_stage(sm + f * ny, ay, st, f, 3, kb, nyh);
+    for (int f = 0; f < 3; ++f) split_stage<NT>(sm + f * ny, ay, st, f, 3, kb, nyh);
     fence_async_smem();
     __syncthreads();
     if (threadIdx.x == 0) stage_store(map_RA, st, ix0, 3, kb, nb);
   } else {
-    for (int f = 0; f < 3; ++f) split_store(sm + f * ny, ay, RA + f * fs, ix0, has1, nx, nyh);
+    for (int f = 0; f < 3; ++f) split_store<NT>(sm + f * ny, ay, RA + f * fs, ix0, has1, nx, nyh);
   }
   static_assert(P3_IFACE == P3_ETA + 5, "rows_A writes P3_ETA .. P3_IFACE");
-  block_reduce_store<6>(acc, partials + (size_t)bx * KKS_NPART + P3_ETA);
+  block_reduce_store<6, NT>(acc, partials + (size_t)bx * KKS_NPART + P3_ETA);
 }
 
 template <int PY>
-__global__ void __launch_bounds__(kThreads, pass_min_blocks<PY>())
+__global__ void __launch_bounds__(pass_threads<PY>(), pass_min_blocks<PY>())
     kf_rows_A(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const KksFftConst* __restrict__ fc,
               const double* __restrict__ eta, const double* __restrict__ X, float2* __restrict__ RA,
               double* __restrict__ partials, KksCtl* ctl, int bulk, const __grid_constant__ CUtensorMap map_RA) {
@@ -670,6 +689,7 @@ template <int PX>
 __device__ __forceinline__ void cols_AB_body(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const KksFftConst* __restrict__ fc,
                const float2* __restrict__ RA, float2* __restrict__ SA, float2* __restrict__ RB,
                const double* __restrict__ kys, double* __restrict__ partials, KksCtl* ctl, int bulk, int bx, int by) {
+  constexpr int NT = pass_threads<PX>();
   if (!par->active) return;
   prime_table_fill<PX>(fc->ax.ptw);
   extern __shared__ float2 sm[];
@@ -694,13 +714,13 @@ __device__ __forceinline__ void cols_AB_body(const KksConst* __restrict__ c, con
     __syncthreads();
     bulk_wait(&bar, 0, ctl);
   } else {
-    for (int i = threadIdx.x; i < nv; i += kThreads) sm[i] = col[i];
+    for (int i = threadIdx.x; i < nv; i += NT) sm[i] = col[i];
     __syncthreads();
   }
   fft_run<-1, PX>(ncol, ax);
   if (g != 1) {
     float2* dst = SA + (g == 2 ? fs : 0) + (size_t)ky0 * nx;
-    for (int i = threadIdx.x; i < nv; i += kThreads) dst[i] = sm[i];
+    for (int i = threadIdx.x; i < nv; i += NT) dst[i] = sm[i];
     if (g == 2) return;
   }
   const float inv_N = (float)c->inv_N;
@@ -712,7 +732,7 @@ __device__ __forceinline__ void cols_AB_body(const KksConst* __restrict__ c, con
     const float ky = (float)kys[iy];
     const double w = (iy == 0 || 2 * iy == ny) ? 1.0 : 2.0;
     float2* z = sm + cc * nx;
-    for (int p = threadIdx.x; p < nx; p += kThreads) {
+    for (int p = threadIdx.x; p < nx; p += NT) {
       const float kx = __ldg(fc->kx_slot + p);
       const float2 v = z[p];
       if (g == 0) {
@@ -744,25 +764,25 @@ __device__ __forceinline__ void cols_AB_body(const KksConst* __restrict__ c, con
       }
     }
   }
-  if (g == 1) block_reduce_store<6>(acc, partials + (size_t)bx * KKS_NPART + P2_OXX2);
+  if (g == 1) block_reduce_store<6, NT>(acc, partials + (size_t)bx * KKS_NPART + P2_OXX2);
   __syncthreads();
   // g = 0: the i k_x columns at [0, nv), the i k_y columns at [nv, 2 nv)
   fft_run<+1, PX>(g == 0 ? 2 * ncol : ncol, ax);
   if (g == 0) {
     float2* dx = RB + fs + (size_t)ky0 * nx;
     float2* dy = RB + 2 * fs + (size_t)ky0 * nx;
-    for (int i = threadIdx.x; i < nv; i += kThreads) {
+    for (int i = threadIdx.x; i < nv; i += NT) {
       dx[i] = sm[i];
       dy[i] = sm[nv + i];
     }
   } else {
     float2* dst = RB + (size_t)ky0 * nx;
-    for (int i = threadIdx.x; i < nv; i += kThreads) dst[i] = sm[i];
+    for (int i = threadIdx.x; i < nv; i += NT) dst[i] = sm[i];
   }
 }
 
 template <int PX>
-__global__ void __launch_bounds__(kThreads, pass_min_blocks<PX>())
+__global__ void __launch_bounds__(pass_threads<PX>(), pass_min_blocks<PX>())
     kf_cols_AB(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const KksFftConst* __restrict__ fc,
                const float2* __restrict__ RA, float2* __restrict__ SA, float2* __restrict__ RB,
                const double* __restrict__ kys, double* __restrict__ partials, KksCtl* ctl, int bulk) {
@@ -778,6 +798,7 @@ __device__ __forceinline__ void rows_BC_body(const KksConst* __restrict__ c, con
                const float* __restrict__ Xal, const float* __restrict__ Xth, float* g0, float* g1, float* g2,
                double* __restrict__ partials, KksCtl* ctl, int bulk, const CUtensorMap* map_RB,
                const CUtensorMap* map_RC, int bx) {
+  constexpr int NT = pass_threads<PY>();
   if (!par->active) return;
   prime_table_fill<PY>(fc->ay.ptw);
   extern __shared__ float2 sm[];
@@ -803,7 +824,7 @@ __device__ __forceinline__ void rows_BC_body(const KksConst* __restrict__ c, con
     }
     __syncthreads();
     bulk_wait(&bar, 0, ctl);
-    for (int f = 0; f < 3; ++f) merge_stage(sm + f * ny, ay, st, f, 3, kb, nyh);
+    for (int f = 0; f < 3; ++f) merge_stage<NT>(sm + f * ny, ay, st, f, 3, kb, nyh);
     __syncthreads();
     if (threadIdx.x == 0) {
       const size_t i0 = (size_t)ix0 * ny;
@@ -814,7 +835,7 @@ __device__ __forceinline__ void rows_BC_body(const KksConst* __restrict__ c, con
       bulk_g2s((void*)s_th, Xth + i0, 8u * ny, &bar);
     }
   } else {
-    for (int f = 0; f < 3; ++f) merge_load(sm + f * ny, ay, RB + f * fs, ix0, has1, nx, nyh);
+    for (int f = 0; f < 3; ++f) merge_load<NT>(sm + f * ny, ay, RB + f * fs, ix0, has1, nx, nyh);
     __syncthreads();
   }
   fft_run<+1, PY>(3, ay);
@@ -826,7 +847,7 @@ __device__ __forceinline__ void rows_BC_body(const KksConst* __restrict__ c, con
   const float epsX = (float)q.epsX;
   const float c3 = (float)((c->C11_0 + 2 * c->C12_0) * q.inv_C44);
   double accG = 0.0;
-  for (int y = threadIdx.x; y < ny; y += kThreads) {
+  for (int y = threadIdx.x; y < ny; y += NT) {
     const float2 tr = sm[y], gx = sm[ny + y], gy = sm[2 * ny + y];
     float dr[2], fxv[2], fyv[2];
 #pragma unroll
@@ -864,19 +885,19 @@ __device__ __forceinline__ void rows_BC_body(const KksConst* __restrict__ c, con
   __syncthreads();
   fft_run<-1, PY>(3, ay);
   if (bulk) {
-    for (int f = 0; f < 3; ++f) split_stage(sm + f * ny, ay, st, f, 3, kb, nyh);
+    for (int f = 0; f < 3; ++f) split_stage<NT>(sm + f * ny, ay, st, f, 3, kb, nyh);
     fence_async_smem();
     __syncthreads();
     if (threadIdx.x == 0) stage_store(map_RC, st, ix0, 3, kb, nb);
   } else {
-    for (int f = 0; f < 3; ++f) split_store(sm + f * ny, ay, RC + f * fs, ix0, has1, nx, nyh);
+    for (int f = 0; f < 3; ++f) split_store<NT>(sm + f * ny, ay, RC + f * fs, ix0, has1, nx, nyh);
   }
   double acc[1] = {accG};
-  block_reduce_store<1>(acc, partials + (size_t)bx * KKS_NPART + P3_G);
+  block_reduce_store<1, NT>(acc, partials + (size_t)bx * KKS_NPART + P3_G);
 }
 
 template <int PY>
-__global__ void __launch_bounds__(kThreads, pass_min_blocks<PY>())
+__global__ void __launch_bounds__(pass_threads<PY>(), pass_min_blocks<PY>())
     kf_rows_BC(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const KksFftConst* __restrict__ fc,
                const float2* __restrict__ RB, float2* __restrict__ RC, const double* __restrict__ eta,
                const float* __restrict__ Xal, const float* __restrict__ Xth, float* g0, float* g1, float* g2,
@@ -890,6 +911,7 @@ template <int PX>
 __device__ __forceinline__ void cols_CD_eta_body(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const KksFftConst* __restrict__ fc,
                    const float2* __restrict__ RC, const float2* __restrict__ SA, float2* __restrict__ RD,
                    const double* __restrict__ kys, KksCtl* ctl, int bulk, int bx) {
+  constexpr int NT = pass_threads<PX>();
   if (!par->active) return;
   prime_table_fill<PX>(fc->ax.ptw);
   extern __shared__ float2 sm[];
@@ -917,7 +939,7 @@ __device__ __forceinline__ void cols_CD_eta_body(const KksConst* __restrict__ c,
       bulk_g2s(s_sa, SA + (size_t)ky0 * nx, 8u * nv, &bar);
     }
   } else {
-    for (int i = threadIdx.x; i < nv; i += kThreads) sm[i] = col[i];
+    for (int i = threadIdx.x; i < nv; i += NT) sm[i] = col[i];
     __syncthreads();
   }
   fft_run<-1, PX>(ncol, ax);
@@ -928,7 +950,7 @@ __device__ __forceinline__ void cols_CD_eta_body(const KksConst* __restrict__ c,
     const float ky = (float)kys[ky0 + cc];
     const float2* ecol = bulk ? s_sa + cc * nx : SA + (size_t)(ky0 + cc) * nx;
     float2* z = sm + cc * nx;
-    for (int p = threadIdx.x; p < nx; p += kThreads) {
+    for (int p = threadIdx.x; p < nx; p += NT) {
       const float kx = __ldg(fc->kx_slot + p);
       const float k2 = kx * kx + ky * ky;
       const float2 dh = z[p];
@@ -940,11 +962,11 @@ __device__ __forceinline__ void cols_CD_eta_body(const KksConst* __restrict__ c,
   __syncthreads();
   fft_run<+1, PX>(ncol, ax);
   float2* dst = RD + (size_t)ky0 * nx;
-  for (int i = threadIdx.x; i < nv; i += kThreads) dst[i] = sm[i];
+  for (int i = threadIdx.x; i < nv; i += NT) dst[i] = sm[i];
 }
 
 template <int PX>
-__global__ void __launch_bounds__(kThreads, pass_min_blocks<PX>())
+__global__ void __launch_bounds__(pass_threads<PX>(), pass_min_blocks<PX>())
     kf_cols_CD_eta(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const KksFftConst* __restrict__ fc,
                    const float2* __restrict__ RC, const float2* __restrict__ SA, float2* __restrict__ RD,
                    const double* __restrict__ kys, KksCtl* ctl, int bulk) {
@@ -956,6 +978,7 @@ template <int PX>
 __device__ __forceinline__ void cols_CD_X_body(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const KksFftConst* __restrict__ fc,
                  const float2* __restrict__ RC, const float2* __restrict__ SA, float2* __restrict__ RD,
                  const double* __restrict__ kys, KksCtl* ctl, int bulk, int bx) {
+  constexpr int NT = pass_threads<PX>();
   if (!par->active) return;
   prime_table_fill<PX>(fc->ax.ptw);
   extern __shared__ float2 sm[];
@@ -987,7 +1010,7 @@ __device__ __forceinline__ void cols_CD_X_body(const KksConst* __restrict__ c, c
       bulk_g2s(s_sa, SA + fs + (size_t)ky0 * nx, 8u * nv, &bar);
     }
   } else {
-    for (int i = threadIdx.x; i < nv; i += kThreads) {
+    for (int i = threadIdx.x; i < nv; i += NT) {
       sm[i] = cx[i];
       sm[nv + i] = cy[i];
     }
@@ -1003,7 +1026,7 @@ __device__ __forceinline__ void cols_CD_X_body(const KksConst* __restrict__ c, c
     const float2* xcol = bulk ? s_sa + cc * nx : SA + fs + (size_t)(ky0 + cc) * nx;
     float2* z = sm + cc * nx;
     const float2* zy = sm + nv + cc * nx;
-    for (int p = threadIdx.x; p < nx; p += kThreads) {
+    for (int p = threadIdx.x; p < nx; p += NT) {
       const float kx = __ldg(fc->kx_slot + p);
       const float k2 = kx * kx + ky * ky;
       const float2 fx = z[p], fy = zy[p];
@@ -1017,11 +1040,11 @@ __device__ __forceinline__ void cols_CD_X_body(const KksConst* __restrict__ c, c
   __syncthreads();
   fft_run<+1, PX>(ncol, ax);
   float2* dst = RD + fs + (size_t)ky0 * nx;
-  for (int i = threadIdx.x; i < nv; i += kThreads) dst[i] = sm[i];
+  for (int i = threadIdx.x; i < nv; i += NT) dst[i] = sm[i];
 }
 
 template <int PX>
-__global__ void __launch_bounds__(kThreads, pass_min_blocks<PX>())
+__global__ void __launch_bounds__(pass_threads<PX>(), pass_min_blocks<PX>())
     kf_cols_CD_X(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const KksFftConst* __restrict__ fc,
                  const float2* __restrict__ RC, const float2* __restrict__ SA, float2* __restrict__ RD,
                  const double* __restrict__ kys, KksCtl* ctl, int bulk) {
@@ -1037,6 +1060,7 @@ __device__ __forceinline__ void rows_D_body(const KksConst* __restrict__ c, cons
               float* __restrict__ Xth_b, const double* __restrict__ eta_m, const double* __restrict__ X_m,
               float* __restrict__ mu, float* g0, float* g1, float* g2, double* __restrict__ partials, KksCtl* ctl,
               int bulk, const CUtensorMap* map_RD, int bx) {
+  constexpr int NT = pass_threads<PY>();
   if (!par->active) return;
   prime_table_fill<PY>(fc->ay.ptw);
   extern __shared__ float2 sm[];
@@ -1061,8 +1085,8 @@ __device__ __forceinline__ void rows_D_body(const KksConst* __restrict__ c, cons
     }
     __syncthreads();
     bulk_wait(&bar, 0, ctl);
-    merge_stage(sm, ay, st, 0, 2, kb, nyh);
-    merge_stage(sm + ny, ay, st, 1, 2, kb, nyh);
+    merge_stage<NT>(sm, ay, st, 0, 2, kb, nyh);
+    merge_stage<NT>(sm + ny, ay, st, 1, 2, kb, nyh);
     __syncthreads();
     if (threadIdx.x == 0) {
       const size_t i0 = (size_t)ix0 * ny;
@@ -1072,8 +1096,8 @@ __device__ __forceinline__ void rows_D_body(const KksConst* __restrict__ c, cons
       bulk_g2s((void*)s_X, X_o + i0, 16u * ny, &bar);
     }
   } else {
-    merge_load(sm, ay, RD, ix0, has1, nx, nyh);
-    merge_load(sm + ny, ay, RD + fs, ix0, has1, nx, nyh);
+    merge_load<NT>(sm, ay, RD, ix0, has1, nx, nyh);
+    merge_load<NT>(sm + ny, ay, RD + fs, ix0, has1, nx, nyh);
     __syncthreads();
   }
   fft_run<+1, PY>(2, ay);
@@ -1087,7 +1111,7 @@ __device__ __forceinline__ void rows_D_body(const KksConst* __restrict__ c, cons
   const float A_t = (float)q.A_thet_s, vt = (float)q.vt, ft0 = (float)q.ft0, w_s = (float)q.w_s;
   const double dt = q.dt;
   double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-  for (int y = threadIdx.x; y < ny; y += kThreads) {
+  for (int y = threadIdx.x; y < ny; y += NT) {
     const float2 de = sm[y], dX = sm[ny + y];
 #pragma unroll
     for (int r = 0; r < 2; ++r) {
@@ -1142,14 +1166,14 @@ __device__ __forceinline__ void rows_D_body(const KksConst* __restrict__ c, cons
   }
   // slots P5_XLO, NLO, XHI, NHI, ETA are consecutive; DIFF, AC, TEMP, COMB follow P5_IFACE
   double a5[5] = {acc[0], acc[1], acc[2], acc[3], acc[4]};
-  block_reduce_store<5>(a5, partials + (size_t)bx * KKS_NPART + P5_XLO);
+  block_reduce_store<5, NT>(a5, partials + (size_t)bx * KKS_NPART + P5_XLO);
   __syncthreads();
   double a4[4] = {acc[5], acc[6], acc[7], acc[8]};
-  block_reduce_store<4>(a4, partials + (size_t)bx * KKS_NPART + P5_DIFF);
+  block_reduce_store<4, NT>(a4, partials + (size_t)bx * KKS_NPART + P5_DIFF);
 }
 
 template <int PY>
-__global__ void __launch_bounds__(kThreads, kMinBlocks)
+__global__ void __launch_bounds__(pass_threads<PY>(), rows_d_min_blocks<PY>())
     kf_rows_D(const KksConst* __restrict__ c, const KksPar* __restrict__ par, const KksFftConst* __restrict__ fc,
               const float2* __restrict__ RD, const double* __restrict__ eta_o, const double* __restrict__ X_o,
               double* __restrict__ eta_b, double* __restrict__ X_b, float* __restrict__ Xal_b,
@@ -1236,7 +1260,7 @@ __device__ __forceinline__ void tensormap_acquire(const CUtensorMap* map) {
 }
 
 template <int PY>
-__global__ void __launch_bounds__(kThreads, pass_min_blocks<PY>())
+__global__ void __launch_bounds__(pass_threads<PY>(), pass_min_blocks<PY>())
     kfb_rows_A(const KksCellDesc* __restrict__ cells, const int2* __restrict__ bmap) {
   const int2 m = bmap[blockIdx.x];
   const KksCellDesc* d = cells + m.x;
@@ -1247,7 +1271,7 @@ __global__ void __launch_bounds__(kThreads, pass_min_blocks<PY>())
 }
 
 template <int PX>
-__global__ void __launch_bounds__(kThreads, pass_min_blocks<PX>())
+__global__ void __launch_bounds__(pass_threads<PX>(), pass_min_blocks<PX>())
     kfb_cols_AB(const KksCellDesc* __restrict__ cells, const int2* __restrict__ bmap) {
   const int2 m = bmap[blockIdx.x];
   const KksCellDesc* d = cells + m.x;
@@ -1256,7 +1280,7 @@ __global__ void __launch_bounds__(kThreads, pass_min_blocks<PX>())
 }
 
 template <int PY>
-__global__ void __launch_bounds__(kThreads, pass_min_blocks<PY>())
+__global__ void __launch_bounds__(pass_threads<PY>(), pass_min_blocks<PY>())
     kfb_rows_BC(const KksCellDesc* __restrict__ cells, const int2* __restrict__ bmap) {
   const int2 m = bmap[blockIdx.x];
   const KksCellDesc* d = cells + m.x;
@@ -1270,7 +1294,7 @@ __global__ void __launch_bounds__(kThreads, pass_min_blocks<PY>())
 }
 
 template <int PX>
-__global__ void __launch_bounds__(kThreads, pass_min_blocks<PX>())
+__global__ void __launch_bounds__(pass_threads<PX>(), pass_min_blocks<PX>())
     kfb_cols_CD_eta(const KksCellDesc* __restrict__ cells, const int2* __restrict__ bmap) {
   const int2 m = bmap[blockIdx.x];
   const KksCellDesc* d = cells + m.x;
@@ -1278,7 +1302,7 @@ __global__ void __launch_bounds__(kThreads, pass_min_blocks<PX>())
 }
 
 template <int PX>
-__global__ void __launch_bounds__(kThreads, pass_min_blocks<PX>())
+__global__ void __launch_bounds__(pass_threads<PX>(), pass_min_blocks<PX>())
     kfb_cols_CD_X(const KksCellDesc* __restrict__ cells, const int2* __restrict__ bmap) {
   const int2 m = bmap[blockIdx.x];
   const KksCellDesc* d = cells + m.x;
@@ -1286,7 +1310,7 @@ __global__ void __launch_bounds__(kThreads, pass_min_blocks<PX>())
 }
 
 template <int PY>
-__global__ void __launch_bounds__(kThreads, kMinBlocks)
+__global__ void __launch_bounds__(pass_threads<PY>(), rows_d_min_blocks<PY>())
     kfb_rows_D(const KksCellDesc* __restrict__ cells, const int2* __restrict__ bmap) {
   const int2 m = bmap[blockIdx.x];
   const KksCellDesc* d = cells + m.x;
@@ -1365,15 +1389,15 @@ void launch_rows(const KksFftLaunch& L, int p, int stage, cudaStream_t s) {
   float2* RA = (float2*)L.RA;
   float2* RB = (float2*)L.RB;
   if (stage == 0) {
-    kf_rows_A<PY><<<npairs, kThreads, rows_a_smem(L.ny), s>>>(dc, par, L.fc, (const double*)f.eta[p],
+    kf_rows_A<PY><<<npairs, pass_threads<PY>(), rows_a_smem(L.ny), s>>>(dc, par, L.fc, (const double*)f.eta[p],
                                                                (const double*)f.X[p], RA, f.partials, L.ctl,
                                                                L.bulk_rows, L.map_RA3);
   } else if (stage == 1) {
-    kf_rows_BC<PY><<<npairs, kThreads, rows_bc_smem(L.ny), s>>>(
+    kf_rows_BC<PY><<<npairs, pass_threads<PY>(), rows_bc_smem(L.ny), s>>>(
         dc, par, L.fc, RB, RA, (const double*)f.eta[p], (const float*)f.X_al[p], (const float*)f.X_th[p],
         (float*)f.g[0], (float*)f.g[1], (float*)f.g[2], f.partials, L.ctl, L.bulk_rows, L.map_RB3, L.map_RA3);
   } else {
-    kf_rows_D<PY><<<npairs, kThreads, rows_d_smem(L.ny), s>>>(
+    kf_rows_D<PY><<<npairs, pass_threads<PY>(), rows_d_smem(L.ny), s>>>(
         dc, par, L.fc, RB, (const double*)f.eta[p], (const double*)f.X[p], (double*)f.eta[q], (double*)f.X[q],
         (float*)f.X_al[q], (float*)f.X_th[q], (const double*)f.eta_m, (const double*)f.X_m, (float*)f.mu,
         (float*)f.g[0], (float*)f.g[1], (float*)f.g[2], f.partials, L.ctl, L.bulk_rows, L.map_RB2);
@@ -1387,12 +1411,12 @@ void launch_cols(const KksFftLaunch& L, int stage, cudaStream_t s) {
   float2* SA = (float2*)L.SA;
   const int nb = col_blocks(L.nyh, L.cols);
   if (stage == 0) {
-    kf_cols_AB<PX><<<dim3(nb, 3), kThreads, seq_smem(L.nx, 2 * L.cols), s>>>(
+    kf_cols_AB<PX><<<dim3(nb, 3), pass_threads<PX>(), seq_smem(L.nx, 2 * L.cols), s>>>(
         L.dc, L.par, L.fc, RA, SA, RB, L.f->ky, L.f->partials, L.ctl, L.bulk_cols);
   } else {
-    kf_cols_CD_eta<PX><<<nb, kThreads, cols_cd_smem(L.nx, 1, L.cols), s>>>(L.dc, L.par, L.fc, RA, SA, RB, L.f->ky,
+    kf_cols_CD_eta<PX><<<nb, pass_threads<PX>(), cols_cd_smem(L.nx, 1, L.cols), s>>>(L.dc, L.par, L.fc, RA, SA, RB, L.f->ky,
                                                                             L.ctl, L.bulk_cols);
-    kf_cols_CD_X<PX><<<nb, kThreads, cols_cd_smem(L.nx, 2, L.cols), s>>>(L.dc, L.par, L.fc, RA, SA, RB, L.f->ky,
+    kf_cols_CD_X<PX><<<nb, pass_threads<PX>(), cols_cd_smem(L.nx, 2, L.cols), s>>>(L.dc, L.par, L.fc, RA, SA, RB, L.f->ky,
                                                                           L.ctl, L.bulk_cols);
   }
 }
@@ -1414,20 +1438,20 @@ cudaError_t set_attr(K* kernel, size_t smem) {
 template <int PY>
 void launch_rows_batch(const KksBatchLaunch& B, int stage, cudaStream_t s) {
   if (stage == 0)
-    kfb_rows_A<PY><<<B.n_rows, kThreads, B.smem_rows_a, s>>>(B.cells, B.map_rows);
+    kfb_rows_A<PY><<<B.n_rows, pass_threads<PY>(), B.smem_rows_a, s>>>(B.cells, B.map_rows);
   else if (stage == 1)
-    kfb_rows_BC<PY><<<B.n_rows, kThreads, B.smem_rows_bc, s>>>(B.cells, B.map_rows);
+    kfb_rows_BC<PY><<<B.n_rows, pass_threads<PY>(), B.smem_rows_bc, s>>>(B.cells, B.map_rows);
   else
-    kfb_rows_D<PY><<<B.n_rows, kThreads, B.smem_rows_d, s>>>(B.cells, B.map_rows);
+    kfb_rows_D<PY><<<B.n_rows, pass_threads<PY>(), B.smem_rows_d, s>>>(B.cells, B.map_rows);
 }
 
 template <int PX>
 void launch_cols_batch(const KksBatchLaunch& B, int stage, cudaStream_t s) {
   if (stage == 0) {
-    kfb_cols_AB<PX><<<B.n_cols3, kThreads, B.smem_cols_ab, s>>>(B.cells, B.map_cols3);
+    kfb_cols_AB<PX><<<B.n_cols3, pass_threads<PX>(), B.smem_cols_ab, s>>>(B.cells, B.map_cols3);
   } else {
-    kfb_cols_CD_eta<PX><<<B.n_cols, kThreads, B.smem_cols_cd1, s>>>(B.cells, B.map_cols);
-    kfb_cols_CD_X<PX><<<B.n_cols, kThreads, B.smem_cols_cd2, s>>>(B.cells, B.map_cols);
+    kfb_cols_CD_eta<PX><<<B.n_cols, pass_threads<PX>(), B.smem_cols_cd1, s>>>(B.cells, B.map_cols);
+    kfb_cols_CD_X<PX><<<B.n_cols, pass_threads<PX>(), B.smem_cols_cd2, s>>>(B.cells, B.map_cols);
   }
 }
 
