@@ -62,27 +62,29 @@ constexpr int kThreads = KKS_FFT_THREADS;
 // blocks per SM the register allocation must allow
 constexpr int kMinBlocks = 2;
 // Passes of grids without a large prime factor (small cells, whose blocks are
-// short and latency-bound) ask for six blocks of five warps per SM (64
+// short and latency-bound) ask for eight blocks of four warps per SM (64
 // registers); the prime-stage passes keep two blocks of ten warps (their warp
 // tasks need 96 registers), and rows_D keeps 96 registers (its FP64 pointwise
 // phase would spill). A batched pass and its single-cell twin use
 // the same bound, so that both compile to the same arithmetic.
 template <int P>
 __host__ __device__ constexpr int pass_min_blocks() {
-  return P > 7 ? kMinBlocks : 6;
+  return P > 7 ? kMinBlocks : 8;
 }
 // Threads of a pass block: ten warps where a prime stage needs one warp per
-// output group; five for grids without a large prime factor, whose rows and
+// output group; four for grids without a large prime factor, whose rows and
 // columns are short (a radix-4 stage of three 128-point sequences has 96
-// butterflies), so that twice as many smaller blocks share an SM.
+// butterflies), so that more, smaller blocks share an SM (measured on the
+// 48-cell ensemble: 8 warps 1.20, 5 warps 0.84, 4 warps 0.81 ms per batch
+// attempt).
 template <int P>
 __host__ __device__ constexpr int pass_threads() {
-  return P > 7 ? kThreads : kThreads / 2;
+  return P > 7 ? kThreads : 128;
 }
 // rows_D (96 registers: its FP64 pointwise phase) keeps 20 warps per SM.
 template <int P>
 __host__ __device__ constexpr int rows_d_min_blocks() {
-  return P > 7 ? kMinBlocks : 4;
+  return P > 7 ? kMinBlocks : 5;
 }
 
 __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
