@@ -236,3 +236,25 @@ def test_ensemble_tunes_the_batch(relaxed_state):
         c.run(5)
         _assert_fields_close(c.download(), g, f"{cfg.nx}x{cfg.ny}")
         c.close()
+
+
+@pytest.mark.parametrize("shapes", [((40, 38), (60, 76), (45, 38)), ((1420, 1420), (1420, 1420))],
+                         ids=["prime19", "prime71"])
+def test_batch_with_a_prime_stage(shapes):
+    """Batches whose cells share a large prime factor of the y axis (19, or 71
+    as at 1420 = 4 * 5 * 71: the batched prime-stage kernels, ten-warp blocks)
+    against the same cells run alone; odd and non-multiple-of-4 sides take the
+    plain-load paths, 1420^2 the tensor copies."""
+    from pf_kks_gpu import workloads
+    from pf_kks_gpu.generator import MicrostructureSpec
+
+    members = []
+    for k, (nx, ny) in enumerate(shapes):
+        cfg = workloads.base_config(nx=nx, ny=ny, n_steps=6, n_map_saves=2, n_surface_samples=3)
+        big = nx * ny > 10 ** 6
+        spec = MicrostructureSpec(nx, ny, n_cells=40 if big else 3, n_particles=1200 if big else 4, seed=30 + k)
+        members.append((cfg, workloads.initial_state(cfg, spec)))
+    plan = [[4]] * len(members)
+    ref = _alone(members, plan)
+    got = _batched(members, plan, groups=2)
+    _assert_same(got, ref)
