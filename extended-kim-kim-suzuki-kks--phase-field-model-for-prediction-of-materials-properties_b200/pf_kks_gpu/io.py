@@ -1,55 +1,49 @@
 """Simulation maps (``.npz`` snapshots) and their file names.
 
-Byte-compatible with ``pf_kks.io`` (``pf_kks/io.py:20-62``): same keys, dtypes
-and ``map{ttime:.2f}s_{T_start}_{T_max:.2f}K.npz`` names, so maps written by
-either implementation can be read by the other's tools.
+The map is a data format shared with ``pf_kks.io`` (``pf_kks/io.py:20-40``):
+the same ``.npz`` keys and dtypes and the same file name
+``map{ttime:.2f}s_{T_start}_{T_max:.2f}K.npz``, so that maps written by either
+implementation can be read by the other's tools.
 """
 
-import glob
 import os
-import re
 
 import numpy as np
 
-MAP_PATTERN = re.compile(r"map(?P<ttime>[0-9.]+)s_(?P<T_start>[0-9.]+)_(?P<T_max>[0-9.]+)K\.npz$")
+# Map keys, in the order they are written: the run time, six history lists
+# up to the save step and the four fields (nx, ny, 1).
+HISTORY_KEYS = (("time_out", "time"), ("T_out", "T"), ("X_al_mean_out", "X_al_mean"),
+                ("X_th_mean_out", "X_th_mean"), ("eta_mean_out", "eta_mean"), ("surf_out", "surf"))
+FIELD_KEYS = ("X", "X_al", "X_th", "eta")
 
 
 def map_filename(ttime, T_start, T_max):
-    """Map file name without extension (pf_kks/io.py:20-22)."""
-    return "map" + "{0:.2f}".format(ttime) + "s_" + str(T_start) + "_" + "{0:.2f}".format(T_max) + "K"
+    """Map file name without extension: the run time and the maximum
+    temperature with two decimals, the start temperature as Python prints it."""
+    return f"map{ttime:.2f}s_{T_start}_{T_max:.2f}K"
 
 
 def save_map(path, ttime, hist, X, X_al, X_th, eta):
-    """Write a map (pf_kks/io.py:25-40)."""
-    np.savez_compressed(
-        path,
-        ttime=ttime,
-        time_out=hist["time"],
-        T_out=hist["T"],
-        X_al_mean_out=hist["X_al_mean"],
-        X_th_mean_out=hist["X_th_mean"],
-        eta_mean_out=hist["eta_mean"],
-        surf_out=hist["surf"],
-        X=X,
-        X_al=X_al,
-        X_th=X_th,
-        eta=eta,
-    )
+    """Write one map: ``ttime``, the histories named in HISTORY_KEYS and the
+    four fields, compressed."""
+    arrays = {"ttime": ttime}
+    arrays.update({key: hist[name] for key, name in HISTORY_KEYS})
+    arrays.update(zip(FIELD_KEYS, (X, X_al, X_th, eta)))
+    np.savez_compressed(path, **arrays)
 
 
 def parse_map_filename(path):
-    m = MAP_PATTERN.search(os.path.basename(path))
-    if m is None:
+    """(ttime, T_start, T_max) of a map file name; ValueError for any other
+    name."""
+    name = os.path.basename(path)
+    try:
+        if not (name.startswith("map") and name.endswith("K.npz")):
+            raise ValueError
+        ttime, rest = name[3:-5].split("s_", 1)
+        T_start, T_max = rest.rsplit("_", 1)
+        values = tuple(float(v) for v in (ttime, T_start, T_max))
+    except ValueError:
+        raise ValueError(f"not a map file name: {path}") from None
+    if any(v < 0 for v in values):
         raise ValueError(f"not a map file name: {path}")
-    return float(m["ttime"]), float(m["T_start"]), float(m["T_max"])
-
-
-def list_maps(directory):
-    files = [f for f in glob.glob(os.path.join(directory, "map*.npz")) if MAP_PATTERN.search(os.path.basename(f))]
-    return sorted(files, key=lambda f: (parse_map_filename(f)[2], parse_map_filename(f)[0]))
-
-
-def load_map(path, fields=True):
-    with np.load(path) as d:
-        keys = d.files if fields else [k for k in d.files if k not in ("X", "X_al", "X_th", "eta")]
-        return {k: d[k] for k in keys}
+    return values

@@ -1,7 +1,7 @@
 """Generate the golden fixtures of tests/golden/ from the reference itself.
 
-Run in a checkout that has the reference package (``pf_kks``) at REF (default
-/root/reference; it is read, never written):
+Run in a checkout that has the reference package (``pf_kks``) at REF (given as the
+argument or in $PF_KKS_REFERENCE; it is read, never written):
 
     NUMBA_CACHE_DIR=/tmp/numba python tests/golden/make_fixtures.py [REF]
 
@@ -159,4 +159,7 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    _ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PF_KKS_REFERENCE")
+    if not _ref:
+        sys.exit(f"usage: python {os.path.basename(__file__)} REFERENCE_CHECKOUT (or set PF_KKS_REFERENCE)")
+    main(_ref)

@@ -3,7 +3,7 @@ and nucleation functions that the device versions are checked against.
 
     NUMBA_CACHE_DIR=/tmp/numba python tests/golden/make_init_fixtures.py [REF]
 
-REF (default /root/reference) is read, never written. Contents:
+REF (the argument, or $PF_KKS_REFERENCE) is read, never written. Contents:
 
 * ``place_*``: ``pf_kks.microstructure.place_precipitates`` (numba,
   pf_kks/microstructure.py:7-52) on a 96 x 80 x 1 grid with circles that cross
@@ -85,4 +85,7 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    _ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PF_KKS_REFERENCE")
+    if not _ref:
+        sys.exit(f"usage: python {os.path.basename(__file__)} REFERENCE_CHECKOUT (or set PF_KKS_REFERENCE)")
+    main(_ref)

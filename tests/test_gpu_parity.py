@@ -220,14 +220,150 @@ def test_fused_fft_path_matches_oracle(tmp_path, shape):
 
 
 def test_fused_fft_1420_short_run(tmp_path):
-    """The bench grid (1420 = 4 * 5 * 71): three steps of the fused mixed step
-    against the FP64 GPU step."""
+    """The bench grid (1420 = 4 * 5 * 71): three steps of the FP64 step and of
+    the fused mixed step against the oracle."""
+    from oracle import kks_oracle
     from pf_kks_gpu import workloads
 
     cfg, spec = workloads.ramp1420(n_steps=3)
     state = workloads.initial_state(cfg, spec)
     fused = _run_gpu(cfg, state, tmp_path / "fused", precision="mixed")
+    assert fused.__class__.__name__ == "SimulationResult", fused
     f64 = _run_gpu(cfg, state, tmp_path / "fp64", precision="fp64")
+    ref = kks_oracle.run(cfg, *copy_state(state), cfg.material_tables, out_dir=str(tmp_path / "cpu"))
+    for name in FIELDS:
+        assert rel_l2(getattr(f64, name), getattr(ref, name)) <= FIELD_TOL, name
+    _assert_hist_close(f64.history, lambda n: ref.history[n])
     for name in ("eta", "X"):
-        assert rel_l2(getattr(fused, name), getattr(f64, name)) <= 1e-6, name
-    np.testing.assert_allclose(fused.history["energy_s"], f64.history["energy_s"], rtol=1e-6)
+        assert rel_l2(getattr(fused, name), getattr(ref, name)) <= 1e-6, name
+    np.testing.assert_allclose(fused.history["energy_s"], ref.history["energy_s"], rtol=1e-6)
+
+
+# ---------------------------------------------------------------------------
+# Parity at the grids the benchmark configurations are quoted on.
+
+
+def _archived_735(n_steps):
+    """The reproducible run of the reference (configs/reproducible_run.toml:
+    the SimulationConfig defaults, 735^2) from the archived precipitates."""
+    from pf_kks_gpu.config import SimulationConfig
+    from pf_kks_gpu.materials import DEFAULT_PRECIPITATES, DEFAULT_TABLES
+    from pf_kks_gpu.microstructure import load_precipitates, place_precipitates
+
+    cfg = SimulationConfig(n_steps=n_steps, material_tables=DEFAULT_TABLES)
+    ox, oy, oz, r = load_precipitates(DEFAULT_PRECIPITATES)
+    state = place_precipitates(cfg.nx, cfg.ny, cfg.nz, cfg.dx, cfg.dy, cfg.dz, cfg.x_matrix, cfg.x_precipitate, r,
+                               ox, oy, oz)
+    return cfg, state
+
+
+def test_fp64_first_step_matches_archived_map(tmp_path):
+    """The FP64 GPU step against the map the reference's 2022 run archived
+    after its first step (reference tests/test_archived_run.py:35-46): the map
+    name and keys, every field at the sampled points within atol 1e-14 (the
+    reference's own bar), the field sums, the history keys and the first
+    dtime.txt line."""
+    a = np.load(os.path.join(GOLDEN, "archived_735.npz"))
+    cfg, state = _archived_735(1)
+    res = _run_gpu(cfg, state, tmp_path)
+    assert os.listdir(tmp_path / "saved_maps") == ["map0.07s_400_400.00K.npz"]
+    with np.load(tmp_path / "saved_maps" / "map0.07s_400_400.00K.npz") as new:
+        assert list(new.files) == list(a["map_files"])
+        for name in FIELDS:
+            flat = new[name].ravel()
+            np.testing.assert_allclose(flat[a[f"map_{name}_idx"]], a[f"map_{name}_val"], rtol=0, atol=1e-14,
+                                       err_msg=name)
+            assert flat.sum() == pytest.approx(float(a[f"map_{name}_sum"]), rel=1e-13)
+            assert (flat * flat).sum() == pytest.approx(float(a[f"map_{name}_sumsq"]), rel=1e-13)
+        for key in new.files:
+            if key not in FIELDS:
+                assert new[key].dtype == a[f"mapkey_{key}"].dtype, key
+                np.testing.assert_allclose(new[key], a[f"mapkey_{key}"], rtol=0, atol=1e-14, err_msg=key)
+    line = (tmp_path / "dtime.txt").read_text().splitlines()[1].rstrip()
+    assert line == str(a["dtime_line1"])
+    assert res.ttime == pytest.approx(float(a["mapkey_ttime"]), rel=1e-14)
+
+
+def test_fp64_twenty_steps_match_archived_histories(tmp_path):
+    """20 FP64 GPU steps against the archived histories of the 2022 run
+    (reference tests/test_archived_run.py:49-61, rtol 1e-12)."""
+    a = np.load(os.path.join(GOLDEN, "archived_735.npz"))
+    cfg, state = _archived_735(20)
+    res = _run_gpu(cfg, state, tmp_path)
+    for ref_key, new_key in [("time_out", "time"), ("T_out", "T"), ("surf_out", "surf"),
+                             ("X_al_mean_out", "X_al_mean"), ("X_th_mean_out", "X_th_mean"),
+                             ("eta_mean_out", "eta_mean")]:
+        np.testing.assert_allclose(np.asarray(res.history[new_key], float), a[f"hist20_{ref_key}"], rtol=1e-12,
+                                   atol=0, err_msg=ref_key)
+
+
+def _assert_config2_scalars(res, ref, rtol):
+    """The history scalars the 735^2 precision check reports: matrix Si mean,
+    precipitate fraction (mean eta) and interface measure, every step."""
+    for name in ("X_al_mean", "eta_mean", "surf"):
+        np.testing.assert_allclose(np.asarray(res.history[name], float), np.asarray(ref.history[name], float),
+                                   rtol=rtol, atol=1e-15, err_msg=name)
+
+
+def test_iso735_fp64_and_mixed_against_oracle(tmp_path):
+    """The 735^2 precision check (735 = 3 * 5 * 7^2: the fused passes with
+    radices 3, 5, 7), isothermal 500 K, fixed dt, 30 steps: the FP64 step
+    within 1e-10 relative L2 of the oracle on every field and 1e-9 on every
+    history; the mixed step within 1e-6 on eta and X and on the matrix Si
+    mean, precipitate fraction and interface measure."""
+    from oracle import kks_oracle
+    from pf_kks_gpu import solver, workloads
+
+    cfg, spec = workloads.iso735(n_steps=30)
+    state = workloads.initial_state(cfg, spec)
+    ref = kks_oracle.run(cfg, *copy_state(state), cfg.material_tables, out_dir=str(tmp_path / "cpu"))
+    f64 = _run_gpu(cfg, state, tmp_path / "fp64", precision="fp64")
+    for name in FIELDS:
+        assert rel_l2(getattr(f64, name), getattr(ref, name)) <= FIELD_TOL, name
+    _assert_hist_close(f64.history, lambda n: ref.history[n])
+    cell = solver.Cell(cfg, solver.MaterialTables.from_npz(cfg.material_tables, cfg.c_gamma, cfg.c_eps0),
+                       precision="mixed")
+    assert cell.pipeline()[0], "735^2 should run the fused passes"
+    cell.close()
+    mixed = _run_gpu(cfg, state, tmp_path / "mixed", precision="mixed")
+    for name in ("eta", "X"):
+        assert rel_l2(getattr(mixed, name), getattr(ref, name)) <= 1e-6, name
+    _assert_config2_scalars(mixed, ref, rtol=1e-6)
+    assert abs(mixed.X.mean() - state[1].mean()) <= 1e-9
+
+
+def _decisions(log_text):
+    """(step, kind) of every adaptive decision in a log.txt."""
+    out = []
+    for line in log_text.splitlines():
+        if ": RE>resmax" in line:
+            out.append((int(line.split()[1].rstrip(":")), "rejected"))
+        elif "(resmin <RE <resmax)" in line:
+            out.append((int(line.split()[1].rstrip(",")), "accepted"))
+        elif ":RE <resmin" in line:
+            out.append((int(line.split()[-1]), "enlarged"))
+    return out
+
+
+@pytest.mark.parametrize("case", ["accepted30", "enlarged40"])
+def test_mixed_decisions_match_reference(tmp_path, relaxed_state, small_golden, small_golden_logs, case):
+    """The mixed step on the reference's accepted and enlarged set-ups
+    (reference tests/test_solver_equivalence.py:89-107): the same adaptive
+    decisions at the same steps as pf_kks, the same good_step, and fields
+    within the mixed path's 1e-6 of the reference's."""
+    from pf_kks_gpu import solver
+
+    if case == "accepted30":
+        cfg = small_config(n_steps=30, x_equilibrium=0.2)
+    else:
+        cfg = small_config(n_steps=40, x_equilibrium=0.2, dtime_s=60, dtime_max=150, residual_min=7.6e-4)
+    res = _run_gpu(cfg, relaxed_state, tmp_path, precision="mixed")
+    assert isinstance(res, solver.SimulationResult), res
+    ref_decisions = _decisions(small_golden_logs[case]["log.txt"])
+    assert ref_decisions, case
+    assert _decisions((tmp_path / "log.txt").read_text()) == ref_decisions
+    g = small_golden
+    assert res.good_step == int(g[f"{case}_good_step"])
+    np.testing.assert_array_equal(res.history["dtime_s"], g[f"{case}_h_dtime_s"])
+    for name in ("eta", "X"):
+        assert rel_l2(getattr(res, name), g[f"{case}_{name}"]) <= 1e-6, name
