@@ -272,6 +272,39 @@ def ensemble_leg(precision, device, steps, warmup, cpu=True):
     return out
 
 
+def sharded_ensemble_leg(precision, device, steps, warmup, rank, world, barrier, max_over_ranks):
+    """The 48-cell ensemble sharded over the job's ranks (one GPU each): every
+    rank builds and advances only its cost-balanced shard
+    (pf_kks_gpu.ensemble.partition) as one tuned Ensemble; no collective in the
+    steps. Whole-job cell-steps/s = all cells' points x steps / the slowest
+    rank's wall time."""
+    import torch
+
+    from pf_kks_gpu import workloads
+    from pf_kks_gpu.ensemble import Ensemble, cell_cost, partition
+
+    specs = workloads.ensemble(48, 100000, precision)
+    shard = partition([cell_cost(c.nx, c.ny, steps) for c, _ in specs], world)[rank]
+    members = [(specs[i][0], workloads.initial_state(*specs[i])) for i in shard]
+    ens = Ensemble(members, precision=precision, device=device, tune=True) if members else None
+    try:
+        if ens is not None:
+            ens.run(warmup)
+        barrier()
+        t0 = time.perf_counter()
+        if ens is not None:
+            ens.run(steps)
+        torch.cuda.synchronize()
+        dt = max_over_ranks(time.perf_counter() - t0)
+    finally:
+        if ens is not None:
+            ens.close()
+    points = sum(c.nx * c.ny for c, _ in specs)
+    return {"cells": len(specs), "points": int(points), "steps": steps, "ranks": world,
+            "cells_on_rank0": len(shard) if rank == 0 else None, "cell_steps_per_s": points * steps / dt,
+            "timing": "host wall clock per rank around Ensemble.run, max over ranks"}
+
+
 def profile_ensemble(args):
     """Profiling run: the 48-cell ensemble as one batch (column tile 4, one
     group), ``--warmup`` then ``--steps`` batch attempts; device time from the
@@ -330,51 +363,46 @@ def init_leg(precision, device):
     return out
 
 
-def adjoint_leg(device, steps=300, checkpoint_every=10):
-    """adjoint256: a fixed-dt FP64 run of 300 steps at 256^2 through the
-    coefficient chain and kks_adj_forward, then the gradient of a
-    finite-difference simulated DSC with respect to (c_D, c_Meta) through the
-    hand-written adjoint (checkpoint every 10 steps, segments recomputed)."""
+def adjoint_leg(device, steps=300, checkpoint_every=50):
+    """adjoint256: the gradient workload. 300 fixed-dt FP64 steps at 256^2
+    through the coefficient chain and kks_adj_forward, the simulated DSC of the
+    run, the loss against the DSC of the target run (Si mobility x 1.2,
+    vacancy annealing rate x 0.8, interface energy x 1.1), and its gradient
+    with respect to the log of the three factors through the hand-written
+    adjoint (checkpoint every 50 steps, segments recomputed)."""
     import torch
 
     from pf_kks_gpu import adjoint as A
     from pf_kks_gpu import workloads
     from pf_kks_gpu.materials import MaterialTables
 
-    class Enthalpy:  # smooth stand-ins for the CALPHAD enthalpies (J/mol)
-        def hm_fcc(self, T, x):
-            return -2000.0 + 5.0 * T + 3.0e4 * x
-
-        def hm_dia(self, T):
-            return 1.0e4 + 2.0 * T
-
-        def dhm_fcc_dx(self, T, x):
-            return 3.0e4 + 0 * T + 0 * x
-
     cfg, spec = workloads.adjoint256(n_steps=steps)
     tables = MaterialTables.from_npz(cfg.material_tables, cfg.c_gamma, cfg.c_eps0)
     state = workloads.initial_state(cfg, spec)
     stepper = A.StepAdjoint.for_config(cfg, tables, device=device)
     s0 = A.initial_state_tensor(*state, device=device)
-    lcD = torch.zeros((), dtype=torch.float64, requires_grad=True)
-    lcM = torch.zeros((), dtype=torch.float64, requires_grad=True)
+    target = torch.tensor(np.log(workloads.ADJOINT_TARGET_FACTORS), dtype=torch.float64)
+    with torch.no_grad():
+        q_target = A.dsc_of_run(cfg, tables, s0, stepper, steps, target, checkpoint_every).total
+    theta = torch.zeros(3, dtype=torch.float64, requires_grad=True)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    coef, t, T = A.coefficients(cfg, tables, steps, lcD, lcM, return_times=True)
-    em, xm, fin = A.FixedDtRun.apply(coef, s0, stepper, checkpoint_every)
-    q = A.finite_difference_dsc(em, xm, t.to(em.device), T.to(em.device), Enthalpy(), 20 / 60)
-    loss = (q**2).sum()
+    q = A.dsc_of_run(cfg, tables, s0, stepper, steps, theta, checkpoint_every).total
+    loss = ((q - q_target) ** 2).sum()
     torch.cuda.synchronize()
     t1 = time.perf_counter()
     loss.backward()
     torch.cuda.synchronize()
     t2 = time.perf_counter()
     stepper.close()
-    return {"workload": "adjoint256: 256^2, 8 cells, 500->520 K, fixed dt, FP64", "steps": steps,
-            "checkpoint_every": checkpoint_every, "forward_s": t1 - t0, "backward_s": t2 - t1,
+    g = theta.grad.tolist()
+    return {"workload": "adjoint256: 256^2, 8 cells, 500->520 K, 300 fixed-dt steps, FP64; loss = squared error of "
+                        "the simulated DSC against the run with Si mobility x1.2, annealing rate x0.8, "
+                        "interface energy x1.1", "steps": steps,
+            "checkpoint_every": checkpoint_every, "loss": float(loss), "forward_s": t1 - t0, "backward_s": t2 - t1,
             "forward_steps_per_s": steps / (t1 - t0), "gradient_steps_per_s": steps / (t2 - t1),
-            "grad_log_c_D": float(lcD.grad), "grad_log_c_Meta": float(lcM.grad),
-            "timing": "host wall clock, coefficient chain and histories included"}
+            "grad_log_c_D": g[0], "grad_log_anneal_rate": g[1], "grad_log_c_gamma": g[2],
+            "timing": "host wall clock, coefficient chain, histories and DSC included"}
 
 
 def main():
@@ -530,6 +558,11 @@ def main():
         with open(tpath) as f:
             traffic = json.load(f).get("dram_bytes_per_attempt")
 
+    # every rank takes part in the sharded ensemble leg (its barrier and max over ranks)
+    sharded = None
+    if world > 1 and not args.no_ensemble and args.precision != "fp64":
+        sharded = sharded_ensemble_leg(args.precision, local_rank, 20, 3, rank, world, barrier, max_over_ranks)
+
     if rank != 0:
         if dist is not None:
             dist.destroy_process_group()
@@ -581,8 +614,11 @@ def main():
         "gpu_launches": int(kernels_per_attempt * attempts),
     }
     if not args.no_ensemble and args.precision != "fp64":
-        line["ensemble"] = ensemble_leg(args.precision, local_rank, steps=20, warmup=3,
-                                        cpu=not args.no_cpu_baseline and world == 1)
+        if world == 1:
+            line["ensemble"] = ensemble_leg(args.precision, local_rank, steps=20, warmup=3,
+                                            cpu=not args.no_cpu_baseline)
+        else:
+            line["ensemble_sharded"] = sharded
     if not args.no_init and world == 1 and args.precision != "fp64":
         line["init"] = init_leg(args.precision, local_rank)
     if not args.no_adjoint and world == 1:

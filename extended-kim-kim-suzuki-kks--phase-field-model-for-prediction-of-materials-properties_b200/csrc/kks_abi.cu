@@ -305,6 +305,7 @@ static int setup_fused(kks_handle* h, const std::vector<double>& kx) {
   CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device));
   if (kks_fft_smem_bytes(c.nx, c.ny, KKS_FFT_COLS) > (size_t)optin) return KKS_OK;
   fc.cols = KKS_FFT_COLS;
+  fc.wait_polls = KKS_FFT_WAIT_POLLS;
   std::vector<float> kx_slot(c.nx);
   for (int k = 0; k < c.nx; ++k) kx_slot[tx.slot[k]] = (float)kx[k];
   // device tables and buffers in one allocation
@@ -1146,6 +1147,35 @@ int kks_download(kks_handle* h, double* eta, double* X, double* X_al, double* X_
   if (X && (rc = get_field(h, X, h->f.X[p], true)) != KKS_OK) return rc;
   if (X_al && (rc = get_field(h, X_al, h->f.X_al[p], d)) != KKS_OK) return rc;
   if (X_th && (rc = get_field(h, X_th, h->f.X_th[p], d)) != KKS_OK) return rc;
+  return KKS_OK;
+}
+
+int kks_set_wait_polls(kks_handle* h, int32_t polls) {
+  if (!h) return set_error(KKS_ERR_ARG, "null handle");
+  if (!h->fused_ok || !h->d_fc) return set_error(KKS_ERR_STATE, "the cell has no fused passes (nothing waits)");
+  const int v = polls < 0 ? KKS_FFT_WAIT_POLLS : polls;
+  CK(cudaSetDevice(h->device));
+  CK(cudaStreamSynchronize(h->stream));
+  CK(cudaMemcpy(&h->d_fc->wait_polls, &v, sizeof(int), cudaMemcpyHostToDevice));
+  return KKS_OK;
+}
+
+int kks_download_pair(kks_handle* h, double* eta_m, double* X_m, double* mu_m, double* G_m) {
+  if (!h) return set_error(KKS_ERR_ARG, "null handle");
+  if (!h->uploaded) return set_error(KKS_ERR_STATE, "kks_download_pair before kks_upload");
+  CK(cudaSetDevice(h->device));
+  const KksCtl* c = h->h_ctl;
+  const bool d = h->precision == KKS_PRECISION_FP64;
+  // after an accepted step the minus entry is the step's input state itself;
+  // after a rejection it is the saved copy of the rejected attempt
+  const void* e = c->minus_is_state ? h->f.eta[h->parity] : h->f.eta_m;
+  const void* x = c->minus_is_state ? h->f.X[h->parity] : h->f.X_m;
+  if (c->gm < 0 || c->gm > 2) return set_error(KKS_ERR_STATE, "residual pair not set");
+  int rc;
+  if (eta_m && (rc = get_field(h, eta_m, e, true)) != KKS_OK) return rc;
+  if (X_m && (rc = get_field(h, X_m, x, true)) != KKS_OK) return rc;
+  if (mu_m && (rc = get_field(h, mu_m, h->f.mu, d)) != KKS_OK) return rc;
+  if (G_m && (rc = get_field(h, G_m, h->f.g[c->gm], d)) != KKS_OK) return rc;
   return KKS_OK;
 }
 

@@ -355,7 +355,7 @@ __device__ __forceinline__ int fdiv(int x, int d, uint32_t m) {
 // pass stages the state rows its pointwise phase needs at kernel entry, so the
 // loads overlap the merge and the inverse FFT. Source, destination and size
 // are multiples of 16 bytes (the host enables this only for ny % 4 == 0).
-constexpr int kWaitLimit = 1 << 20;  // try_wait polls before a wait is declared lost
+constexpr int kWaitLimit = KKS_FFT_WAIT_POLLS;  // try_wait polls before a wait is declared lost
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -387,12 +387,13 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 }
 
 // Wait for the phase of bar with the given parity, with a bounded number of
-// polls. If it runs out the cell's status becomes KKS_STATUS_TIMEOUT (the host
-// stops the run and reports it) and the block waits once more, again bounded,
-// for its copies in flight.
-__device__ __forceinline__ void bulk_wait(uint64_t* bar, uint32_t parity, KksCtl* ctl) {
+// polls (`polls`, the cell's KksFftConst::wait_polls). If it runs out the
+// cell's status becomes KKS_STATUS_TIMEOUT (the host stops the run and reports
+// it) and the block waits once more, bounded by kWaitLimit, for its copies in
+// flight, so that no copy lands in shared memory after the block has moved on.
+__device__ __forceinline__ void bulk_wait(uint64_t* bar, uint32_t parity, KksCtl* ctl, int polls) {
   bool done = false;
-  for (int i = 0; i < kWaitLimit && !done; ++i) done = mbar_try_wait(bar, parity);
+  for (int i = 0; i < polls && !done; ++i) done = mbar_try_wait(bar, parity);
   if (!done) {
     atomicCAS(&ctl->status, KKS_STATUS_OK, KKS_STATUS_TIMEOUT);
     for (int i = 0; i < kWaitLimit && !done; ++i) done = mbar_try_wait(bar, parity);
@@ -627,7 +628,7 @@ __device__ __forceinline__ void rows_A_body(const KksConst* __restrict__ c, cons
       bulk_g2s((void*)s_eta, eta + i0, 16u * ny, &bar);
       bulk_g2s((void*)s_X, X + i0, 16u * ny, &bar);
     }
-    bulk_wait(&bar, 0, ctl);
+    bulk_wait(&bar, 0, ctl, fc->wait_polls);
   }
   const bool surface = par->surface;
   double acc[6] = {0, 0, 0, 0, 0, 0};
@@ -714,7 +715,7 @@ __device__ __forceinline__ void cols_AB_body(const KksConst* __restrict__ c, con
       bulk_g2s(sm, col, 8u * nv, &bar);
     }
     __syncthreads();
-    bulk_wait(&bar, 0, ctl);
+    bulk_wait(&bar, 0, ctl, fc->wait_polls);
   } else {
     for (int i = threadIdx.x; i < nv; i += NT) sm[i] = col[i];
     __syncthreads();
@@ -825,7 +826,7 @@ __device__ __forceinline__ void rows_BC_body(const KksConst* __restrict__ c, con
       stage_load(st, map_RB, ix0, 3, kb, nb, &bar);
     }
     __syncthreads();
-    bulk_wait(&bar, 0, ctl);
+    bulk_wait(&bar, 0, ctl, fc->wait_polls);
     for (int f = 0; f < 3; ++f) merge_stage<NT>(sm + f * ny, ay, st, f, 3, kb, nyh);
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -841,7 +842,7 @@ __device__ __forceinline__ void rows_BC_body(const KksConst* __restrict__ c, con
     __syncthreads();
   }
   fft_run<+1, PY>(3, ay);
-  if (bulk) bulk_wait(&bar, 1, ctl);
+  if (bulk) bulk_wait(&bar, 1, ctl, fc->wait_polls);
   const KksPar q = *par;
   float* gs_buf = q.gs == 0 ? g0 : (q.gs == 1 ? g1 : g2);
   const float A_a = (float)q.A_alp_s, va = (float)q.va, fa0 = (float)q.fa0;
@@ -935,7 +936,7 @@ __device__ __forceinline__ void cols_CD_eta_body(const KksConst* __restrict__ c,
       bulk_g2s(sm, col, 8u * nv, &bar);
     }
     __syncthreads();
-    bulk_wait(&bar, 0, ctl);
+    bulk_wait(&bar, 0, ctl, fc->wait_polls);
     if (threadIdx.x == 0) {
       mbar_expect_tx(&bar, 8u * nv);
       bulk_g2s(s_sa, SA + (size_t)ky0 * nx, 8u * nv, &bar);
@@ -945,7 +946,7 @@ __device__ __forceinline__ void cols_CD_eta_body(const KksConst* __restrict__ c,
     __syncthreads();
   }
   fft_run<-1, PX>(ncol, ax);
-  if (bulk) bulk_wait(&bar, 1, ctl);
+  if (bulk) bulk_wait(&bar, 1, ctl, fc->wait_polls);
   const float inv_N = (float)c->inv_N;
   const float ac_mul = (float)par->ac_mul, ac_den = (float)par->ac_den;
   for (int cc = 0; cc < ncol; ++cc) {
@@ -1006,7 +1007,7 @@ __device__ __forceinline__ void cols_CD_X_body(const KksConst* __restrict__ c, c
       bulk_g2s(sm + nv, cy, 8u * nv, &bar);
     }
     __syncthreads();
-    bulk_wait(&bar, 0, ctl);
+    bulk_wait(&bar, 0, ctl, fc->wait_polls);
     if (threadIdx.x == 0) {
       mbar_expect_tx(&bar, 8u * nv);
       bulk_g2s(s_sa, SA + fs + (size_t)ky0 * nx, 8u * nv, &bar);
@@ -1019,7 +1020,7 @@ __device__ __forceinline__ void cols_CD_X_body(const KksConst* __restrict__ c, c
     __syncthreads();
   }
   fft_run<-1, PX>(2 * ncol, ax);
-  if (bulk) bulk_wait(&bar, 1, ctl);
+  if (bulk) bulk_wait(&bar, 1, ctl, fc->wait_polls);
   const float inv_N = (float)c->inv_N;
   const float ch_mul = (float)par->ch_mul;
   const float dtD = (float)(par->dt * par->D_s);
@@ -1086,7 +1087,7 @@ __device__ __forceinline__ void rows_D_body(const KksConst* __restrict__ c, cons
       stage_load(st, map_RD, ix0, 2, kb, nb, &bar);
     }
     __syncthreads();
-    bulk_wait(&bar, 0, ctl);
+    bulk_wait(&bar, 0, ctl, fc->wait_polls);
     merge_stage<NT>(sm, ay, st, 0, 2, kb, nyh);
     merge_stage<NT>(sm + ny, ay, st, 1, 2, kb, nyh);
     __syncthreads();
@@ -1103,7 +1104,7 @@ __device__ __forceinline__ void rows_D_body(const KksConst* __restrict__ c, cons
     __syncthreads();
   }
   fft_run<+1, PY>(2, ay);
-  if (bulk) bulk_wait(&bar, 1, ctl);
+  if (bulk) bulk_wait(&bar, 1, ctl, fc->wait_polls);
   const KksPar q = *par;
   float* gb_buf = q.gb == 0 ? g0 : (q.gb == 1 ? g1 : g2);
   const float* gm_buf = q.gm == 0 ? g0 : (q.gm == 1 ? g1 : g2);

@@ -36,7 +36,11 @@ struct KksFftConst {
   KksFftAxis ay;         // y axis (row passes)
   const float* kx_slot;  // k_x of the frequency held at each x slot after the DIF
   int cols;              // y-frequency columns per column-pass block (1..KKS_FFT_COLS_MAX)
+  int wait_polls;        // polls of the first wait for a block's bulk / tensor copies (KKS_FFT_WAIT_POLLS;
+                         // kks_set_wait_polls changes it for fault-path tests)
 };
+
+#define KKS_FFT_WAIT_POLLS (1 << 20)
 
 // Spectrum buffers are column-major: element (ix, ky) of field f at
 // f * nx * nyh + ky * nx + ix, so that a column pass reads and writes one

@@ -16,13 +16,18 @@
 //
 // Host code cannot use the array's name as a device address (it is a host
 // stand-in), so the first call on each device looks the address up with
-// cudaGetSymbolAddress while that device is current and caches it; make that
-// first call before any stream capture. All calls share the one array and it
+// cudaGetSymbolAddress while that device is current and caches it, together
+// with the device's current context; make that first call before any stream
+// capture. A call that finds another context current (after cudaDeviceReset,
+// or a primary context released and created again, the module is loaded anew
+// and the array may sit elsewhere) looks the address up again. All calls share the one array and it
 // keeps the last call's contents: every block overwrites its own row before
 // the final kernel reads it, so nothing has to start at zero, but calls that
 // overlap on the GPU (two streams, or two host threads) race on the array and
 // must be serialised by the caller.
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -41,10 +46,25 @@ constexpr int kKksNoallocSlots = 6;
 
 static __device__ __align__(256) double g_noalloc_scratch[kKksNoallocBlocks * kKksNoallocSlots];
 
-// Per-device address of the scratch array, filled on the first call.
+// Per-device address of the scratch array and the context it belongs to,
+// filled on the first call on the device (and again after a context change).
 constexpr int kMaxDevices = 64;
 double* g_scratch_addr[kMaxDevices] = {nullptr};
+CUcontext g_scratch_ctx[kMaxDevices] = {nullptr};
 std::mutex g_scratch_mu;
+
+// cuCtxGetCurrent through the runtime's driver entry point (no link to libcuda).
+PFN_cuCtxGetCurrent_v4000 ctx_getter() {
+  static PFN_cuCtxGetCurrent_v4000 fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (PFN_cuCtxGetCurrent_v4000)p;
+  }
+  return fn;
+}
 
 __device__ __forceinline__ bool in_iface(double e) { return e >= 0.1 && e <= 0.9; }
 
@@ -103,13 +123,22 @@ extern "C" int kks_state_sums_noalloc(const double* eta, const double* X, int32_
   double* scratch;
   {
     std::lock_guard<std::mutex> lock(g_scratch_mu);
-    if (!g_scratch_addr[dev]) {
+    PFN_cuCtxGetCurrent_v4000 get_ctx = ctx_getter();
+    CUcontext ctx = nullptr;
+    if (!get_ctx || get_ctx(&ctx) != CUDA_SUCCESS)
+      return fail(KKS_ERR_CUDA, "kks_state_sums_noalloc: cannot read the current CUDA context");
+    if (!ctx || !g_scratch_addr[dev] || g_scratch_ctx[dev] != ctx) {
+      // set-up for this device and context (the lookup also makes the
+      // device's primary context current when no context was yet)
       void* p = nullptr;
       cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
       if (e != cudaSuccess || !p)
         return fail(KKS_ERR_CUDA, std::string("kks_state_sums_noalloc: cudaGetSymbolAddress: ") +
                                       cudaGetErrorString(e));
+      if (!ctx && (get_ctx(&ctx) != CUDA_SUCCESS || !ctx))
+        return fail(KKS_ERR_CUDA, "kks_state_sums_noalloc: no current CUDA context");
       g_scratch_addr[dev] = (double*)p;
+      g_scratch_ctx[dev] = ctx;
     }
     scratch = g_scratch_addr[dev];
   }

@@ -54,7 +54,8 @@ EXPORTS = (
     "kks_adj_create", "kks_adj_forward", "kks_adj_backward", "kks_adj_destroy",
     "kks_voronoi_edges", "kks_generate_fields", "kks_place_precipitates", "kks_add_nuclei", "kks_count_below",
     "kks_insert_nuclei", "kks_batch_create", "kks_batch_run", "kks_batch_timing", "kks_batch_destroy",
-    "kks_get_launch_shape", "kks_set_launch_shape", "kks_autotune",
+    "kks_get_launch_shape", "kks_set_launch_shape", "kks_autotune", "kks_download_pair",
+    "kks_set_wait_polls",
 )
 
 
@@ -146,6 +147,9 @@ def load(path=LIB_PATH):
                               P(ctypes.c_int64)]
     lib.kks_get_state.argtypes = [vp, P(KksRunState)]
     lib.kks_download.argtypes = [vp, dp, dp, dp, dp]
+    lib.kks_download_pair.argtypes = [vp, dp, dp, dp, dp]
+    lib.kks_set_wait_polls.argtypes = [vp, ctypes.c_int32]
+    lib.kks_set_wait_polls.restype = ctypes.c_int
     lib.kks_elastic_fields.argtypes = [vp, dp, dp]
     lib.kks_checkpoint.argtypes = [vp, vp, ctypes.c_size_t, P(ctypes.c_size_t)]
     lib.kks_restore.argtypes = [vp, vp, ctypes.c_size_t]
@@ -186,7 +190,7 @@ def load(path=LIB_PATH):
         getattr(lib, name).restype = ctypes.c_int
     lib.kks_last_error.restype = ctypes.c_char_p
     lib.kks_version.restype = ctypes.c_char_p
-    for name in ("kks_create", "kks_upload", "kks_run", "kks_drain", "kks_get_state", "kks_download",
+    for name in ("kks_create", "kks_upload", "kks_run", "kks_drain", "kks_get_state", "kks_download", "kks_download_pair",
                  "kks_elastic_fields", "kks_checkpoint", "kks_restore", "kks_timing", "kks_pipeline", "kks_destroy"):
         getattr(lib, name).restype = ctypes.c_int
     _lib = lib

@@ -11,20 +11,30 @@ parameters, not on the fields. The gradient is therefore split in two:
   (schedule T(t), vacancy relaxation, Si diffusivity, interface mobility,
   Allen-Cahn coefficient, normalisation; ``pf_kks/kinetics.py:9-107``,
   ``pf_kks/solver.py:179-240``) in float64 torch, so that the 15 per-step
-  coefficients are differentiable functions of the calibration factors
-  ``c_D`` and ``c_Meta`` (as log-scale offsets).
+  coefficients are differentiable functions of log-scale offsets of four
+  parameters: the Si mobility prefactor ``c_D`` (``D0``), the interface
+  mobility ``c_Meta``, the interface energy ``c_gamma`` (the gamma table,
+  ``pf_kks/materials.py:50-51``: it enters kappa^2, w and L) and the vacancy
+  annealing rate (``Deff / Lv^2``, ``pf_kks/kinetics.py:52-56``: the offset
+  divides ``vacancy_sink_distance^2``).
 * :class:`FixedDtRun` runs the field steps on the GPU (``kks_adj_forward``)
   and, in its backward pass, the hand-written adjoint of the step
   (``kks_adj_backward``, ``csrc/kks_adjoint.cu``), checkpointing the state
   every ``checkpoint_every`` steps and recomputing the steps in between. It
   returns the per-step histories ``eta_mean`` and ``X_al_mean`` of the
   reference (``pf_kks/solver.py:380-390``: mean of eta, mean of X over
-  eta < 0.05, both of the step's input state) and the final state.
+  eta < 0.05, both of the step's input state), the interface measure ``surf``
+  of each step's input state (a cell count: no gradient) and the final state.
 
-    coef = coefficients(cfg, tables, n, log_c_D, log_c_Meta)    # needs_grad
-    eta_mean, X_al_mean, final = FixedDtRun.apply(coef, state0, stepper, 10)
-    loss = my_dsc_loss(eta_mean, X_al_mean)
-    loss.backward()                                             # -> log_c_D.grad, log_c_Meta.grad
+:func:`dsc_of_run` chains both with the simulated DSC of :mod:`pf_kks_gpu.dsc`.
+The window is fixed in steps, as the reference's API counts it: a change of
+``c_D`` changes D(t = 0) and with it the physical time of every step
+(``dx^2 / D_0 * dtime_s``, ``pf_kks/solver.py:188-190, 368-369``), so the
+times and temperatures of the steps are differentiable outputs too.
+
+    theta = torch.zeros(3, dtype=torch.float64, requires_grad=True)  # log c_D, log rate, log c_gamma
+    q = dsc_of_run(cfg, tables, state0, stepper, n_steps, theta, checkpoint_every=50).total
+    loss = ((q - q_target) ** 2).sum(); loss.backward()               # -> theta.grad
 """
 
 import ctypes
@@ -63,14 +73,17 @@ def _interp(x, xp, fp):
     return slope * (x - xp[i]) + fp[i]
 
 
-def coefficients(cfg, tables, n_steps, log_c_D=None, log_c_Meta=None, return_times=False):
+def coefficients(cfg, tables, n_steps, log_c_D=None, log_c_Meta=None, return_times=False, log_c_gamma=None,
+                 log_anneal=None):
     """Per-step coefficients of a fixed-dt run, shape (n_steps, 15), float64,
     in the order of ``KKS_COEF_*`` (``include/kks.h``).
 
-    ``log_c_D`` / ``log_c_Meta`` (0-d float64 tensors, default 0) multiply
-    ``cfg.c_D`` / ``cfg.c_Meta`` by their exponential; gradients flow to them.
-    With ``return_times`` the result is (coef, time, T): the time [s] and
-    temperature [K] of each step's input state (the ``time`` / ``T``
+    The log offsets (0-d float64 tensors, default 0; gradients flow to them)
+    multiply ``cfg.c_D`` (``log_c_D``), ``cfg.c_Meta`` (``log_c_Meta``), the
+    interface energy of the tables (``log_c_gamma``, on top of ``cfg.c_gamma``)
+    and the vacancy annealing rate Deff / Lv^2 (``log_anneal``) by their
+    exponential. With ``return_times`` the result is (coef, time, T): the time
+    [s] and temperature [K] of each step's input state (the ``time`` / ``T``
     histories), which also depend on the parameters through D(t = 0).
     """
     torch = _torch()
@@ -78,11 +91,13 @@ def coefficients(cfg, tables, n_steps, log_c_D=None, log_c_Meta=None, return_tim
     zero = torch.zeros((), dtype=f64)
     lcD = zero if log_c_D is None else log_c_D
     lcM = zero if log_c_Meta is None else log_c_Meta
+    lcG = zero if log_c_gamma is None else log_c_gamma
+    lAn = zero if log_anneal is None else log_anneal
     D0 = float(tables.D0 if cfg.D0 is None else cfg.D0) * cfg.c_D * torch.exp(lcD)
     QD = float(tables.QD if cfg.QD is None else cfg.QD)
     Meta0 = cfg.Meta0 * cfg.c_Meta * torch.exp(lcM)
     QMeta = float(cfg.QMeta)
-    Lv2 = cfg.vacancy_sink_distance**2
+    Lv2 = cfg.vacancy_sink_distance**2 / torch.exp(lAn)
     lambd = cfg.half_width_cells * cfg.dx
     dx = cfg.dx
     cap = cfg.diffusion_enhancement_cap
@@ -121,7 +136,7 @@ def coefficients(cfg, tables, n_steps, log_c_D=None, log_c_Meta=None, return_tim
         dtime = (dx**2 / D_0) * dtime_s_ini
         Xv = Xv + (1 - torch.exp(-dtime * (Deff / Lv2))) * (Xve - Xv)
         at = {k: _interp(T, tT, v) for k, v in tab.items()}
-        sigma, Omega0 = at["gamma"], at["Vm"]
+        sigma, Omega0 = at["gamma"] * torch.exp(lcG), at["Vm"]
         kappa2 = 2 * lambd * sigma * 3 / cfg.alpha
         w = (sigma * 3 * cfg.alpha) / lambd
         kappa = torch.sqrt(kappa2)
@@ -145,9 +160,10 @@ class StepAdjoint:
     Tensors are float64 CUDA tensors of shape (4, nx, ny) (eta, X, X_al,
     X_th); coefficient rows are 15 float64 values."""
 
-    def __init__(self, nx, ny, C11_0, C12_0, C44_0, device=0):
+    def __init__(self, nx, ny, C11_0, C12_0, C44_0, device=0, surf_scale=1.0):
         self.lib = L.load()
         self.nx, self.ny, self.device = int(nx), int(ny), int(device)
+        self.surf_scale = float(surf_scale)  # dx^2 / (2 lambda): interface cells -> interface measure
         h = ctypes.c_void_p()
         L.check(self.lib.kks_adj_create(self.nx, self.ny, float(C11_0), float(C12_0), float(C44_0), self.device,
                                         ctypes.byref(h)), "kks_adj_create")
@@ -157,7 +173,8 @@ class StepAdjoint:
     def for_config(cls, cfg, tables, device=0):
         """Stiffness frozen at T(t = 0) (pf_kks/solver.py:152-154)."""
         T0 = float(np.interp(0.0, np.asarray(cfg.schedule_time, float), np.asarray(cfg.schedule_temperature, float)))
-        return cls(cfg.nx, cfg.ny, tables.at(T0, "C11"), tables.at(T0, "C12"), tables.at(T0, "C44"), device)
+        return cls(cfg.nx, cfg.ny, tables.at(T0, "C11"), tables.at(T0, "C12"), tables.at(T0, "C44"), device,
+                   surf_scale=cfg.dx**2 / (2 * cfg.lambd))
 
     def _check(self, *tensors):
         torch = _torch()
@@ -216,6 +233,13 @@ def _histories(state):
     return eta.mean(), xal, mask, cnt
 
 
+def _interface_cells(eta):
+    """Cells (nx-1)(ny-1) whose four corners lie in 0.1 <= eta <= 0.9
+    (pf_kks/microstructure.py:117-128)."""
+    s = (eta >= 0.1) & (eta <= 0.9)
+    return (s[:-1, :-1] & s[1:, :-1] & s[1:, 1:] & s[:-1, 1:]).sum()
+
+
 def _make_function():
     torch = _torch()
 
@@ -224,8 +248,9 @@ def _make_function():
 
         forward(coef (n, 15) float64, state0 (4, nx, ny) float64 CUDA,
         stepper: StepAdjoint, checkpoint_every: int) returns eta_mean (n),
-        X_al_mean (n) (histories of the input state of each step, on the
-        state's device) and the final state (4, nx, ny)."""
+        X_al_mean (n), surf (n) (histories of the input state of each step,
+        on the state's device; surf is the interface measure, a cell count
+        with no gradient) and the final state (4, nx, ny)."""
 
         @staticmethod
         def forward(ctx, coef, state0, stepper, checkpoint_every=10):
@@ -236,10 +261,12 @@ def _make_function():
             ckpt = {0: s.clone()}
             eta_mean = torch.empty(n, dtype=torch.float64, device=s.device)
             xal_mean = torch.empty(n, dtype=torch.float64, device=s.device)
+            surf = torch.empty(n, dtype=torch.float64, device=s.device)
             for i in range(n):
                 em, xm, _, _ = _histories(s)
                 eta_mean[i] = em
                 xal_mean[i] = xm
+                surf[i] = _interface_cells(s[0]) * stepper.surf_scale
                 nxt = torch.empty_like(s)
                 stepper.forward(s, c[i], nxt)
                 s = nxt
@@ -251,10 +278,11 @@ def _make_function():
             ctx.coef_np = c
             ctx.coef_shape = coef.shape
             ctx.coef_dtype = coef.dtype
-            return eta_mean, xal_mean, s
+            ctx.mark_non_differentiable(surf)
+            return eta_mean, xal_mean, surf, s
 
         @staticmethod
-        def backward(ctx, g_eta, g_xal, g_final):
+        def backward(ctx, g_eta, g_xal, g_surf, g_final):
             stepper, K, c = ctx.stepper, ctx.K, ctx.coef_np
             n = c.shape[0]
             s0 = ctx.ckpt[0]
@@ -300,35 +328,24 @@ def __getattr__(name):
     raise AttributeError(name)
 
 
-M_AL, M_SI = 26.98154, 28.0855  # molar masses [g/mol] (pf_kks/postprocess/dsc.py:24-25)
+def dsc_of_run(cfg, tables, state0, stepper, n_steps, theta, checkpoint_every=50, params=None,
+               return_run=False):
+    """Simulated DSC (:func:`pf_kks_gpu.dsc.simulated_dsc`) of a fixed-dt run
+    of ``n_steps`` from ``state0`` ((4, nx, ny) float64 CUDA tensor), as a
+    differentiable function of ``theta`` = (log c_D, log annealing rate,
+    log c_gamma) offsets (a float64 tensor of 3). ``params``: DSCParameters
+    (default: for_config(cfg)). With ``return_run`` also returns
+    (eta_mean, X_al_mean, surf, final, time, T)."""
+    from .dsc import DSCParameters, simulated_dsc
 
-
-def finite_difference_dsc(eta_mean, X_al_mean, time, T, enthalpy, heating_rate):
-    """Per-step simulated DSC signal from the histories, differentiable in them.
-
-    The precipitation / desaturation term of the reference's simulated DSC
-    (``pf_kks/postprocess/dsc.py:124-129``) with forward differences of the
-    histories in place of the derivatives of their smoothing splines, divided by
-    the heating rate [K/s] to give an apparent heat capacity [J/(g K)]:
-
-        f = eta_mean, x = X_al_mean (matrix Si), n = 0..len-2
-        q_n = (1 - f_n) dHfcc/dx(T_n, x_n) (x_{n+1} - x_n) / dt_n / M_AL
-              + (f_{n+1} - f_n) / dt_n (Hdia(T_n) / M_SI - Hfcc(T_n, x_n) / M_AL)
-
-    ``enthalpy`` supplies the molar enthalpies as torch functions
-    ``hm_fcc(T, x)``, ``hm_dia(T)`` and ``dhm_fcc_dx(T, x)`` [J/mol] (the
-    reference takes them from its CALPHAD description, ``pf_kks/thermo.py``).
-    ``time`` and ``T`` are the run's time [s] and temperature [K] histories.
-    """
-    torch = _torch()
-    f, x = eta_mean, X_al_mean
-    t = torch.as_tensor(time, dtype=f.dtype, device=f.device)
-    TT = torch.as_tensor(T, dtype=f.dtype, device=f.device)
-    dt = t[1:] - t[:-1]
-    Tn, xn, fn = TT[:-1], x[:-1], f[:-1]
-    q = ((1 - fn) * enthalpy.dhm_fcc_dx(Tn, xn) * (x[1:] - xn) / dt / M_AL
-         + (f[1:] - fn) / dt * (enthalpy.hm_dia(Tn) / M_SI - enthalpy.hm_fcc(Tn, xn) / M_AL))
-    return q / heating_rate
+    coef, t, T = coefficients(cfg, tables, n_steps, log_c_D=theta[0], log_anneal=theta[1], log_c_gamma=theta[2],
+                              return_times=True)
+    em, xm, surf, fin = __getattr__("FixedDtRun").apply(coef, state0, stepper, checkpoint_every)
+    p = DSCParameters.for_config(cfg) if params is None else params
+    q = simulated_dsc(em, xm, surf, t.to(em.device), T.to(em.device), p)
+    if return_run:
+        return q, (em, xm, surf, fin, t, T)
+    return q
 
 
 def initial_state_tensor(eta, X, X_al, X_th, device=0):

@@ -63,6 +63,56 @@ def gather_results(local, group=None):
     return merged
 
 
+def _rank_world():
+    try:
+        import torch.distributed as dist
+
+        if dist.is_available() and dist.is_initialized():
+            return dist.get_rank(), dist.get_world_size()
+    except Exception:
+        pass
+    return 0, 1
+
+
+def run_sharded(members, n_steps, precision="mixed", device=None, tune=False, fields=False, rank=None, world=None,
+                make_ensemble=None):
+    """Run an ensemble over the ranks of a job, one process per GPU.
+
+    ``members``: the whole ensemble, a list of (cfg, state) pairs on every
+    rank (``state`` may be a callable returning the four fields, so that a
+    rank builds only its own cells). The cells are partitioned by cost
+    (:func:`partition`, cost = N log N x steps); this rank advances its shard
+    as one :class:`Ensemble` on ``device`` (default: $LOCAL_RANK) by
+    ``n_steps`` (an int or one count per member); the per-cell results
+    (:meth:`Ensemble.results`) are then gathered on every rank with one
+    all-gather. There is no collective inside the steps. ``rank`` / ``world``
+    default to the initialised process group (else 0 / 1); ``make_ensemble``
+    replaces the Ensemble class (tests). Returns (results by member index,
+    this rank's shard, its status list)."""
+    import os
+
+    if rank is None or world is None:
+        rank, world = _rank_world()
+    if device is None:
+        device = int(os.environ.get("LOCAL_RANK", 0))
+    counts = [int(n_steps)] * len(members) if np.isscalar(n_steps) else [int(k) for k in n_steps]
+    costs = [cell_cost(cfg.nx, cfg.ny, k) for (cfg, _), k in zip(members, counts)]
+    shard = partition(costs, world)[rank]
+    local = {}
+    status = []
+    if shard:
+        cells = [(members[i][0], members[i][1]() if callable(members[i][1]) else members[i][1]) for i in shard]
+        ens = (make_ensemble or Ensemble)(cells, precision=precision, device=device, tune=tune)
+        try:
+            status = ens.run([counts[i] for i in shard])
+            for i, r in zip(shard, ens.results(fields=fields)):
+                r["rank"] = rank
+                local[i] = r
+        finally:
+            ens.close()
+    return gather_results(local), shard, status
+
+
 class Ensemble:
     """Cells of one shard resident on one GPU, advanced together.
 
@@ -134,6 +184,8 @@ class Ensemble:
                 L.check(rc, "kks_batch_create")
         if tuned_batch and batched is None:
             self._choose_mode(tune_attempts)
+        # history rows of the run proper (tuning attempts are rolled back)
+        self.rows = [[] for _ in self.cells]
 
     def _choose_mode(self, attempts):
         """Time the batch and the per-cell streams on the same attempts of the
@@ -264,9 +316,34 @@ class Ensemble:
         steps = (ctypes.c_int32 * n)(*counts)
         status = (ctypes.c_int32 * n)()
         L.check(getattr(L.load(), fn)(*head, steps, status), fn)
-        for c in self.cells:
-            c.drain()
+        self._collect()
         return list(status)
+
+    def _collect(self):
+        """Drain every cell's device records, keeping its history rows."""
+        if not hasattr(self, "rows"):
+            self.rows = [[] for _ in self.cells]
+        for k, c in enumerate(self.cells):
+            _, rows = c.drain()
+            if len(rows):
+                self.rows[k].append(rows)
+
+    def results(self, fields=False):
+        """Per-cell results, in member order: the loop state (status, step,
+        attempts, good_step or None, ttime), the history rows of all steps run
+        so far ((steps, 32) float64, columns KKS_H_* of include/kks.h) and, with
+        ``fields``, the final (eta, X, X_al, X_th)."""
+        out = []
+        for k, c in enumerate(self.cells):
+            s = c.state()
+            rows = getattr(self, "rows", [[]] * len(self.cells))[k]
+            r = {"status": int(s.status), "istep": int(s.istep), "attempts": int(s.attempts),
+                 "good_step": int(s.good_step) if s.flag else None, "ttime": float(s.ttime),
+                 "rows": np.concatenate(rows) if rows else np.zeros((0, 32))}
+            if fields:
+                r["fields"] = c.download()
+            out.append(r)
+        return out
 
     def batch_timing(self):
         """(device ms, batch attempts) of all batched runs so far."""
@@ -285,7 +362,7 @@ class Ensemble:
         out = []
         for c in self.cells:
             out.append(c.run(n_steps))
-            c.drain()
+        self._collect()
         return out
 
     def close(self):

@@ -178,6 +178,18 @@ class Cell:
         L.check(self.lib.kks_download(self.h, *(L.dptr(v) for v in out)), "kks_download")
         return tuple(out)  # eta, X, X_al, X_th
 
+    def set_wait_polls(self, polls):
+        """Poll count of the first bounded wait of the fused passes (a test
+        hook for the timeout path; negative restores the default)."""
+        L.check(self.lib.kks_set_wait_polls(self.h, int(polls)), "kks_set_wait_polls")
+
+    def download_pair(self):
+        """The minus entry of the energy residual's pair: (eta-, X-, mu-, G-),
+        each (nx, ny, 1) float64 (kks_download_pair)."""
+        out = [np.empty((self.nx, self.ny, 1), dtype=np.float64) for _ in range(4)]
+        L.check(self.lib.kks_download_pair(self.h, *(L.dptr(v) for v in out)), "kks_download_pair")
+        return tuple(out)
+
     def elastic_fields(self):
         """sig_el, eps_el with shape (3, 3, nx, ny, 1)."""
         s4 = np.empty((4, self.nx, self.ny), dtype=np.float64)
@@ -316,6 +328,21 @@ class Cell:
             pass
 
 
+def raise_for_status(cell, status):
+    """The error a stopped cell reports: AdaptiveStepError with the reference's
+    messages for its two stops (pf_kks/solver.py:292-295, 312-313), KksError
+    when a bounded device wait ran out."""
+    if status == L.KKS_STATUS_OK:
+        return
+    s = cell.state()
+    if status == L.KKS_STATUS_TIMEOUT:
+        raise L.KksError(f"step {s.istep}: a bounded device wait ran out (bulk copy not completed)")
+    if status == L.KKS_STATUS_MAX_ITER:
+        raise AdaptiveStepError(f"step {s.error_istep}: no admissible time step after "
+                                f"{s.error_iteration} attempts (dtime_s={s.error_dtime_s:.2e})")
+    raise AdaptiveStepError(f"step {s.error_istep}: non-finite energy residual")
+
+
 def _residual(r):
     return Residual(r.res_total, r.res_energy_derivative, r.res_diffusion, r.res_allen_cahn, r.res_temperature)
 
@@ -447,14 +474,7 @@ def run(cfg, eta, X, X_al, X_th, out_dir=".", base_dir=".", write_logs=True, ver
             hb.records(recs)
             hb.rows(rows)
             log.flush()
-            if status != L.KKS_STATUS_OK:
-                s = cell.state()
-                if status == L.KKS_STATUS_TIMEOUT:
-                    raise L.KksError(f"step {s.istep}: a bounded device wait ran out (bulk copy not completed)")
-                if status == L.KKS_STATUS_MAX_ITER:
-                    raise AdaptiveStepError(f"step {s.error_istep}: no admissible time step after "
-                                            f"{s.error_iteration} attempts (dtime_s={s.error_dtime_s:.2e})")
-                raise AdaptiveStepError(f"step {s.error_istep}: non-finite energy residual")
+            raise_for_status(cell, status)
             done = stop
             if stop in schedule.map_steps:
                 e, x, xa, xt = cell.download()

@@ -20,8 +20,9 @@ ramp1420   1420^2, 40 cells, ~1200 particles R~U(3,10); 400->719 K at 20 K/min,
            adaptive, mixed precision
 ensemble   48 cells of side {128,192,256,384,512}, seeds 0-47, particles
            proportional to area, heating U(5,40) K/min from 400 to 600 K
-adjoint256 256^2, 8 cells; 500->520 K ramp, 300 fixed-dt steps; c_D x 1.2, sink distance
-           x 1/sqrt(0.8), c_gamma x 1.1 (the gradient workload)
+adjoint256 256^2, 8 cells; 500->520 K ramp, 300 fixed-dt steps at the demo parameters; the
+           target DSC comes from the same run with Si mobility x 1.2, vacancy annealing
+           rate x 0.8 and interface energy x 1.1 (ADJOINT_TARGET_FACTORS)
 =========  ==========================================================================
 """
 
@@ -111,13 +112,20 @@ def ensemble(n_instances=48, n_steps=1000, precision="mixed"):
     return out
 
 
-def adjoint256(n_steps=300, precision="fp64", seed=0):
-    """Fixed-dt run for gradients: the diffusivity (c_D x 1.2), sink distance
-    (x 1/sqrt(0.8)) and interface energy (c_gamma x 1.1) perturbed from the
-    demo parameters."""
+# (Si mobility prefactor, vacancy annealing rate, interface energy) of the
+# target run of the gradient workload, relative to the base parameters
+ADJOINT_TARGET_FACTORS = (1.2, 0.8, 1.1)
+
+
+def adjoint256(n_steps=300, precision="fp64", seed=0, factors=(1.0, 1.0, 1.0)):
+    """Fixed-dt run for gradients at the demo parameters; ``factors``
+    multiply the Si mobility prefactor (c_D), the vacancy annealing rate
+    (Deff / Lv^2: the sink distance is divided by its square root) and the
+    interface energy (c_gamma)."""
+    fD, fA, fG = factors
     cfg = base_config(nx=256, ny=256, n_steps=n_steps, schedule_time=[0, 60.0], schedule_temperature=[500, 520],
-                      x_equilibrium=0.0, n_map_saves=2, n_surface_samples=n_steps, c_D=1.2,
-                      vacancy_sink_distance=250e-9 / 0.8**0.5, c_gamma=1.1)
+                      x_equilibrium=0.0, n_map_saves=2, n_surface_samples=n_steps, c_D=1.0 * fD,
+                      vacancy_sink_distance=250e-9 / fA**0.5, c_gamma=1.0 * fG)
     cfg.gpu = GpuOptions(precision=precision)
     spec = MicrostructureSpec(256, 256, n_cells=8, n_particles=102, r_min=3, r_max=8, seed=seed)
     return cfg, spec

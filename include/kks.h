@@ -202,6 +202,25 @@ int kks_get_state(kks_handle* h, kks_run_state* state);
 /* Download the current fields (host float64, nx*ny each); any pointer may be NULL. */
 int kks_download(kks_handle* h, double* eta, double* X, double* X_al, double* X_th);
 
+/* Fault-path test hook; no counterpart in the reference. The fused passes of
+ * the mixed path wait for their bulk and tensor copies on an mbarrier with a
+ * bounded number of polls; when a wait runs out, the cell's status becomes
+ * KKS_STATUS_TIMEOUT, the block still waits (bounded again) for its copies in
+ * flight, and kks_run stops after that attempt. This sets the poll count of the
+ * first wait of a cell's passes (0: every such wait gives up at once; < 0: the
+ * default, 2^20). KKS_ERR_STATE for a cell without fused passes. */
+int kks_set_wait_polls(kks_handle* h, int32_t polls);
+
+/* The "minus" entry of the energy residual's pair (the second-to-last element
+ * of the reference's pair lists, pf_kks/solver.py:172-173, 278-290, 353-365):
+ * eta- and X- (after an accepted step the current state, after a rejection the
+ * rejected attempt's fields), the diffusion potential mu- of the last attempt
+ * and the free energy G- (after an accepted step the step's pre-update G_s),
+ * each host float64, nx*ny, in the units of the normalised step. With the
+ * current state and kks_get_state this is the whole loop state of the
+ * reference's solver at a step boundary. Any pointer may be NULL. */
+int kks_download_pair(kks_handle* h, double* eta_m, double* X_m, double* mu_m, double* G_m);
+
 /* Elastic stress and strain of the last attempt (returned by solve_elasticity,
  * pf_kks/elasticity.py:107-163; SimulationResult.sig_el / eps_el). Components
  * xx, yy, zz, xy (xz = yz = 0 in 2-D), nx*ny each: sig4 and eps4 hold 4*nx*ny. */
@@ -237,10 +256,13 @@ int kks_destroy(kks_handle* h);
  * Runs asynchronously on `stream` (a cudaStream_t, NULL = default stream).
  * Its scratch is a fixed device array of KKS_NOALLOC_MAX_BLOCKS x 6 doubles
  * (48 KiB) held by every GPU that loads the library; nx*ny above
- * KKS_NOALLOC_MAX_POINTS is rejected with KKS_ERR_CAPACITY. The first call on
- * a device looks up that array's address (make it before any stream capture).
- * Calls share the array: calls that overlap on the GPU race and must be
- * serialised by the caller. */
+ * KKS_NOALLOC_MAX_POINTS is rejected with KKS_ERR_CAPACITY, and nx or ny below
+ * 2 with KKS_ERR_ARG (the interface count needs 2 x 2 corners). The first call
+ * on a device looks up that array's address (make it before any stream
+ * capture); a call that finds another context current than the one of that
+ * lookup (after cudaDeviceReset, for instance) looks it up again. Calls share
+ * the array: calls that overlap on the GPU race and must be serialised by the
+ * caller. */
 #define KKS_NOALLOC_MAX_BLOCKS 1024
 #define KKS_NOALLOC_MAX_POINTS (1 << 26)
 int kks_state_sums_noalloc(const double* eta, const double* X, int32_t nx, int32_t ny, double* out, void* stream);

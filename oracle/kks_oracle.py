@@ -438,6 +438,7 @@ class Result:
     map_files: list = field(default_factory=list)
     history: dict = field(default_factory=dict)
     attempts: int = 0
+    snapshots: dict = field(default_factory=dict)
 
 
 HIST_NAMES = ("deta_mean", "eta_mean", "T", "dT", "dtime", "time", "time_s", "surf", "X_al_mean", "X_th_mean",
@@ -462,13 +463,25 @@ def _nanmean_masked(a, mask):
 
 
 def run(cfg, eta, X, X_al, X_th, tables_path, out_dir=".", write_logs=True, verbose=False, save_maps=True,
-        fft_workers=None, max_steps=None, on_attempt=None):
+        fft_workers=None, max_steps=None, on_attempt=None, resume=None, snapshot_steps=()):
     """Restatement of ``pf_kks.solver.run`` (pf_kks/solver.py:76-414).
 
     ``tables_path`` is the resolved material-table file (the reference resolves
     ``cfg.material_tables`` against ``base_dir``, :102). ``max_steps`` stops the
     loop early (used for bounded CPU-baseline samples); ``on_attempt`` is called
     after each attempt with a dict of the attempt's scalars.
+
+    ``resume`` restarts the loop at a step boundary from a complete loop state
+    (the reference itself has no restart): a dict with ``istep`` (the next
+    step), the scalars ``flag, good_step, t, t_s, t_b, ttime, Xv, dtime_s, D_0,
+    Meta_0, surf, surf_b, T_b`` (``T_b`` None while unset), the per-step
+    ``history`` lists of the steps before (at least ``time_s``), ``energy`` and
+    ``dtime_s_hist`` arrays of those steps (optionally ``residuals``: the five
+    residual-term arrays by name), and, once the adaptive scheme is
+    armed, the pair's last entry ``eta_m, X_m, mu_m, G_m`` (pf_kks/solver.py:
+    172-173, 353-365). eta, X, X_al, X_th are then the state at ``istep``.
+    ``snapshot_steps``: steps at whose start such a dict (plus the four fields
+    under ``state``) is recorded in ``Result.snapshots``.
     """
     t_wall = time.time()
     log = RunLog(out_dir, enabled=write_logs)
@@ -523,7 +536,41 @@ def run(cfg, eta, X, X_al, X_th, tables_path, out_dir=".", write_logs=True, verb
     attempts = 0
     sig_el = eps_el = None
 
-    for istep in range(nstep):
+    start = 0
+    if resume is not None:
+        start = int(resume["istep"])
+        flag = int(resume["flag"])
+        good_step = int(resume["good_step"]) if flag else None
+        t, t_s, t_b, ttime = resume["t"], resume["t_s"], resume["t_b"], resume["ttime"]
+        Xv, dtime_s = resume["Xv"], resume["dtime_s"]
+        D_0, Meta_0 = resume["D_0"], resume["Meta_0"]
+        surf, surf_b, T_b = resume["surf"], resume["surf_b"], resume["T_b"]
+        for name, values in resume["history"].items():
+            hist[name] = list(values)[:start]
+        energy_hist[:start] = np.asarray(resume["energy"])[:start]
+        dtime_s_hist[:start] = np.asarray(resume["dtime_s_hist"])[:start]
+        for name, values in resume.get("residuals", {}).items():
+            res_hist[name][:start] = np.asarray(values)[:start]
+        if flag:
+            for name in pair:
+                pair[name] = [None]
+            pair["eta"], pair["X"] = [resume["eta_m"]], [resume["X_m"]]
+            pair["mu"], pair["G"] = [resume["mu_m"]], [resume["G_m"]]
+
+    snapshots = {}
+    for istep in range(start, nstep):
+        if istep in snapshot_steps:
+            snapshots[istep] = {
+                "istep": istep, "flag": flag, "good_step": good_step, "t": t, "t_s": t_s, "t_b": t_b,
+                "ttime": ttime, "Xv": Xv, "dtime_s": dtime_s, "D_0": D_0, "Meta_0": Meta_0, "surf": surf,
+                "surf_b": surf_b, "T_b": T_b, "history": {k: list(v) for k, v in hist.items()},
+                "energy": energy_hist[:istep].copy(), "dtime_s_hist": dtime_s_hist[:istep].copy(),
+                "residuals": {k: v[:istep].copy() for k, v in res_hist.items()},
+                "state": tuple(np.array(a, copy=True) for a in (eta, X, X_al, X_th)),
+            }
+            if flag:
+                snapshots[istep].update(eta_m=pair["eta"][-1], X_m=pair["X"][-1], mu_m=pair["mu"][-1],
+                                        G_m=pair["G"][-1])
         iteration = 1
         while True:
             attempts += 1
@@ -712,4 +759,4 @@ def run(cfg, eta, X, X_al, X_th, tables_path, out_dir=".", write_logs=True, verb
     hist["dtime_s"] = dtime_s_hist
     for name, values in res_hist.items():
         hist["residual_" + name] = values
-    return Result(X, X_al, X_th, eta, sig_el, eps_el, good_step, ttime, map_files, hist, attempts)
+    return Result(X, X_al, X_th, eta, sig_el, eps_el, good_step, ttime, map_files, hist, attempts, snapshots)

@@ -107,3 +107,30 @@ def relaxed_state(small_golden):
     pf_kks and stored in the golden fixtures."""
     g = small_golden
     return tuple(np.array(g[f"relaxed_{k}"]) for k in ("eta", "X", "X_al", "X_th"))
+
+
+def gpu_loop_state(cell, rows):
+    """The loop state of a GPU cell at its current step boundary, in the form
+    the oracle's ``resume`` takes, and the current fields. ``rows`` are all the
+    history rows the cell produced so far (one per step, from ``drain``)."""
+    from pf_kks_gpu import _lib as L
+    from pf_kks_gpu.solver import HIST_NAMES
+
+    s = cell.state()
+    rows = np.asarray(rows)
+    assert rows.shape[0] == s.istep
+    H = L.H
+    hist = {name: [float(v) for v in rows[:, H[name]]] for name in HIST_NAMES}
+    if s.istep:
+        hist["time"][0] = 0
+    resume = {
+        "istep": int(s.istep), "flag": int(s.flag), "good_step": int(s.good_step), "t": s.t, "t_s": s.t_s,
+        "t_b": s.t_b, "ttime": s.ttime, "Xv": s.Xv, "dtime_s": s.dtime_s, "D_0": s.D_0, "Meta_0": s.Meta_0,
+        "surf": s.surf, "surf_b": s.surf_b, "T_b": s.T_b, "history": hist,
+        "energy": rows[:, H["energy_s"]].copy(), "dtime_s_hist": rows[:, H["dtime_s"]].copy(),
+        "residuals": {name: rows[:, H["residual_" + name]].copy()
+                      for name in ("total", "energy_derivative", "diffusion", "allen_cahn", "temperature")},
+    }
+    if s.flag:
+        resume["eta_m"], resume["X_m"], resume["mu_m"], resume["G_m"] = cell.download_pair()
+    return resume, cell.download()

@@ -62,34 +62,80 @@ def test_coefficients_are_differentiable():
     assert float(lcM.grad) != 0.0
 
 
-class _ToyEnthalpy:
-    """Smooth stand-ins for the CALPHAD enthalpies (J/mol)."""
+def test_thermo_restatement_matches_reference():
+    """The torch restatement of the CALPHAD functions of the simulated DSC
+    against pf_kks.thermo (golden/make_thermo_fixture.py)."""
+    from conftest import GOLDEN
+    from pf_kks_gpu import dsc
 
-    def hm_fcc(self, T, x):
-        return -2000.0 + 5.0 * T + 3.0e4 * x
+    g = np.load(f"{GOLDEN}/reference_thermo.npz")
+    T = torch.tensor(g["T"])[:, None].expand(-1, g["x"].size)
+    x = torch.tensor(g["x"])[None, :].expand(g["T"].size, -1)
+    th = dsc.phase_thermo(T, x)
+    for name, value in (("Hm_fcc", th.Hm_fcc), ("d_Hm_fcc_dSi", th.dHm_fcc_dx), ("cp_fcc", th.cp_fcc),
+                        ("Vmfcc", th.Vm_fcc)):
+        np.testing.assert_allclose(value.numpy(), g[name], rtol=1e-12, atol=0, err_msg=name)
+    for name, value in (("Hm_dia", th.Hm_dia[:, 0]), ("cp_dia", th.cp_dia[:, 0]), ("Vmdia", th.Vm_dia[:, 0])):
+        np.testing.assert_allclose(value.numpy(), g[name], rtol=1e-12, atol=0, err_msg=name)
 
-    def hm_dia(self, T):
-        return 1.0e4 + 2.0 * T
 
-    def dhm_fcc_dx(self, T, x):
-        return 3.0e4 + 0 * T + 0 * x
+def test_thermo_derivative_in_x_is_the_enthalpy_slope():
+    from pf_kks_gpu import dsc
+
+    T = torch.tensor([450.0, 520.0, 710.0], dtype=torch.float64)
+    x = torch.tensor([0.004, 0.02, 0.05], dtype=torch.float64, requires_grad=True)
+    th = dsc.phase_thermo(T, x)
+    (g,) = torch.autograd.grad(th.Hm_fcc.sum(), x)
+    np.testing.assert_allclose(g.numpy(), th.dHm_fcc_dx.detach().numpy(), rtol=1e-12)
 
 
-def test_finite_difference_dsc_follows_the_histories():
+def test_simulated_dsc_terms_by_hand():
+    """The three terms of pf_kks/postprocess/dsc.py:121-130 with forward
+    differences, checked by hand on the first interval."""
+    from pf_kks_gpu import dsc
+
     cfg, tables, _ = fixed_dt_case(n=5)
     coef, t, T = A.coefficients(cfg, tables, 5, return_times=True)
     assert t[0] == 0 and torch.all(t[1:] > t[:-1])
     assert float(T[-1]) == pytest.approx(float(np.interp(float(t[-1]), cfg.schedule_time, cfg.schedule_temperature)))
     f = torch.tensor([0.10, 0.11, 0.13, 0.16, 0.17], dtype=torch.float64, requires_grad=True)
     x = torch.tensor([0.020, 0.019, 0.017, 0.016, 0.0158], dtype=torch.float64, requires_grad=True)
-    q = A.finite_difference_dsc(f, x, t, T, _ToyEnthalpy(), heating_rate=20 / 60)
-    assert q.shape == (4,)
-    # by hand for the first interval
-    e = _ToyEnthalpy()
-    dt0 = float(t[1] - t[0])
-    T0 = float(T[0])
-    ref0 = ((1 - 0.10) * 3.0e4 * (0.019 - 0.020) / dt0 / A.M_AL
-            + (0.11 - 0.10) / dt0 * (e.hm_dia(T0) / A.M_SI - e.hm_fcc(T0, 0.020) / A.M_AL)) / (20 / 60)
-    assert float(q[0].detach()) == pytest.approx(ref0, rel=1e-12)
-    q.sum().backward()
+    surf = torch.tensor([1.0e-8, 1.2e-8, 1.1e-8, 1.5e-8, 1.6e-8], dtype=torch.float64)
+    p = dsc.DSCParameters.for_config(cfg)
+    q = dsc.simulated_dsc(f, x, surf, t, T, p)
+    assert q.total.shape == (4,)
+    dt0, T0 = float(t[1] - t[0]), float(T[0])
+    th = dsc.phase_thermo(torch.tensor([T0], dtype=torch.float64), torch.tensor([0.020], dtype=torch.float64))
+    rho = 0.10 * dsc.M_SI / float(th.Vm_dia) + 0.90 * dsc.M_AL / float(th.Vm_fcc)
+    bg = p.heating_rate * (0.10 * float(th.cp_dia) / dsc.M_SI + 0.90 * float(th.cp_fcc) / dsc.M_AL)
+    su = p.interface_energy * (0.2e-8) / dt0 / (p.simulated_area * rho)
+    pr = (0.90 * float(th.dHm_fcc_dx) / dsc.M_AL * (0.019 - 0.020) / dt0
+          + (0.11 - 0.10) / dt0 * (float(th.Hm_dia) / dsc.M_SI - float(th.Hm_fcc) / dsc.M_AL))
+    assert float(q.background[0]) == pytest.approx(bg, rel=1e-12)
+    assert float(q.surface[0]) == pytest.approx(su, rel=1e-12)
+    assert float(q.precipitation[0]) == pytest.approx(pr, rel=1e-12)
+    assert float(q.total[0]) == pytest.approx((bg + su + pr) * p.output_scale, rel=1e-12)
+    q.total.sum().backward()
     assert torch.all(torch.isfinite(f.grad)) and torch.all(torch.isfinite(x.grad))
+
+
+def test_three_parameter_offsets():
+    """c_gamma scales the interface energy: kappa^2 and w scale with it, while
+    the thin-interface L (pf_kks/kinetics.py:72-80) does not depend on it
+    (sigma / kappa^2 and kappa / sqrt(w) are both free of sigma). The
+    annealing-rate offset moves the vacancy fraction and with it D. Zero
+    offsets reproduce the unperturbed chain bit for bit."""
+    cfg, tables, _ = fixed_dt_case(n=4)
+    base = A.coefficients(cfg, tables, 4)
+    z = torch.zeros((), dtype=torch.float64)
+    same = A.coefficients(cfg, tables, 4, z, z, log_c_gamma=z, log_anneal=z)
+    assert torch.equal(base, same)
+    lg = torch.tensor(np.log(1.1), dtype=torch.float64)
+    g = A.coefficients(cfg, tables, 4, log_c_gamma=lg)
+    np.testing.assert_allclose((g[:, 2] / base[:, 2]).numpy(), 1.1, rtol=1e-14)  # kappa^2 ~ gamma
+    np.testing.assert_allclose((g[:, 4] / base[:, 4]).numpy(), 1.1, rtol=1e-14)  # w ~ gamma
+    np.testing.assert_allclose(g[:, 1].numpy(), base[:, 1].numpy(), rtol=1e-14)
+    la = torch.tensor(np.log(0.8), dtype=torch.float64, requires_grad=True)
+    an = A.coefficients(cfg, tables, 4, log_anneal=la)
+    an[1:, 3].sum().backward()  # D_s of the steps after the first relaxation
+    assert float(la.grad) != 0.0

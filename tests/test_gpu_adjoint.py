@@ -58,23 +58,35 @@ def test_vjp_matches_autograd():
         assert abs(dcoef[j] - gc[j]) <= 1e-8 * scale + 1e-12 * np.max(np.abs(gc)), (j, dcoef[j], gc[j])
 
 
-def _loss_fn(n, N):
-    from test_adjoint_cpu import _ToyEnthalpy
+def _torch_run(tstep, coef, s0, surf_scale):
+    """The fixed-dt run through the pure-torch step (autograd reference):
+    eta_mean, X_al_mean, surf of each step's input state and the final state."""
+    from pf_kks_gpu.adjoint import _interface_cells
+
+    s = s0.clone()
+    ems, xms, surf = [], [], []
+    for i in range(coef.shape[0]):
+        mask = s[0] < 0.05
+        ems.append(s[0].mean())
+        xms.append((s[1] * mask).sum() / mask.sum())
+        surf.append((_interface_cells(s[0].detach()) * surf_scale).to(torch.float64))
+        s = tstep(s, coef[i])
+    return torch.stack(ems), torch.stack(xms), torch.stack(surf), s
+
+
+def _loss_fn(n, cfg):
+    from pf_kks_gpu.dsc import DSCParameters, simulated_dsc
 
     gen = np.random.default_rng(11)
     w = torch.tensor(gen.normal(size=n), dtype=torch.float64, device="cuda")
     v = torch.tensor(gen.normal(size=n), dtype=torch.float64, device="cuda")
+    params = DSCParameters.for_config(cfg)
 
-    def loss(eta_mean, xal_mean, final, t=None, T=None):
+    def loss(eta_mean, xal_mean, surf, final, t, T):
         # a smooth functional of the histories and the final state, plus the
-        # sum of squares of a finite-difference simulated DSC when times are given
-        val = (w * eta_mean).sum() * 10 + (v * xal_mean).sum() * 100 + (final[0] ** 2).mean()
-        if t is not None:
-            from pf_kks_gpu.adjoint import finite_difference_dsc
-
-            q = finite_difference_dsc(eta_mean, xal_mean, t.to("cuda"), T.to("cuda"), _ToyEnthalpy(), 20 / 60)
-            val = val + 1e-3 * (q**2).sum()
-        return val
+        # sum of squares of the simulated DSC
+        q = simulated_dsc(eta_mean, xal_mean, surf, t.to("cuda"), T.to("cuda"), params).total
+        return (w * eta_mean).sum() * 10 + (v * xal_mean).sum() * 100 + (final[0] ** 2).mean() + 1e-3 * (q**2).sum()
 
     return loss
 
@@ -82,13 +94,13 @@ def _loss_fn(n, N):
 def test_gradient_matches_finite_differences_and_torch_autograd():
     n = 12
     A, cfg, tables, state, stepper, tstep, s0 = _setup(n=n)
-    loss = _loss_fn(n, cfg.nx * cfg.ny)
+    loss = _loss_fn(n, cfg)
     run = A.FixedDtRun
 
     def objective(lcD, lcM):
         coef, t, T = A.coefficients(cfg, tables, n, lcD, lcM, return_times=True)
-        em, xm, fin = run.apply(coef, s0, stepper, 5)
-        return loss(em, xm, fin, t, T)
+        em, xm, surf, fin = run.apply(coef, s0, stepper, 5)
+        return loss(em, xm, surf, fin, t, T)
 
     lcD = torch.zeros((), dtype=torch.float64, requires_grad=True)
     lcM = torch.zeros((), dtype=torch.float64, requires_grad=True)
@@ -114,17 +126,69 @@ def test_gradient_matches_finite_differences_and_torch_autograd():
     lcD2 = torch.zeros((), dtype=torch.float64, requires_grad=True)
     lcM2 = torch.zeros((), dtype=torch.float64, requires_grad=True)
     coef, t2, T2 = A.coefficients(cfg, tables, n, lcD2, lcM2, return_times=True)
-    coef = coef.to("cuda")
-    s = s0.clone()
-    ems, xms = [], []
-    for i in range(n):
-        mask = s[0] < 0.05
-        ems.append(s[0].mean())
-        xms.append((s[1] * mask).sum() / mask.sum())
-        s = tstep(s, coef[i])
-    loss(torch.stack(ems), torch.stack(xms), s, t2, T2).backward()
+    em, xm, surf, fin = _torch_run(tstep, coef.to("cuda"), s0, stepper.surf_scale)
+    loss(em, xm, surf, fin, t2, T2).backward()
     g2 = np.array([float(lcD2.grad), float(lcM2.grad)])
     assert np.all(np.abs(g - g2) <= 1e-9 * np.abs(g2)), (g, g2)
+
+
+def test_dsc_gradient_of_the_three_kinetic_parameters():
+    """The gradient workload as specified (adjoint256: 256^2, 8 Voronoi cells,
+    300 fixed-dt steps on the 500 -> 520 K ramp, checkpoints every 50 steps):
+    loss = sum over the window of (simulated DSC - target)^2, the target made
+    by the same forward run with Si mobility x 1.2, vacancy annealing rate x
+    0.8 and interface energy x 1.1; gradients with respect to the log of the
+    three factors at the base parameters, against central differences of the
+    GPU forward with h = 1e-6 (relative) and against autograd through the
+    pure-torch FP64 step."""
+    from pf_kks_gpu import adjoint as A
+    from pf_kks_gpu import workloads
+    from pf_kks_gpu.materials import MaterialTables
+
+    n, K = 300, 50
+    cfg, spec = workloads.adjoint256(n_steps=n)
+    tables = MaterialTables.from_npz(cfg.material_tables, cfg.c_gamma, cfg.c_eps0)
+    state = workloads.initial_state(cfg, spec)
+    stepper = A.StepAdjoint.for_config(cfg, tables, device=0)
+    s0 = A.initial_state_tensor(*state, device=0)
+    target_theta = torch.tensor(np.log(workloads.ADJOINT_TARGET_FACTORS), dtype=torch.float64)
+    with torch.no_grad():
+        q_target = A.dsc_of_run(cfg, tables, s0, stepper, n, target_theta, checkpoint_every=K).total
+
+    def loss_at(theta):
+        q = A.dsc_of_run(cfg, tables, s0, stepper, n, theta, checkpoint_every=K).total
+        return ((q - q_target) ** 2).sum()
+
+    theta = torch.zeros(3, dtype=torch.float64, requires_grad=True)
+    loss = loss_at(theta)
+    loss.backward()
+    g = theta.grad.numpy().copy()
+    assert float(loss) > 0 and np.all(np.isfinite(g))
+    h = 1e-6
+    fd = np.zeros(3)
+    for k in range(3):
+        vals = []
+        for sgn in (1, -1):
+            th = torch.zeros(3, dtype=torch.float64)
+            th[k] = sgn * h
+            with torch.no_grad():
+                vals.append(float(loss_at(th)))
+        fd[k] = (vals[0] - vals[1]) / (2 * h)
+    assert np.all(np.abs(g - fd) <= 1e-4 * np.max(np.abs(fd)) + 1e-3 * np.abs(fd)), (g, fd)
+    # autograd through the pure-torch FP64 step
+    T0 = float(np.interp(0.0, cfg.schedule_time, cfg.schedule_temperature))
+    tstep = TorchStep(cfg.nx, cfg.ny, tables.at(T0, "C11"), tables.at(T0, "C12"), tables.at(T0, "C44"), "cuda")
+    from pf_kks_gpu.dsc import DSCParameters, simulated_dsc
+
+    theta2 = torch.zeros(3, dtype=torch.float64, requires_grad=True)
+    coef, t, T = A.coefficients(cfg, tables, n, log_c_D=theta2[0], log_anneal=theta2[1], log_c_gamma=theta2[2],
+                                return_times=True)
+    em, xm, surf, _ = _torch_run(tstep, coef.to("cuda"), s0, stepper.surf_scale)
+    q = simulated_dsc(em, xm, surf, t.to("cuda"), T.to("cuda"), DSCParameters.for_config(cfg)).total
+    ((q - q_target) ** 2).sum().backward()
+    g2 = theta2.grad.numpy()
+    assert np.all(np.abs(g - g2) <= 1e-8 * np.max(np.abs(g2))), (g, g2)
+    stepper.close()
 
 
 def test_forward_run_matches_main_fp64_cell():
@@ -134,7 +198,7 @@ def test_forward_run_matches_main_fp64_cell():
     A, cfg, tables, state, stepper, tstep, s0 = _setup(n=n)
     coef = A.coefficients(cfg, tables, n)
     with torch.no_grad():
-        _, _, fin = A.FixedDtRun.apply(coef, s0, stepper, 3)
+        _, _, _, fin = A.FixedDtRun.apply(coef, s0, stepper, 3)
     cell = solver.Cell(cfg, tables, precision="fp64", device=0)
     cell.upload(*state)
     cell.run(n)

@@ -185,3 +185,30 @@ def test_logs_fixture_is_consistent():
     with open(os.path.join(GOLDEN, "reference_small_logs.json")) as f:
         logs = json.load(f)
     assert logs["rejected40"]["dtime.txt"].count("RE>resmax") == 49
+
+
+@pytest.mark.parametrize("case", ["accepted30", "enlarged40"])
+def test_resume_from_loop_state_is_exact(tmp_path, relaxed_state, small_golden, case):
+    """The oracle restarted at a step boundary of an armed run from its
+    complete loop state (fields, scalars, histories, the residual pair's last
+    entry) continues exactly as the uninterrupted run: this is how device
+    states are handed to the oracle at large step counts."""
+    if case == "accepted30":
+        cfg = small_config(n_steps=30, x_equilibrium=0.2)
+    else:
+        cfg = small_config(n_steps=40, x_equilibrium=0.2, dtime_s=60, dtime_max=150, residual_min=7.6e-4)
+    full = kks_oracle.run(cfg, *copy_state(relaxed_state), cfg.material_tables, out_dir=str(tmp_path / "full"),
+                          snapshot_steps={17})
+    snap = full.snapshots[17]
+    assert snap["flag"] == 1 and snap["good_step"] == 2
+    part = kks_oracle.run(cfg, *copy_state(snap["state"]), cfg.material_tables, out_dir=str(tmp_path / "part"),
+                          resume=snap)
+    for name in FIELDS:
+        np.testing.assert_array_equal(getattr(part, name), getattr(full, name), err_msg=name)
+    for name in HIST:
+        np.testing.assert_array_equal(np.asarray(part.history[name], float), np.asarray(full.history[name], float),
+                                      err_msg=name)
+    np.testing.assert_array_equal(full.X, small_golden[f"{case}_X"])
+    full_log = (tmp_path / "full" / "log.txt").read_text().splitlines()
+    part_log = (tmp_path / "part" / "log.txt").read_text().splitlines()
+    assert part_log[1:] == full_log[-(len(part_log) - 1):]
