@@ -25,8 +25,21 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "kks_fft.cuh"
 #include "kks_internal.cuh"
+
+// NVTX ranges around the library's calls (header-only NVTX v3: free when no
+// profiler is attached), so that a timeline shows which call a device span
+// belongs to; the attempt graphs' kernels carry their own names.
+namespace {
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+};
+}  // namespace
+#define KKS_RANGE(name) NvtxRange kks_nvtx_range_(name)
 
 static thread_local std::string g_last_error;
 
@@ -585,6 +598,7 @@ const char* kks_version(void) { return "kks_b200 1.0 (sm_100a, cuFFT)"; }
 
 int kks_create(const kks_params* params, int precision, int device, int32_t n_steps, const uint8_t* step_flags,
                int64_t record_capacity, kks_handle** out) {
+  KKS_RANGE("kks_create");
   if (!params || !out) return set_error(KKS_ERR_ARG, "null argument");
   *out = nullptr;
   if (params->nx < 2 || params->ny < 2) return set_error(KKS_ERR_ARG, "nx and ny must be >= 2 (np.gradient)");
@@ -643,6 +657,7 @@ static int get_field(kks_handle* h, double* dst, const void* src, bool is_double
 static int reset_loop(kks_handle* h);
 
 int kks_upload(kks_handle* h, const double* eta, const double* X, const double* X_al, const double* X_th) {
+  KKS_RANGE("kks_upload");
   if (!h || !eta || !X || !X_al || !X_th) return set_error(KKS_ERR_ARG, "null argument");
   CK(cudaSetDevice(h->device));
   const bool d = h->precision == KKS_PRECISION_FP64;
@@ -697,6 +712,7 @@ static int drain_device(kks_handle* h) {
 }
 
 int kks_run(kks_handle* h, int32_t n_steps, int32_t* status) {
+  KKS_RANGE("kks_run");
   if (!h || n_steps < 0) return set_error(KKS_ERR_ARG, "bad argument");
   if (!h->uploaded) return set_error(KKS_ERR_STATE, "kks_run before kks_upload");
   CK(cudaSetDevice(h->device));
@@ -714,6 +730,7 @@ int kks_run(kks_handle* h, int32_t n_steps, int32_t* status) {
   long long launched = 0;
   while (c->istep < target && c->status == KKS_STATUS_OK) {
     long long todo = std::min(target - c->istep, max_batch);
+    KKS_RANGE("attempt graphs");
     for (long long a = 0; a < todo; ++a) {
       CK(cudaGraphLaunch(h->graph[h->parity], h->stream));
       h->parity ^= 1;
@@ -738,6 +755,7 @@ int kks_run(kks_handle* h, int32_t n_steps, int32_t* status) {
 }
 
 int kks_run_many(kks_handle** cells, int32_t n_cells, const int32_t* n_steps, int32_t* status) {
+  KKS_RANGE("kks_run_many");
   if (!cells || n_cells < 0 || (n_cells > 0 && !n_steps)) return set_error(KKS_ERR_ARG, "bad argument");
   std::vector<long long> target(n_cells), launched(n_cells, 0);
   for (int i = 0; i < n_cells; ++i) {
@@ -975,6 +993,7 @@ static int batch_create_impl(kks_batch* b, int n_groups) {
 }
 
 int kks_batch_create(kks_handle* const* cells, int32_t n_cells, int32_t groups, kks_batch** out) {
+  KKS_RANGE("kks_batch_create");
   if (!cells || !out || n_cells < 1 || groups < 1) return set_error(KKS_ERR_ARG, "bad argument");
   *out = nullptr;
   for (int i = 0; i < n_cells; ++i) {
@@ -1005,6 +1024,7 @@ int kks_batch_create(kks_handle* const* cells, int32_t n_cells, int32_t groups, 
 }
 
 int kks_batch_run(kks_batch* b, const int32_t* n_steps, int32_t* status) {
+  KKS_RANGE("kks_batch_run");
   if (!b || !n_steps) return set_error(KKS_ERR_ARG, "bad argument");
   const int n = (int)b->cells.size();
   std::vector<long long> target(n);
@@ -1089,6 +1109,7 @@ int kks_batch_destroy(kks_batch* b) {
 
 int kks_drain(kks_handle* h, kks_record* records, int64_t record_cap, int64_t* n_records, kks_step_row* rows,
               int64_t row_cap, int64_t* n_rows) {
+  KKS_RANGE("kks_drain");
   if (!h) return set_error(KKS_ERR_ARG, "null handle");
   if (n_records) {
     if (!records && record_cap > 0) return set_error(KKS_ERR_ARG, "null record buffer");
@@ -1137,6 +1158,7 @@ int kks_get_state(kks_handle* h, kks_run_state* s) {
 }
 
 int kks_download(kks_handle* h, double* eta, double* X, double* X_al, double* X_th) {
+  KKS_RANGE("kks_download");
   if (!h) return set_error(KKS_ERR_ARG, "null handle");
   if (!h->uploaded) return set_error(KKS_ERR_STATE, "kks_download before kks_upload");
   CK(cudaSetDevice(h->device));
@@ -1161,6 +1183,7 @@ int kks_set_wait_polls(kks_handle* h, int32_t polls) {
 }
 
 int kks_download_pair(kks_handle* h, double* eta_m, double* X_m, double* mu_m, double* G_m) {
+  KKS_RANGE("kks_download_pair");
   if (!h) return set_error(KKS_ERR_ARG, "null handle");
   if (!h->uploaded) return set_error(KKS_ERR_STATE, "kks_download_pair before kks_upload");
   CK(cudaSetDevice(h->device));
@@ -1212,6 +1235,7 @@ static int sel_total(kks_handle* h, long long* total) {
 static size_t align256(size_t v) { return (v + 255) / 256 * 256; }
 
 int kks_voronoi_edges(kks_handle* h, int32_t n_seeds, const double* seeds, int64_t* n_edges) {
+  KKS_RANGE("kks_voronoi_edges");
   if (!h || !seeds || !n_edges) return set_error(KKS_ERR_ARG, "null argument");
   if (n_seeds < 1) return set_error(KKS_ERR_ARG, "kks_voronoi_edges: n_seeds < 1");
   CK(cudaSetDevice(h->device));
@@ -1234,6 +1258,7 @@ int kks_voronoi_edges(kks_handle* h, int32_t n_seeds, const double* seeds, int64
 }
 
 int kks_generate_fields(kks_handle* h, const kks_gen_args* a) {
+  KKS_RANGE("kks_generate_fields");
   if (!h || !a) return set_error(KKS_ERR_ARG, "null argument");
   const int n = a->n_particles;
   if (n < 0 || (n > 0 && (!a->pick || !a->jitter || !a->radii)))
@@ -1316,11 +1341,13 @@ static int place_impl(kks_handle* h, bool add, double dx, double dy, double x_ma
 
 int kks_place_precipitates(kks_handle* h, double dx, double dy, double x_matrix, double x_precipitate, int32_t n,
                            const double* r, const double* ox, const double* oy, const double* oz) {
+  KKS_RANGE("kks_place_precipitates");
   return place_impl(h, false, dx, dy, x_matrix, x_precipitate, n, r, ox, oy, oz);
 }
 
 int kks_add_nuclei(kks_handle* h, double dx, double dy, int32_t n, const double* r, const double* ox,
                    const double* oy, const double* oz) {
+  KKS_RANGE("kks_add_nuclei");
   return place_impl(h, true, dx, dy, 0.0, 0.0, n, r, ox, oy, oz);
 }
 
@@ -1343,6 +1370,7 @@ int kks_count_below(kks_handle* h, double eta_below, int64_t* count) {
 }
 
 int kks_insert_nuclei(kks_handle* h, double eta_below, int32_t n, const int64_t* ranks) {
+  KKS_RANGE("kks_insert_nuclei");
   if (!h || (n > 0 && !ranks)) return set_error(KKS_ERR_ARG, "null argument");
   if (n < 0) return set_error(KKS_ERR_ARG, "kks_insert_nuclei: n < 0");
   if (!h->uploaded) return set_error(KKS_ERR_STATE, "kks_insert_nuclei before the fields are set");
@@ -1391,6 +1419,7 @@ static int elastic_impl(kks_handle* h, int p, double* d_out) {
 extern "C" {
 
 int kks_elastic_fields(kks_handle* h, double* sig4, double* eps4) {
+  KKS_RANGE("kks_elastic_fields");
   if (!h || !sig4 || !eps4) return set_error(KKS_ERR_ARG, "null argument");
   if (!h->uploaded || h->attempts_launched == 0) return set_error(KKS_ERR_STATE, "no attempt has run yet");
   CK(cudaSetDevice(h->device));
@@ -1438,6 +1467,7 @@ static void ckpt_regions(kks_handle* h, void** ptr, size_t* len) {
 }
 
 int kks_checkpoint(kks_handle* h, void* buf, size_t cap, size_t* size) {
+  KKS_RANGE("kks_checkpoint");
   if (!h || !size) return set_error(KKS_ERR_ARG, "null argument");
   const size_t need = ckpt_bytes(h);
   *size = need;
@@ -1461,6 +1491,7 @@ int kks_checkpoint(kks_handle* h, void* buf, size_t cap, size_t* size) {
 }
 
 int kks_restore(kks_handle* h, const void* buf, size_t size) {
+  KKS_RANGE("kks_restore");
   if (!h || !buf) return set_error(KKS_ERR_ARG, "null argument");
   const size_t need = ckpt_bytes(h);
   if (size < need) return set_error(KKS_ERR_CAPACITY, "checkpoint blob too small");
@@ -1543,6 +1574,7 @@ int kks_get_launch_shape(const kks_handle* h, kks_launch_shape* shape) {
 }
 
 int kks_set_launch_shape(kks_handle* h, const kks_launch_shape* shape) {
+  KKS_RANGE("kks_set_launch_shape");
   if (!h || !shape) return set_error(KKS_ERR_ARG, "null argument");
   return apply_shape(h, *shape);
 }
@@ -1567,6 +1599,7 @@ static std::vector<kks_launch_shape> candidate_shapes(const kks_handle* h, bool 
 
 int kks_autotune(kks_handle* h, int32_t attempts, int32_t flags, kks_launch_shape* best,
                  double* best_ms_per_attempt) {
+  KKS_RANGE("kks_autotune");
   if (!h || attempts < 1 || (flags & ~KKS_TUNE_BATCHABLE)) return set_error(KKS_ERR_ARG, "bad argument");
   if (!h->uploaded) return set_error(KKS_ERR_STATE, "kks_autotune before kks_upload");
   if (h->in_batch) return set_error(KKS_ERR_STATE, "the cell belongs to a batch: its launch shape is fixed");
@@ -1654,6 +1687,7 @@ int kks_pipeline(kks_handle* h, int32_t* fused, int32_t* kernels) {
 }
 
 int kks_destroy(kks_handle* h) {
+  KKS_RANGE("kks_destroy");
   free_handle(h);
   return KKS_OK;
 }

@@ -230,7 +230,8 @@ def test_fused_fft_1420_short_run(tmp_path):
     fused = _run_gpu(cfg, state, tmp_path / "fused", precision="mixed")
     assert fused.__class__.__name__ == "SimulationResult", fused
     f64 = _run_gpu(cfg, state, tmp_path / "fp64", precision="fp64")
-    ref = kks_oracle.run(cfg, *copy_state(state), cfg.material_tables, out_dir=str(tmp_path / "cpu"))
+    ref = kks_oracle.run(cfg, *copy_state(state), cfg.material_tables, out_dir=str(tmp_path / "cpu"),
+                         fft_workers=os.cpu_count())
     for name in FIELDS:
         assert rel_l2(getattr(f64, name), getattr(ref, name)) <= FIELD_TOL, name
     _assert_hist_close(f64.history, lambda n: ref.history[n])
@@ -316,7 +317,8 @@ def test_iso735_fp64_and_mixed_against_oracle(tmp_path):
 
     cfg, spec = workloads.iso735(n_steps=30)
     state = workloads.initial_state(cfg, spec)
-    ref = kks_oracle.run(cfg, *copy_state(state), cfg.material_tables, out_dir=str(tmp_path / "cpu"))
+    ref = kks_oracle.run(cfg, *copy_state(state), cfg.material_tables, out_dir=str(tmp_path / "cpu"),
+                         fft_workers=os.cpu_count())
     f64 = _run_gpu(cfg, state, tmp_path / "fp64", precision="fp64")
     for name in FIELDS:
         assert rel_l2(getattr(f64, name), getattr(ref, name)) <= FIELD_TOL, name
