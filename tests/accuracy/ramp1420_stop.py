@@ -7,9 +7,10 @@ whether the oracle stops there too.
    scheme stops the run (AdaptiveStepError: no admissible dt after
    max_iterations attempts, pf_kks/solver.py:292-295) or 6000 steps pass.
 2. A second FP64 cell runs the same steps up to ``back`` steps before the
-   stop (the run is deterministic: the same kernels give the same bits) and
-   hands its complete loop state to the oracle (fields, scalars, history rows
-   and the residual pair's minus entry; tests/conftest.py:gpu_loop_state).
+   stop, and no later than the step at which the adaptive scheme arms (the run
+   is deterministic: the same kernels give the same bits), and hands its
+   complete loop state to the oracle (fields, scalars and history rows;
+   tests/conftest.py:gpu_loop_state), which then arms by itself.
 3. The oracle (FP64 numpy, every host core for its FFTs) continues from there
    and the adaptive decisions of both, attempt by attempt, are compared, with
    the residual each attempt computed.
@@ -50,7 +51,10 @@ def _gpu_run(cfg, state, tables, precision, n_steps, chunk=500):
     while cell.state().istep < n_steps:
         status = cell.run(min(chunk, n_steps - cell.state().istep))
         recs, r = cell.drain()
-        decisions += [(int(x.istep), kinds[x.kind], float(x.res_total)) for x in recs if x.kind in kinds]
+        decisions += [(int(x.istep), kinds[x.kind], float(x.res_total),
+                       {"energy_derivative": x.res_energy_derivative, "diffusion": x.res_diffusion,
+                        "allen_cahn": x.res_allen_cahn, "temperature": x.res_temperature, "dtime_s": x.dtime_s})
+                      for x in recs if x.kind in kinds]
         rows.append(r)
         if status != 0:
             break
@@ -84,11 +88,13 @@ def main(argv=None):
                    "T_at_end_K": float(rows64[-1, L.H["T"]]),
                    "X_al_mean_at_end": float(rows64[-1, L.H["X_al_mean"]]), "wall_s": time.time() - t0,
                    "decisions": len(dec64), "rejections": sum(d[1] == "rejected" for d in dec64),
-                   "last_decisions": dec64[-6:]}
+                   "first_decisions": dec64[:3], "last_decisions": dec64[-3:]}
     print("fp64", rec["fp64"], flush=True)
 
     if stop is not None:
-        start = max(stop - args.back, (int(s.good_step) + 2) if s.flag else 0, 1)
+        # before the scheme arms (flag is set at the end of step good_step), so that the
+        # oracle arms by itself; the state then carries no residual pair
+        start = max(min(stop - args.back, int(s.good_step) if s.flag else stop - args.back), 1)
         cell, st, _, rows = _gpu_run(cfg, state, tables, "fp64", start)
         assert st == 0 and cell.state().istep == start
         resume, fields = gpu_loop_state(cell, rows)

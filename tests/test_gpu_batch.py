@@ -44,21 +44,21 @@ def _members(relaxed):
     return out
 
 
-def _cell(cfg, state):
+def _cell(cfg, state, precision="mixed"):
     from pf_kks_gpu import solver
     from pf_kks_gpu.materials import MaterialTables
 
     tables = MaterialTables.from_npz(cfg.material_tables, cfg.c_gamma, cfg.c_eps0)
-    c = solver.Cell(cfg, tables, precision="mixed")
+    c = solver.Cell(cfg, tables, precision=precision)
     c.upload(*copy_state(state))
     return c
 
 
-def _alone(members, plan):
+def _alone(members, plan, precision="mixed"):
     """Each cell run alone through kks_run, in the given segments."""
     out = []
     for (cfg, state), segs in zip(members, plan):
-        c = _cell(cfg, state)
+        c = _cell(cfg, state, precision)
         recs, rows, st = [], [], 0
         for n in segs:
             st = c.run(n)
@@ -113,18 +113,18 @@ def _batched(members, plan, single=None, groups=1):
     return out
 
 
-def _assert_fields_close(got, ref, what):
+def _assert_fields_close(got, ref, what, tol=1e-6):
     for name, a, e in zip(("eta", "X", "X_al", "X_th"), got, ref):
-        tol = 1e-6 if name in ("eta", "X") else 1e-5
-        assert rel_l2(a, e) <= tol, f"{what}: {name}"
+        t = tol if name in ("eta", "X") else 10 * tol
+        assert rel_l2(a, e) <= t, f"{what}: {name}"
 
 
-def _assert_same(got, ref):
+def _assert_same(got, ref, field_tol=1e-6):
     """Batch against the cells alone: the mixed path's round-off, same decisions."""
     from pf_kks_gpu import _lib as L
 
     for i, (g, r) in enumerate(zip(got, ref)):
-        _assert_fields_close(g[0], r[0], f"cell {i}")
+        _assert_fields_close(g[0], r[0], f"cell {i}", field_tol)
         assert len(g[1]) == len(r[1]), f"cell {i}: number of log records"
         for x, y in zip(g[1], r[1]):
             a, b = L.KksRecord.from_buffer_copy(x), L.KksRecord.from_buffer_copy(y)
@@ -257,4 +257,14 @@ def test_batch_with_a_prime_stage(shapes):
     plan = [[4]] * len(members)
     ref = _alone(members, plan)
     got = _batched(members, plan, groups=2)
-    _assert_same(got, ref)
+    # Each path is held to the mixed step's bar against the FP64 step; the two
+    # FP32 paths (separately compiled batched and single-cell kernels) then
+    # differ by at most the sum of their errors. From these sharp generated
+    # states the first steps' increments are large: at 1420^2 the two differ
+    # by ~1.5e-6 after 4 steps while each stays within 1e-6 of FP64.
+    f64 = _alone(members, plan, precision="fp64")
+    for i, (g, r, e) in enumerate(zip(got, ref, f64)):
+        for k, name in enumerate(("eta", "X")):
+            assert rel_l2(g[0][k], e[0][k]) <= 1e-6, f"cell {i} batch vs fp64: {name}"
+            assert rel_l2(r[0][k], e[0][k]) <= 1e-6, f"cell {i} alone vs fp64: {name}"
+    _assert_same(got, ref, field_tol=2e-6)
