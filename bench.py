@@ -364,12 +364,13 @@ def init_leg(precision, device):
 
 
 def adjoint_leg(device, steps=300, checkpoint_every=50):
-    """adjoint256: the gradient workload. 300 fixed-dt FP64 steps at 256^2
-    through the coefficient chain and kks_adj_forward, the simulated DSC of the
-    run, the loss against the DSC of the target run (Si mobility x 1.2,
-    vacancy annealing rate x 0.8, interface energy x 1.1), and its gradient
-    with respect to the log of the three factors through the hand-written
-    adjoint (checkpoint every 50 steps, segments recomputed)."""
+    """adjoint256: the gradient workload. 300 fixed-dt steps at 256^2 through
+    the coefficient chain and kks_adj_forward, the simulated DSC of the run,
+    the loss against the DSC of the target run (Si mobility x 1.2, vacancy
+    annealing rate x 0.8, interface energy x 1.1), and its gradient with
+    respect to the log of the three factors through the hand-written adjoint
+    (checkpoint every 50 steps, segments recomputed); FP64 and mixed
+    precision (FP32 transforms of the increments)."""
     import torch
 
     from pf_kks_gpu import adjoint as A
@@ -379,30 +380,34 @@ def adjoint_leg(device, steps=300, checkpoint_every=50):
     cfg, spec = workloads.adjoint256(n_steps=steps)
     tables = MaterialTables.from_npz(cfg.material_tables, cfg.c_gamma, cfg.c_eps0)
     state = workloads.initial_state(cfg, spec)
-    stepper = A.StepAdjoint.for_config(cfg, tables, device=device)
     s0 = A.initial_state_tensor(*state, device=device)
     target = torch.tensor(np.log(workloads.ADJOINT_TARGET_FACTORS), dtype=torch.float64)
-    with torch.no_grad():
-        q_target = A.dsc_of_run(cfg, tables, s0, stepper, steps, target, checkpoint_every).total
-    theta = torch.zeros(3, dtype=torch.float64, requires_grad=True)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    q = A.dsc_of_run(cfg, tables, s0, stepper, steps, theta, checkpoint_every).total
-    loss = ((q - q_target) ** 2).sum()
-    torch.cuda.synchronize()
-    t1 = time.perf_counter()
-    loss.backward()
-    torch.cuda.synchronize()
-    t2 = time.perf_counter()
-    stepper.close()
-    g = theta.grad.tolist()
-    return {"workload": "adjoint256: 256^2, 8 cells, 500->520 K, 300 fixed-dt steps, FP64; loss = squared error of "
-                        "the simulated DSC against the run with Si mobility x1.2, annealing rate x0.8, "
-                        "interface energy x1.1", "steps": steps,
-            "checkpoint_every": checkpoint_every, "loss": float(loss), "forward_s": t1 - t0, "backward_s": t2 - t1,
-            "forward_steps_per_s": steps / (t1 - t0), "gradient_steps_per_s": steps / (t2 - t1),
-            "grad_log_c_D": g[0], "grad_log_anneal_rate": g[1], "grad_log_c_gamma": g[2],
-            "timing": "host wall clock, coefficient chain, histories and DSC included"}
+    out = {"workload": "adjoint256: 256^2, 8 cells, 500->520 K, 300 fixed-dt steps; loss = squared error of the "
+                       "simulated DSC against the run with Si mobility x1.2, annealing rate x0.8, interface "
+                       "energy x1.1", "steps": steps, "checkpoint_every": checkpoint_every,
+           "timing": "host wall clock, coefficient chain, histories and DSC included"}
+    q_target = None
+    for precision in ("fp64", "mixed"):
+        stepper = A.StepAdjoint.for_config(cfg, tables, device=device, precision=precision)
+        if q_target is None:
+            with torch.no_grad():
+                q_target = A.dsc_of_run(cfg, tables, s0, stepper, steps, target, checkpoint_every).total
+        theta = torch.zeros(3, dtype=torch.float64, requires_grad=True)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        q = A.dsc_of_run(cfg, tables, s0, stepper, steps, theta, checkpoint_every).total
+        loss = ((q - q_target) ** 2).sum()
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        loss.backward()
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        stepper.close()
+        g = theta.grad.tolist()
+        out[precision] = {"loss": float(loss), "forward_s": t1 - t0, "backward_s": t2 - t1,
+                          "forward_steps_per_s": steps / (t1 - t0), "gradient_steps_per_s": steps / (t2 - t1),
+                          "grad_log_c_D": g[0], "grad_log_anneal_rate": g[1], "grad_log_c_gamma": g[2]}
+    return out
 
 
 def main():

@@ -20,6 +20,16 @@
 // even in k, so the operators IFT m(k) FT are self-adjoint and i k_a is
 // anti-self-adjoint; the pointwise parts are differentiated by hand. The
 // phase-composition guards (+/-inf, NaN) are treated as inactive.
+//
+// Mixed precision (kks_adj_set_precision): every transform runs in FP32 (the
+// real input rounded to float, cuFFT R2C / C2R in single precision, the
+// output widened back), everything else stays FP64, and, as in the main mixed
+// step, the semi-implicit updates carry only the increments through the FP32
+// transforms: eta_b = eta + IFT[(-dt L_s FT drive - dt L_s kappa^2 k^2 FT eta)
+// / (1 + dt L_s kappa^2 k^2)] and X_b = X + IFT[(dt D_s S^ - dt D_s k^2 FT X) /
+// (1 + dt D_s k^2)], so that the FP32 rounding scales with the step's change,
+// not with the fields. The backward pass writes the adjoint operators the same
+// way: A[l] = l + IFT[(A(k) - 1) FT l].
 
 #include <cuda_runtime.h>
 #include <cufft.h>
@@ -65,7 +75,7 @@ __device__ double otr(double kx, double ky, double c11, double c12) {
 }
 
 // multiplier kinds applied to a half spectrum (all include the 1/N of the inverse)
-enum { M_TR = 0, M_DX, M_DY, M_AETA, M_AX, M_LAP };
+enum { M_TR = 0, M_DX, M_DY, M_AETA, M_AX, M_LAP, M_AETA_INC, M_AX_INC };
 
 // in and out may be the same array (an in-place multiply)
 __global__ void k_spec_mul(const double2* in, double2* out, Spec s, const double* kx, const double* ky, int kind,
@@ -81,14 +91,17 @@ __global__ void k_spec_mul(const double2* in, double2* out, Spec s, const double
       case M_DY: r = cmi(v, b * p0 * s.invN); break;
       case M_AETA: r = cm(v, s.invN / (1.0 + p0 * p1 * k2)); break;          // p0 = dt L_s, p1 = kappa^2
       case M_AX: r = cm(v, s.invN / (1.0 + p0 * k2)); break;                  // p0 = dt D_s
+      case M_AETA_INC: r = cm(v, -p0 * p1 * k2 / (1.0 + p0 * p1 * k2) * s.invN); break;  // M_AETA - 1
+      case M_AX_INC: r = cm(v, -p0 * k2 / (1.0 + p0 * k2) * s.invN); break;              // M_AX - 1
       default: r = cm(v, -k2 * s.invN); break;                                // Laplacian
     }
     out[i] = r;
   }
 }
 
-// eta_b^ and X_b^ (not normalised) from FT eta, FT drive, FT X, FT flux_x, FT flux_y;
-// with lap = 1 the outputs are instead IFT-ready -k^2 eta_b^ / N and (S^ - k^2 X_b^) / N.
+// eta_b^ and X_b^ / N from FT eta, FT drive, FT X, FT flux_x, FT flux_y; with
+// lap = 1 the outputs are instead IFT-ready -k^2 eta_b^ / N and (S^ - k^2 X_b^) / N,
+// with lap = 2 the increments (eta_b^ - eta^) / N and (X_b^ - X^) / N.
 __global__ void k_spec_update(const double2* __restrict__ e, const double2* __restrict__ d,
                               const double2* __restrict__ x, const double2* __restrict__ fx,
                               const double2* __restrict__ fy, double2* __restrict__ eb, double2* __restrict__ xb,
@@ -103,7 +116,10 @@ __global__ void k_spec_update(const double2* __restrict__ e, const double2* __re
     const double de = 1.0 + p * c.kappa2 * k2, dx = 1.0 + q * k2;
     const double2 Eb = make_double2((E.x - p * D.x) / de, (E.y - p * D.y) / de);
     const double2 Xb = make_double2((X.x + q * S.x) / dx, (X.y + q * S.y) / dx);
-    if (!lap) {
+    if (lap == 2) {  // increments
+      eb[i] = make_double2((Eb.x - E.x) * s.invN, (Eb.y - E.y) * s.invN);
+      xb[i] = make_double2((Xb.x - X.x) * s.invN, (Xb.y - X.y) * s.invN);
+    } else if (!lap) {
       eb[i] = cm(Eb, s.invN);
       xb[i] = cm(Xb, s.invN);
     } else {
@@ -111,6 +127,17 @@ __global__ void k_spec_update(const double2* __restrict__ e, const double2* __re
       xb[i] = make_double2((S.x - k2 * Xb.x) * s.invN, (S.y - k2 * Xb.y) * s.invN);
     }
   }
+}
+
+__global__ void k_narrow(const double* __restrict__ in, float* __restrict__ out, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = (float)in[i];
+}
+__global__ void k_widen(const float* __restrict__ in, double* __restrict__ out, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = (double)in[i];
+}
+// out = a + b (FP64 state plus an increment); out may be b
+__global__ void k_add(const double* a, const double* b, double* out, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = a[i] + b[i];
 }
 
 __global__ void k_square(const double* __restrict__ e, double* __restrict__ sq, int N) {
@@ -294,9 +321,13 @@ void wave_numbers(int n, std::vector<double>& out, int count) {
 
 struct kks_adj {
   int device = 0;
+  int mixed = 0;  // 1: FP32 transforms (kks_adj_set_precision)
   Spec s{};
   cudaStream_t stream = nullptr;
   cufftHandle r2c = 0, c2r = 0;
+  cufftHandle r2c32 = 0, c2r32 = 0;
+  float* fbuf = nullptr;   // FP32 real transform buffer (N)
+  float* zbuf = nullptr;   // FP32 half-spectrum buffer (2 NC)
   double *kx = nullptr, *ky = nullptr;
   double* f = nullptr;      // real work fields
   double2* z = nullptr;     // half-spectrum work
@@ -332,6 +363,38 @@ Coef coef_of(const double* c) {
 double* fld(kks_adj* h, int k) { return h->f + (size_t)k * h->s.N; }
 double2* spc(kks_adj* h, int k) { return h->z + (size_t)k * h->s.NC; }
 
+// Forward / inverse real transforms of the step: FP64 cuFFT, or in mixed
+// precision FP32 cuFFT on the rounded input with the output widened back.
+int r2c(kks_adj* h, const double* in, double2* out) {
+  if (!h->mixed) {
+    AFK(cufftExecD2Z(h->r2c, (double*)in, (cufftDoubleComplex*)out));
+    return KKS_OK;
+  }
+  const Spec& s = h->s;
+  k_narrow<<<kBlocks, kT, 0, h->stream>>>(in, h->fbuf, s.N);
+  AFK(cufftExecR2C(h->r2c32, h->fbuf, (cufftComplex*)h->zbuf));
+  k_widen<<<kBlocks, kT, 0, h->stream>>>(h->zbuf, (double*)out, 2 * s.NC);
+  return KKS_OK;
+}
+
+int c2r(kks_adj* h, double2* in, double* out) {
+  if (!h->mixed) {
+    AFK(cufftExecZ2D(h->c2r, (cufftDoubleComplex*)in, out));
+    return KKS_OK;
+  }
+  const Spec& s = h->s;
+  k_narrow<<<kBlocks, kT, 0, h->stream>>>((const double*)in, h->zbuf, 2 * s.NC);
+  AFK(cufftExecC2R(h->c2r32, (cufftComplex*)h->zbuf, h->fbuf));
+  k_widen<<<kBlocks, kT, 0, h->stream>>>(h->fbuf, out, s.N);
+  return KKS_OK;
+}
+
+#define XF(expr)                        \
+  do {                                  \
+    const int _rc = (expr);             \
+    if (_rc != KKS_OK) return _rc;      \
+  } while (0)
+
 // Shared front part of the forward and the backward pass: drive, fluxes and
 // the spectra of eta, drive, X, flux_x, flux_y.
 //   fields: 0 eta^2 / tr, 1 gx, 2 gy, 3 drive, 4 fx, 5 fy
@@ -344,20 +407,20 @@ int front(kks_adj* h, const double* in, const Coef& c) {
   const double* ca = in + 2 * (size_t)s.N;
   const double* ct = in + 3 * (size_t)s.N;
   k_square<<<kBlocks, kT, 0, st>>>(e, fld(h, 0), s.N);
-  AFK(cufftExecD2Z(h->r2c, fld(h, 0), (cufftDoubleComplex*)spc(h, 5)));
+  XF(r2c(h, fld(h, 0), spc(h, 5)));
   k_spec_mul<<<kBlocks, kT, 0, st>>>(spc(h, 5), spc(h, 5), s, h->kx, h->ky, M_TR, c.epsX * s.c3n, 0.0);
-  AFK(cufftExecZ2D(h->c2r, (cufftDoubleComplex*)spc(h, 5), fld(h, 0)));  // tr eps
-  AFK(cufftExecD2Z(h->r2c, (double*)e, (cufftDoubleComplex*)spc(h, 0)));
+  XF(c2r(h, spc(h, 5), fld(h, 0)));  // tr eps
+  XF(r2c(h, e, spc(h, 0)));
   k_spec_mul<<<kBlocks, kT, 0, st>>>(spc(h, 0), spc(h, 5), s, h->kx, h->ky, M_DX, 1.0, 0.0);
-  AFK(cufftExecZ2D(h->c2r, (cufftDoubleComplex*)spc(h, 5), fld(h, 1)));
+  XF(c2r(h, spc(h, 5), fld(h, 1)));
   k_spec_mul<<<kBlocks, kT, 0, st>>>(spc(h, 0), spc(h, 5), s, h->kx, h->ky, M_DY, 1.0, 0.0);
-  AFK(cufftExecZ2D(h->c2r, (cufftDoubleComplex*)spc(h, 5), fld(h, 2)));
+  XF(c2r(h, spc(h, 5), fld(h, 2)));
   k_fwd_pointwise<<<kBlocks, kT, 0, st>>>(e, ca, ct, fld(h, 0), fld(h, 1), fld(h, 2), fld(h, 3), fld(h, 4), fld(h, 5),
                                           s, c);
-  AFK(cufftExecD2Z(h->r2c, fld(h, 3), (cufftDoubleComplex*)spc(h, 1)));
-  AFK(cufftExecD2Z(h->r2c, (double*)X, (cufftDoubleComplex*)spc(h, 2)));
-  AFK(cufftExecD2Z(h->r2c, fld(h, 4), (cufftDoubleComplex*)spc(h, 3)));
-  AFK(cufftExecD2Z(h->r2c, fld(h, 5), (cufftDoubleComplex*)spc(h, 4)));
+  XF(r2c(h, fld(h, 3), spc(h, 1)));
+  XF(r2c(h, X, spc(h, 2)));
+  XF(r2c(h, fld(h, 4), spc(h, 3)));
+  XF(r2c(h, fld(h, 5), spc(h, 4)));
   ACK(cudaGetLastError());
   return KKS_OK;
 }
@@ -413,11 +476,18 @@ int kks_adj_forward(kks_adj* h, const double* state_in, const double* coef, doub
   int rc = front(h, state_in, c);
   if (rc != KKS_OK) return rc;
   k_spec_update<<<kBlocks, kT, 0, st>>>(spc(h, 0), spc(h, 1), spc(h, 2), spc(h, 3), spc(h, 4), spc(h, 6), spc(h, 7),
-                                        s, h->kx, h->ky, c, 0);
+                                        s, h->kx, h->ky, c, h->mixed ? 2 : 0);
   double* eb = state_out;
   double* xb = state_out + s.N;
-  AFK(cufftExecZ2D(h->c2r, (cufftDoubleComplex*)spc(h, 6), eb));
-  AFK(cufftExecZ2D(h->c2r, (cufftDoubleComplex*)spc(h, 7), xb));
+  if (h->mixed) {  // FP32 transforms of the increments, added to the FP64 state
+    XF(c2r(h, spc(h, 6), fld(h, 6)));
+    XF(c2r(h, spc(h, 7), fld(h, 7)));
+    k_add<<<kBlocks, kT, 0, st>>>(state_in, fld(h, 6), eb, s.N);
+    k_add<<<kBlocks, kT, 0, st>>>(state_in + s.N, fld(h, 7), xb, s.N);
+  } else {
+    XF(c2r(h, spc(h, 6), eb));
+    XF(c2r(h, spc(h, 7), xb));
+  }
   k_phase<<<kBlocks, kT, 0, st>>>(state_in + s.N, eb, state_out + 2 * (size_t)s.N, state_out + 3 * (size_t)s.N, s.N, c);
   ACK(cudaGetLastError());
   ACK(cudaStreamSynchronize(st));
@@ -438,24 +508,28 @@ int kks_adj_backward(kks_adj* h, const double* state_in, const double* state_out
   // laplacian of eta_b and S + laplacian X_b from the same spectra
   k_spec_update<<<kBlocks, kT, 0, st>>>(spc(h, 0), spc(h, 1), spc(h, 2), spc(h, 3), spc(h, 4), spc(h, 6), spc(h, 7),
                                         s, h->kx, h->ky, c, 1);
-  AFK(cufftExecZ2D(h->c2r, (cufftDoubleComplex*)spc(h, 6), fld(h, 6)));   // lap eta_b
-  AFK(cufftExecZ2D(h->c2r, (cufftDoubleComplex*)spc(h, 7), fld(h, 7)));   // S + lap X_b
+  XF(c2r(h, spc(h, 6), fld(h, 6)));   // lap eta_b
+  XF(c2r(h, spc(h, 7), fld(h, 7)));   // S + lap X_b
   // phase compositions
   k_back_phase<<<kBlocks, kT, 0, st>>>(state_in + N, state_out, state_out + 2 * N, lam_out, lam_out + 2 * N,
                                        lam_out + 3 * N, fld(h, 8), fld(h, 9), s.N, c, h->partials);
   // mu_eta = A_eta[lambda eta_b], mu_X = A_X[lambda X_b]
-  AFK(cufftExecD2Z(h->r2c, fld(h, 8), (cufftDoubleComplex*)spc(h, 5)));
-  k_spec_mul<<<kBlocks, kT, 0, st>>>(spc(h, 5), spc(h, 5), s, h->kx, h->ky, M_AETA, c.dt * c.Ls, c.kappa2);
-  AFK(cufftExecZ2D(h->c2r, (cufftDoubleComplex*)spc(h, 5), fld(h, 10)));  // mu_eta
-  AFK(cufftExecD2Z(h->r2c, (double*)(lam_out + N), (cufftDoubleComplex*)spc(h, 5)));
-  k_spec_mul<<<kBlocks, kT, 0, st>>>(spc(h, 5), spc(h, 5), s, h->kx, h->ky, M_AX, c.dt * c.Ds, 0.0);
-  AFK(cufftExecZ2D(h->c2r, (cufftDoubleComplex*)spc(h, 5), fld(h, 11)));  // mu_X
+  XF(r2c(h, fld(h, 8), spc(h, 5)));
+  k_spec_mul<<<kBlocks, kT, 0, st>>>(spc(h, 5), spc(h, 5), s, h->kx, h->ky, h->mixed ? M_AETA_INC : M_AETA,
+                                     c.dt * c.Ls, c.kappa2);
+  XF(c2r(h, spc(h, 5), fld(h, 10)));  // mu_eta (mixed: its increment over the cotangent)
+  if (h->mixed) k_add<<<kBlocks, kT, 0, st>>>(fld(h, 8), fld(h, 10), fld(h, 10), s.N);
+  XF(r2c(h, (lam_out + N), spc(h, 5)));
+  k_spec_mul<<<kBlocks, kT, 0, st>>>(spc(h, 5), spc(h, 5), s, h->kx, h->ky, h->mixed ? M_AX_INC : M_AX,
+                                     c.dt * c.Ds, 0.0);
+  XF(c2r(h, spc(h, 5), fld(h, 11)));  // mu_X (mixed: its increment over the cotangent)
+  if (h->mixed) k_add<<<kBlocks, kT, 0, st>>>(lam_out + N, fld(h, 11), fld(h, 11), s.N);
   // lambda flux_a = -dt D_s d_a mu_X
-  AFK(cufftExecD2Z(h->r2c, fld(h, 11), (cufftDoubleComplex*)spc(h, 5)));
+  XF(r2c(h, fld(h, 11), spc(h, 5)));
   k_spec_mul<<<kBlocks, kT, 0, st>>>(spc(h, 5), spc(h, 6), s, h->kx, h->ky, M_DX, -c.dt * c.Ds, 0.0);
-  AFK(cufftExecZ2D(h->c2r, (cufftDoubleComplex*)spc(h, 6), fld(h, 12)));
+  XF(c2r(h, spc(h, 6), fld(h, 12)));
   k_spec_mul<<<kBlocks, kT, 0, st>>>(spc(h, 5), spc(h, 6), s, h->kx, h->ky, M_DY, -c.dt * c.Ds, 0.0);
-  AFK(cufftExecZ2D(h->c2r, (cufftDoubleComplex*)spc(h, 6), fld(h, 13)));
+  XF(c2r(h, spc(h, 6), fld(h, 13)));
   // main pointwise back pass
   double* lam_e = lam_in;
   double* lam_x = lam_in + N;
@@ -464,13 +538,13 @@ int kks_adj_backward(kks_adj* h, const double* state_in, const double* state_out
                                       fld(h, 14), fld(h, 15), fld(h, 16), fld(h, 17), lam_in + 2 * N, lam_in + 3 * N, s,
                                       c, h->partials);
   // lambda of eta^2 = epsX c3n T[lambda tr]; divergence of lambda g
-  AFK(cufftExecD2Z(h->r2c, fld(h, 14), (cufftDoubleComplex*)spc(h, 5)));
+  XF(r2c(h, fld(h, 14), spc(h, 5)));
   k_spec_mul<<<kBlocks, kT, 0, st>>>(spc(h, 5), spc(h, 5), s, h->kx, h->ky, M_TR, c.epsX * s.c3n, 0.0);
-  AFK(cufftExecZ2D(h->c2r, (cufftDoubleComplex*)spc(h, 5), fld(h, 18)));
-  AFK(cufftExecD2Z(h->r2c, fld(h, 15), (cufftDoubleComplex*)spc(h, 5)));
-  AFK(cufftExecD2Z(h->r2c, fld(h, 16), (cufftDoubleComplex*)spc(h, 6)));
+  XF(c2r(h, spc(h, 5), fld(h, 18)));
+  XF(r2c(h, fld(h, 15), spc(h, 5)));
+  XF(r2c(h, fld(h, 16), spc(h, 6)));
   k_spec_div<<<kBlocks, kT, 0, st>>>(spc(h, 5), spc(h, 6), spc(h, 7), s, h->kx, h->ky);
-  AFK(cufftExecZ2D(h->c2r, (cufftDoubleComplex*)spc(h, 7), fld(h, 19)));
+  XF(c2r(h, spc(h, 7), fld(h, 19)));
   k_back_final<<<kBlocks, kT, 0, st>>>(state_in, fld(h, 17), fld(h, 18), fld(h, 19), fld(h, 11), fld(h, 9), lam_e,
                                        lam_x, s.N);
   k_finish<<<1, 32, 0, st>>>(h->partials, kBlocks, h->sums);
@@ -497,11 +571,36 @@ int kks_adj_backward(kks_adj* h, const double* state_in, const double* state_out
   return KKS_OK;
 }
 
+int kks_adj_set_precision(kks_adj* h, int precision) {
+  if (!h || (precision != KKS_PRECISION_FP64 && precision != KKS_PRECISION_MIXED))
+    return kks_set_error(KKS_ERR_ARG, "precision must be KKS_PRECISION_FP64 or KKS_PRECISION_MIXED");
+  ACK(cudaSetDevice(h->device));
+  ACK(cudaStreamSynchronize(h->stream));
+  if (precision == KKS_PRECISION_MIXED && !h->r2c32) {
+    const Spec& s = h->s;
+    ACK(cudaMalloc(&h->fbuf, (size_t)s.N * sizeof(float)));
+    ACK(cudaMalloc(&h->zbuf, (size_t)2 * s.NC * sizeof(float)));
+    cufftHandle a = 0, b = 0;
+    if (cufftPlan2d(&a, s.nx, s.ny, CUFFT_R2C) != CUFFT_SUCCESS) return kks_set_error(KKS_ERR_CUFFT, "FP32 plans");
+    h->r2c32 = a;
+    if (cufftPlan2d(&b, s.nx, s.ny, CUFFT_C2R) != CUFFT_SUCCESS) return kks_set_error(KKS_ERR_CUFFT, "FP32 plans");
+    h->c2r32 = b;
+    AFK(cufftSetStream(h->r2c32, h->stream));
+    AFK(cufftSetStream(h->c2r32, h->stream));
+  }
+  h->mixed = precision == KKS_PRECISION_MIXED;
+  return KKS_OK;
+}
+
 int kks_adj_destroy(kks_adj* h) {
   if (!h) return KKS_OK;
   cudaSetDevice(h->device);
   if (h->r2c) cufftDestroy(h->r2c);
   if (h->c2r) cufftDestroy(h->c2r);
+  if (h->r2c32) cufftDestroy(h->r2c32);
+  if (h->c2r32) cufftDestroy(h->c2r32);
+  cudaFree(h->fbuf);
+  cudaFree(h->zbuf);
   cudaFree(h->kx);
   cudaFree(h->ky);
   cudaFree(h->f);

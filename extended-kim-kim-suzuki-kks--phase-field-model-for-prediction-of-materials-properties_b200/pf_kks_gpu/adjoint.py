@@ -160,7 +160,7 @@ class StepAdjoint:
     Tensors are float64 CUDA tensors of shape (4, nx, ny) (eta, X, X_al,
     X_th); coefficient rows are 15 float64 values."""
 
-    def __init__(self, nx, ny, C11_0, C12_0, C44_0, device=0, surf_scale=1.0):
+    def __init__(self, nx, ny, C11_0, C12_0, C44_0, device=0, surf_scale=1.0, precision="fp64"):
         self.lib = L.load()
         self.nx, self.ny, self.device = int(nx), int(ny), int(device)
         self.surf_scale = float(surf_scale)  # dx^2 / (2 lambda): interface cells -> interface measure
@@ -168,13 +168,18 @@ class StepAdjoint:
         L.check(self.lib.kks_adj_create(self.nx, self.ny, float(C11_0), float(C12_0), float(C44_0), self.device,
                                         ctypes.byref(h)), "kks_adj_create")
         self.h = h
+        self.precision = precision
+        if precision != "fp64":
+            code = {"mixed": L.KKS_PRECISION_MIXED}[precision]
+            L.check(self.lib.kks_adj_set_precision(self.h, code), "kks_adj_set_precision")
 
     @classmethod
-    def for_config(cls, cfg, tables, device=0):
-        """Stiffness frozen at T(t = 0) (pf_kks/solver.py:152-154)."""
+    def for_config(cls, cfg, tables, device=0, precision="fp64"):
+        """Stiffness frozen at T(t = 0) (pf_kks/solver.py:152-154). ``precision``:
+        "fp64" or "mixed" (FP32 transforms of the increments, FP64 elsewhere)."""
         T0 = float(np.interp(0.0, np.asarray(cfg.schedule_time, float), np.asarray(cfg.schedule_temperature, float)))
         return cls(cfg.nx, cfg.ny, tables.at(T0, "C11"), tables.at(T0, "C12"), tables.at(T0, "C44"), device,
-                   surf_scale=cfg.dx**2 / (2 * cfg.lambd))
+                   surf_scale=cfg.dx**2 / (2 * cfg.lambd), precision=precision)
 
     def _check(self, *tensors):
         torch = _torch()

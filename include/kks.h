@@ -295,6 +295,13 @@ int kks_adj_forward(kks_adj* h, const double* state_in, const double* coef, doub
  * with respect to coef (host array). */
 int kks_adj_backward(kks_adj* h, const double* state_in, const double* state_out, const double* coef,
                      const double* lam_out, double* lam_in, double* dcoef);
+/* Precision of the handle's step and adjoint: KKS_PRECISION_FP64 (default)
+ * or KKS_PRECISION_MIXED: every transform in FP32 (cuFFT R2C / C2R on the
+ * rounded input, output widened back), all pointwise work, the state and the
+ * sums in FP64, and the semi-implicit updates (and their adjoints) carrying
+ * only the increments through the FP32 transforms, as the main mixed step
+ * does. */
+int kks_adj_set_precision(kks_adj* h, int precision);
 int kks_adj_destroy(kks_adj* h);
 
 /* Initial state written on the device. No nx*ny host array crosses the ABI:

@@ -27,6 +27,35 @@ def _setup(nx=48, ny=40, n=6):
     return A, cfg, tables, state, stepper, tstep, s0
 
 
+def test_mixed_forward_step_is_the_increment_form():
+    """The mixed step (FP32 transforms of the increments) within 1e-6 of the
+    FP64 step on eta and X after 6 steps, and its vector-Jacobian product
+    within 1e-4 (relative L2) of the FP64 one."""
+    A, cfg, tables, state, stepper, tstep, s0 = _setup()
+    mixed = A.StepAdjoint.for_config(cfg, tables, device=0, precision="mixed")
+    coef = A.coefficients(cfg, tables, 6).numpy()
+    a, b = s0.clone(), s0.clone()
+    for i in range(6):
+        na, nb = torch.empty_like(a), torch.empty_like(b)
+        stepper.forward(a, coef[i], na)
+        mixed.forward(b, coef[i], nb)
+        a, b = na, nb
+    for k in range(2):
+        assert rel_l2(b[k].cpu().numpy(), a[k].cpu().numpy()) <= 1e-6, k
+    gen = torch.Generator(device="cuda").manual_seed(3)
+    lam = torch.randn(s0.shape, generator=gen, dtype=torch.float64, device="cuda").contiguous()
+    outs = []
+    for st in (stepper, mixed):
+        out, lin = torch.empty_like(s0), torch.empty_like(s0)
+        st.forward(s0, coef[0], out)
+        d = st.backward(s0, out, coef[0], lam, lin)
+        outs.append((lin, d))
+    for k in range(4):
+        assert rel_l2(outs[1][0][k].cpu().numpy(), outs[0][0][k].cpu().numpy()) <= 1e-4, k
+    assert rel_l2(outs[1][1], outs[0][1]) <= 1e-4
+    mixed.close()
+
+
 def test_forward_step_matches_torch_step():
     A, cfg, tables, state, stepper, tstep, s0 = _setup()
     coef = A.coefficients(cfg, tables, 1)[0]
@@ -189,6 +218,28 @@ def test_dsc_gradient_of_the_three_kinetic_parameters():
     g2 = theta2.grad.numpy()
     assert np.all(np.abs(g - g2) <= 1e-8 * np.max(np.abs(g2))), (g, g2)
     stepper.close()
+
+    # mixed precision: FP32 transforms of the increments, FP64 elsewhere, same
+    # target; its DSC within 1e-6 (relative L2) of the FP64 one and its gradient
+    # within 1e-3 of the FP64 gradient (relative to the gradient's norm)
+    mixed = A.StepAdjoint.for_config(cfg, tables, device=0, precision="mixed")
+    with torch.no_grad():
+        q64 = A.dsc_of_run(cfg, tables, s0, stepper_fp64(cfg, tables), n, torch.zeros(3, dtype=torch.float64),
+                           checkpoint_every=K).total
+        q32 = A.dsc_of_run(cfg, tables, s0, mixed, n, torch.zeros(3, dtype=torch.float64), checkpoint_every=K).total
+    assert rel_l2(q32.cpu().numpy(), q64.cpu().numpy()) <= 1e-6
+    theta3 = torch.zeros(3, dtype=torch.float64, requires_grad=True)
+    qm = A.dsc_of_run(cfg, tables, s0, mixed, n, theta3, checkpoint_every=K).total
+    ((qm - q_target) ** 2).sum().backward()
+    gm = theta3.grad.numpy()
+    assert np.all(np.abs(gm - g) <= 1e-3 * np.max(np.abs(g))), (gm, g)
+    mixed.close()
+
+
+def stepper_fp64(cfg, tables):
+    from pf_kks_gpu import adjoint as A
+
+    return A.StepAdjoint.for_config(cfg, tables, device=0)
 
 
 def test_forward_run_matches_main_fp64_cell():
