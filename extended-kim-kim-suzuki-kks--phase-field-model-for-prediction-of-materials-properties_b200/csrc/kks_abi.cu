@@ -355,6 +355,10 @@ static int setup_fused(kks_handle* h, const std::vector<double>& kx) {
   void* RB = a; a += al(3 * fs);
   void* SA = a; a += al(2 * fs);
   CK(cudaMemset(RA, 0, b_spec));
+  // every kernel of the pipeline writes one partial-sum row per block: the
+  // buffer holds the largest grid of them (row pairs, column tiles, extras)
+  // under any launch shape; the decide kernel reads the rows of the current one
+  fc.part_cap = std::max(kks_fft_partial_rows(c.nx, c.ny, h->nblocks_cap), h->nblocks_cap);
   CK(cudaMalloc(&h->d_fc, sizeof(KksFftConst)));
   CK(cudaMemcpy(h->d_fc, &fc, sizeof(KksFftConst), cudaMemcpyHostToDevice));
   KksFftLaunch& L = h->fl;
@@ -382,10 +386,7 @@ static int setup_fused(kks_handle* h, const std::vector<double>& kx) {
       encode_spectrum_map(&L.map_RB3, RB, c.nx, c.nyh, 3) && encode_spectrum_map(&L.map_RB2, RB, c.nx, c.nyh, 2))
     L.bulk_rows = 1;
   if (kks_fft_set_attributes(L) != 0) return set_error(KKS_ERR_CUDA, "fft kernel attributes");
-  // every kernel of the pipeline writes one partial-sum row per block: the
-  // buffer holds the largest grid of them (row pairs, column tiles, extras)
-  // under any launch shape; the decide kernel reads the rows of the current one
-  h->part_cap_fused = std::max(kks_fft_partial_rows(c.nx, c.ny, h->nblocks_cap), h->nblocks_cap);
+  h->part_cap_fused = fc.part_cap;
   h->nb_fused = fused_rows(h);
   CK(cudaMalloc(&h->partials_fused, (size_t)h->part_cap_fused * KKS_NPART * sizeof(double)));
   CK(cudaMemset(h->partials_fused, 0, (size_t)h->part_cap_fused * KKS_NPART * sizeof(double)));
@@ -1169,6 +1170,17 @@ int kks_download(kks_handle* h, double* eta, double* X, double* X_al, double* X_
   if (X && (rc = get_field(h, X, h->f.X[p], true)) != KKS_OK) return rc;
   if (X_al && (rc = get_field(h, X_al, h->f.X_al[p], d)) != KKS_OK) return rc;
   if (X_th && (rc = get_field(h, X_th, h->f.X_th[p], d)) != KKS_OK) return rc;
+  return KKS_OK;
+}
+
+int kks_bounds_report(int device, int32_t* checked, uint64_t* first) {
+  if (!checked || !first) return set_error(KKS_ERR_ARG, "null argument");
+  CK(cudaSetDevice(device));
+  unsigned long long w = 0;
+  const int rc = kks_fft_bounds_word(&w, 1);
+  if (rc < 0) return set_error(KKS_ERR_CUDA, "reading the bounds-check word");
+  *checked = rc;
+  *first = (uint64_t)w;
   return KKS_OK;
 }
 

@@ -55,8 +55,31 @@
 
 #include "kks_internal.cuh"
 #include "kks_fft.cuh"
+#include "kks_check.cuh"
 
 namespace {
+
+// sites of the bounds-check build (kks_check.cuh): pass * 10 + check
+enum {
+  kSiteRowsA = 10, kSiteColsAB = 20, kSiteRowsBC = 30, kSiteColsCDeta = 40, kSiteColsCDX = 50, kSiteRowsD = 60,
+  kSiteExtras = 70, kSiteFFT = 80
+};
+
+// The rows ix0 and ix0 + 1 (if any) of a row-pass block lie in the grid and its
+// partial-sum row in the buffer.
+__device__ __forceinline__ bool row_block_in_range(const KksConst* c, const KksFftConst* fc, int ix0, int bx, int site) {
+  return KKS_IN((long long)(ix0 + 1 < c->nx ? ix0 + 1 : ix0) * c->ny + c->ny - 1, c->N, site) &&
+         KKS_IN(bx, fc->part_cap, site + 1);
+}
+
+// The columns ky0 .. ky0 + ncol - 1 of a column-pass block lie in the half
+// spectrum, its nseq columns in the launch's dynamic shared memory, and its
+// partial-sum row in the buffer.
+__device__ __forceinline__ bool col_block_in_range(const KksConst* c, const KksFftConst* fc, int ky0, int ncol, int nseq,
+                                                   int bx, int site) {
+  return KKS_IN(ky0 + ncol - 1, c->nyh, site) && KKS_IN((long long)nseq * c->nx * 8 - 1, kks_dyn_smem_bytes(), site + 1) &&
+         KKS_IN(bx, fc->part_cap, site + 2);
+}
 
 constexpr int kThreads = KKS_FFT_THREADS;
 // blocks per SM the register allocation must allow
@@ -452,6 +475,12 @@ __device__ __forceinline__ void fft_run(int nseq, const KksFftAxis& ax) {
   extern __shared__ float2 sm[];
   float2* buf = sm;
   const int n = ax.n;
+  // the sequences must lie in the launch's dynamic shared memory (a uniform
+  // condition: the whole block skips the transform)
+  if (!KKS_IN((long long)nseq * n * 8 - 1, kks_dyn_smem_bytes(), kSiteFFT)) {
+    __syncthreads();
+    return;
+  }
   for (int si = 0; si < ax.nst; ++si) {
     const int s = DIR < 0 ? si : ax.nst - 1 - si;
     const int r = ax.r[s];
@@ -614,6 +643,7 @@ __device__ __forceinline__ void rows_A_body(const KksConst* __restrict__ c, cons
   const int nx = c->nx, ny = c->ny, nyh = c->nyh;
   const int ix0 = 2 * bx;
   const bool has1 = ix0 + 1 < nx;
+  if (!row_block_in_range(c, fc, ix0, bx, kSiteRowsA)) return;
   const size_t i0 = (size_t)ix0 * ny;
   // staging after the three sequences: rows ix0, ix0+1 of eta and X, later
   // the three split half spectra of the pair
@@ -706,6 +736,7 @@ __device__ __forceinline__ void cols_AB_body(const KksConst* __restrict__ c, con
   const int ky0 = bx * cols;
   const int ncol = min(cols, nyh - ky0);
   const int nv = ncol * nx;
+  if (!col_block_in_range(c, fc, ky0, ncol, g == 0 ? 2 * ncol : ncol, bx, kSiteColsAB)) return;
   const int src_field = g == 0 ? 0 : (g == 1 ? 2 : 1);
   const float2* col = RA + src_field * fs + (size_t)ky0 * nx;
   if (bulk) {  // the block's columns are one contiguous run: one bulk copy
@@ -811,6 +842,7 @@ __device__ __forceinline__ void rows_BC_body(const KksConst* __restrict__ c, con
   const size_t fs = (size_t)nx * nyh;
   const int ix0 = 2 * bx;
   const bool has1 = ix0 + 1 < nx;
+  if (!row_block_in_range(c, fc, ix0, bx, kSiteRowsBC)) return;
   const int kb = nyh < 256 ? nyh : 256, nb = (nyh + kb - 1) / kb;
   // staging after the three sequences: the pair's three half spectra (tensor
   // load), then rows ix0, ix0+1 of eta, X_al, X_th (bulk copies, overlapping
@@ -926,6 +958,7 @@ __device__ __forceinline__ void cols_CD_eta_body(const KksConst* __restrict__ c,
   const int ky0 = bx * cols;
   const int ncol = min(cols, nyh - ky0);
   const int nv = ncol * nx;
+  if (!col_block_in_range(c, fc, ky0, ncol, ncol, bx, kSiteColsCDeta)) return;
   const float2* col = RC + (size_t)ky0 * nx;
   // FT(eta) of the same columns, staged during the forward FFT
   float2* s_sa = (float2*)stage_base(sm, (uint32_t)(cols * nx * sizeof(float2)));
@@ -994,6 +1027,7 @@ __device__ __forceinline__ void cols_CD_X_body(const KksConst* __restrict__ c, c
   const int ky0 = bx * cols;
   const int ncol = min(cols, nyh - ky0);
   const int nv = ncol * nx;
+  if (!col_block_in_range(c, fc, ky0, ncol, 2 * ncol, bx, kSiteColsCDX)) return;
   // flux_x columns at [0, nv), flux_y columns at [nv, 2 nv); FT(X) of the same
   // columns staged during the forward FFT
   const float2* cx = RC + fs + (size_t)ky0 * nx;
@@ -1073,6 +1107,7 @@ __device__ __forceinline__ void rows_D_body(const KksConst* __restrict__ c, cons
   const size_t fs = (size_t)nx * nyh;
   const int ix0 = 2 * bx;
   const bool has1 = ix0 + 1 < nx;
+  if (!row_block_in_range(c, fc, ix0, bx, kSiteRowsD)) return;
   // staging after the two sequences: the pair's two half spectra (tensor
   // load), then rows ix0, ix0+1 of the old eta and X (bulk copies,
   // overlapping the inverse FFT)
@@ -1540,6 +1575,21 @@ int kks_fft_set_attributes(const KksFftLaunch& L) {
 #undef KKS_ROWS_ATTR
 #undef KKS_COLS_ATTR
   return rc != 0 ? rc : rc2;
+}
+
+int kks_fft_bounds_word(unsigned long long* first, int reset) {
+  *first = 0;
+#ifdef KKS_BOUNDS_CHECK
+  if (cudaMemcpyFromSymbol(first, g_kks_oob, sizeof(unsigned long long)) != cudaSuccess) return -1;
+  if (reset) {
+    const unsigned long long zero = 0;
+    if (cudaMemcpyToSymbol(g_kks_oob, &zero, sizeof(zero)) != cudaSuccess) return -1;
+  }
+  return 1;
+#else
+  (void)reset;
+  return 0;
+#endif
 }
 
 int kks_fft_prime_table(int P, float2* out) {

@@ -38,6 +38,7 @@ struct KksFftConst {
   int cols;              // y-frequency columns per column-pass block (1..KKS_FFT_COLS_MAX)
   int wait_polls;        // polls of the first wait for a block's bulk / tensor copies (KKS_FFT_WAIT_POLLS;
                          // kks_set_wait_polls changes it for fault-path tests)
+  int part_cap;          // partial-sum rows allocated (the bounds-check build checks each block's row)
 };
 
 #define KKS_FFT_WAIT_POLLS (1 << 20)
@@ -83,6 +84,10 @@ int kks_fft_set_attributes(const KksFftLaunch& L);
 // the count, or 0 for an unsupported P.
 #define KKS_FFT_PRIME_TABLE_MAX (5 * 35 * 8)
 int kks_fft_prime_table(int P, float2* out);
+// The first out-of-range index recorded by the bounds-check build's kernels of
+// kks_fft.cu on the current device (0: none; site << 44 | index), cleared when
+// reset is nonzero. Returns 1 in a bounds-check build, 0 otherwise (*first = 0).
+int kks_fft_bounds_word(unsigned long long* first, int reset);
 void kks_fft_launch_attempt(const KksFftLaunch& L, int parity, cudaStream_t s);
 
 // ---------------------------------------------------------------------------

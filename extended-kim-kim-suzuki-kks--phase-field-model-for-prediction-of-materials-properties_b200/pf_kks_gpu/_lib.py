@@ -10,7 +10,10 @@ import os
 import numpy as np
 
 LIB_NAME = "libkks_b200.so"
-LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), LIB_NAME)
+# $KKS_LIBRARY selects another build of the library (e.g. the bounds-check
+# build libkks_b200_check.so of pf_kks_gpu.build --bounds-check)
+LIB_PATH = os.environ.get("KKS_LIBRARY") or os.path.join(os.path.dirname(os.path.abspath(__file__)), LIB_NAME)
+CHECK_LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libkks_b200_check.so")
 
 KKS_OK = 0
 KKS_STATUS_OK = 0
@@ -55,7 +58,7 @@ EXPORTS = (
     "kks_voronoi_edges", "kks_generate_fields", "kks_place_precipitates", "kks_add_nuclei", "kks_count_below",
     "kks_insert_nuclei", "kks_batch_create", "kks_batch_run", "kks_batch_timing", "kks_batch_destroy",
     "kks_get_launch_shape", "kks_set_launch_shape", "kks_autotune", "kks_download_pair",
-    "kks_set_wait_polls",
+    "kks_set_wait_polls", "kks_bounds_report",
 )
 
 
@@ -150,6 +153,8 @@ def load(path=LIB_PATH):
     lib.kks_download_pair.argtypes = [vp, dp, dp, dp, dp]
     lib.kks_set_wait_polls.argtypes = [vp, ctypes.c_int32]
     lib.kks_set_wait_polls.restype = ctypes.c_int
+    lib.kks_bounds_report.argtypes = [ctypes.c_int, P(ctypes.c_int32), P(ctypes.c_uint64)]
+    lib.kks_bounds_report.restype = ctypes.c_int
     lib.kks_elastic_fields.argtypes = [vp, dp, dp]
     lib.kks_checkpoint.argtypes = [vp, vp, ctypes.c_size_t, P(ctypes.c_size_t)]
     lib.kks_restore.argtypes = [vp, vp, ctypes.c_size_t]
@@ -207,6 +212,15 @@ def check(rc, what):
     if rc != KKS_OK:
         msg = load().kks_last_error().decode(errors="replace")
         raise KksError(f"{what} failed ({rc}): {msg}")
+
+
+def bounds_report(device=0):
+    """(checked, first): whether the loaded library is the bounds-check build,
+    and the first out-of-range block it recorded on ``device`` since the last
+    report (0 = none; site << 44 | index). Clears the record."""
+    checked, first = ctypes.c_int32(0), ctypes.c_uint64(0)
+    check(load().kks_bounds_report(int(device), ctypes.byref(checked), ctypes.byref(first)), "kks_bounds_report")
+    return bool(checked.value), int(first.value)
 
 
 def dptr(a):

@@ -202,6 +202,16 @@ int kks_get_state(kks_handle* h, kks_run_state* state);
 /* Download the current fields (host float64, nx*ny each); any pointer may be NULL. */
 int kks_download(kks_handle* h, double* eta, double* X, double* X_al, double* X_th);
 
+/* Debug aid; no counterpart in the reference. The library built with
+ * -DKKS_BOUNDS_CHECK (libkks_b200_check.so) checks, in the fused passes, the
+ * range each block works on (its rows or columns against the grid, its
+ * partial-sum row against the buffer, its sequences against the launch's
+ * shared memory) and, instead of faulting, records the first failed check and
+ * skips that block's work. *checked = 1 for that build (0 otherwise: nothing
+ * is checked); *first = the first recorded failure on `device` since the last
+ * report (site << 44 | index; 0 = none), which the call clears. */
+int kks_bounds_report(int device, int32_t* checked, uint64_t* first);
+
 /* Fault-path test hook; no counterpart in the reference. The fused passes of
  * the mixed path wait for their bulk and tensor copies on an mbarrier with a
  * bounded number of polls; when a wait runs out, the cell's status becomes
