@@ -234,6 +234,26 @@ __device__ __forceinline__ void bfly_small(float2* base, int q, int j, const flo
   for (int m = 0; m < R; ++m) base[m * q] = x[m];
 }
 
+// The butterfly of a stage with stride q = 1 (the last DIF / first DIT stage
+// when the last radix is 2 or 4): its R values are contiguous and j = 0 (no
+// twiddles), so they move as 16-byte pairs: one shared-memory access per pair
+// instead of two 8-byte ones 16 or 32 bytes apart across the warp's lanes.
+template <int R, int DIR>
+__device__ __forceinline__ void bfly_contig(float2* base) {
+  static_assert(R == 2 || R == 4, "pairs of values");
+  float2 x[R];
+  float4* b4 = reinterpret_cast<float4*>(base);
+#pragma unroll
+  for (int m = 0; m < R / 2; ++m) {
+    const float4 v = b4[m];
+    x[2 * m] = make_float2(v.x, v.y);
+    x[2 * m + 1] = make_float2(v.z, v.w);
+  }
+  dft_small<R, DIR>(x);
+#pragma unroll
+  for (int m = 0; m < R / 2; ++m) b4[m] = make_float4(x[2 * m].x, x[2 * m].y, x[2 * m + 1].x, x[2 * m + 1].y);
+}
+
 // ---------------------------------------------------------------------------
 // Prime stages. The H = (P-1)/2 output pairs (k, P-k) of a DFT are split into
 // NG groups of G; the table of prime P holds (cos, sin)(2 pi ((n k) mod P) / P)
@@ -496,6 +516,19 @@ __device__ __forceinline__ void fft_run(int nseq, const KksFftAxis& ax) {
     const uint32_t qm = ax.qm[s], pm = ax.pm[s];
     const float2* tw = ax.tw + ax.tw_off[s];
     const int total = nseq * per;
+    // stride-1 stages of radix 2 / 4 on 16-byte aligned sequences: paired
+    // loads (n even keeps every sequence and butterfly 16-byte aligned once the
+    // dynamic shared memory is)
+    if (q == 1 && (r == 2 || r == 4) && (n & 1) == 0 && (smem_u32(sm) & 15u) == 0) {
+      for (int t = threadIdx.x; t < total; t += pass_threads<P>()) {
+        const int sq = nseq == 1 ? 0 : fdiv(t, per, pm);
+        float2* base = buf + sq * n + (t - sq * per) * r;
+        if (r == 2) bfly_contig<2, DIR>(base);
+        else bfly_contig<4, DIR>(base);
+      }
+      __syncthreads();
+      continue;
+    }
     for (int t = threadIdx.x; t < total; t += pass_threads<P>()) {
       const int sq = nseq == 1 ? 0 : fdiv(t, per, pm);
       const int bt = t - sq * per;
