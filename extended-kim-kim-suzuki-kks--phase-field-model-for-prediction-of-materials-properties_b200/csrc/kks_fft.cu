@@ -1003,6 +1003,10 @@ __device__ __forceinline__ void cols_CD_eta_body(const KksConst* __restrict__ c,
     }
     __syncthreads();
     bulk_wait(&bar, 0, ctl, fc->wait_polls);
+    // every thread has seen phase 0 complete before the barrier is armed for
+    // phase 1: a thread still polling parity 0 once phase 1 has completed too
+    // would find phase 2 (parity 0) open and wait until its poll limit
+    __syncthreads();
     if (threadIdx.x == 0) {
       mbar_expect_tx(&bar, 8u * nv);
       bulk_g2s(s_sa, SA + (size_t)ky0 * nx, 8u * nv, &bar);
@@ -1075,6 +1079,7 @@ __device__ __forceinline__ void cols_CD_X_body(const KksConst* __restrict__ c, c
     }
     __syncthreads();
     bulk_wait(&bar, 0, ctl, fc->wait_polls);
+    __syncthreads();  // phase 0 seen by every thread before phase 1 is armed (as in cols_CD_eta)
     if (threadIdx.x == 0) {
       mbar_expect_tx(&bar, 8u * nv);
       bulk_g2s(s_sa, SA + fs + (size_t)ky0 * nx, 8u * nv, &bar);
