@@ -622,9 +622,11 @@ __device__ __forceinline__ void split_stage(const float2* z, const KksFftAxis& a
   for (int k = threadIdx.x; k < nyh; k += NT) {
     const float2 Zk = z[__ldg(ay.slot + k)];
     const float2 Zm = z[__ldg(ay.slot + (k == 0 ? 0 : ny - k))];
+    // rows x = 0, 1 of frequency k: one 16-byte store (the staging area is
+    // 128-byte aligned and i is even)
     const int i = stage_at(k, f, F, kb, 0);
-    stage[i] = make_float2(0.5f * (Zk.x + Zm.x), 0.5f * (Zk.y - Zm.y));
-    stage[i + 1] = make_float2(0.5f * (Zk.y + Zm.y), -0.5f * (Zk.x - Zm.x));
+    *reinterpret_cast<float4*>(stage + i) =
+        make_float4(0.5f * (Zk.x + Zm.x), 0.5f * (Zk.y - Zm.y), 0.5f * (Zk.y + Zm.y), -0.5f * (Zk.x - Zm.x));
   }
 }
 
@@ -634,7 +636,8 @@ __device__ __forceinline__ void merge_stage(float2* z, const KksFftAxis& ay, con
   const int ny = ay.n;
   for (int k = threadIdx.x; k < nyh; k += NT) {
     const int i = stage_at(k, f, F, kb, 0);
-    float2 A = stage[i], B = stage[i + 1];
+    const float4 v = *reinterpret_cast<const float4*>(stage + i);
+    float2 A = make_float2(v.x, v.y), B = make_float2(v.z, v.w);
     const bool self = k == 0 || 2 * k == ny;
     if (self) {
       A.y = 0.f;
@@ -789,6 +792,10 @@ __device__ __forceinline__ void cols_AB_body(const KksConst* __restrict__ c, con
     float2* dst = SA + (g == 2 ? fs : 0) + (size_t)ky0 * nx;
     for (int i = threadIdx.x; i < nv; i += NT) dst[i] = sm[i];
     if (g == 2) return;
+    // the eta role rewrites these columns in place below, element cc nx + p by
+    // thread p % NT, which is not the thread that copied it unless NT divides
+    // nx: every copy must have read its value first
+    __syncthreads();
   }
   const float inv_N = (float)c->inv_N;
   const float a = (float)(par->epsX * c->c3) * inv_N;

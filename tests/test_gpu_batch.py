@@ -272,7 +272,10 @@ def test_concurrent_prime71_cells_finish():
     (The column passes once re-armed their copy barrier for a second copy
     before every thread had seen the first complete; a warp delayed by the
     other cell's blocks then waited on a phase that could not complete, the
-    bounded wait ran out, and the run stopped with KKS_STATUS_TIMEOUT.)"""
+    bounded wait ran out, and the run stopped with KKS_STATUS_TIMEOUT. And the
+    first column pass once rewrote its FT(eta) columns in place while a
+    delayed warp was still copying them out: one spectral mode of the kept
+    FT(eta) came out wrong now and then, and the fields drifted by 1e-10.)"""
     from pf_kks_gpu import _lib as L
     from pf_kks_gpu import workloads
     from pf_kks_gpu.generator import MicrostructureSpec

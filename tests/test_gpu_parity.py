@@ -189,12 +189,14 @@ def test_checkpoint_restore_is_exact(precision):
     b.close()
 
 
-@pytest.mark.parametrize("shape", [(160, 160), (45, 38), (33, 64), (64, 31), (40, 50), (100, 80)])
+@pytest.mark.parametrize("shape", [(160, 160), (45, 38), (33, 64), (64, 31), (40, 50), (100, 80), (128, 192),
+                                   (384, 96), (256, 512)])
 def test_fused_fft_path_matches_oracle(tmp_path, shape):
     """The mixed step with the hand-written shared-memory FFTs (radices 2, 3,
     4, 5, 7 and the prime stages 11, 19, 71) against the FP64 oracle, and
     against the same step with cuFFT transforms. (64 x 31 has a prime factor
-    without a direct stage and runs cuFFT.)"""
+    without a direct stage and runs cuFFT; 128 x 192, 384 x 96 and 256 x 512
+    are sides of the ensemble workload.)"""
     from oracle import kks_oracle
     from pf_kks_gpu import workloads
     from pf_kks_gpu.generator import MicrostructureSpec
