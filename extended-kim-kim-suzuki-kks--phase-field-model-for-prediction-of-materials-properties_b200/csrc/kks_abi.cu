@@ -196,7 +196,8 @@ static int enqueue_fused(kks_handle* h, int p) {
   kks_fft_launch_attempt(h->fl, p, s);
   kks_launch_decide(h->dc, h->d_ctl, h->d_par, h->partials_fused, h->nb_fused, h->d_ring, h->ring_cap, h->d_rows,
                     h->row_cap, s);
-  kks_launch_restore<true>(&h->hc, h->dc, h->d_ctl, h->f, p, h->nblocks, s);
+  if (h->fl.f64) kks_launch_restore<false>(&h->hc, h->dc, h->d_ctl, h->f, p, h->nblocks, s);
+  else kks_launch_restore<true>(&h->hc, h->dc, h->d_ctl, h->f, p, h->nblocks, s);
   CK(cudaGetLastError());
   return KKS_OK;
 }
@@ -211,6 +212,7 @@ static int enqueue(kks_handle* h, int p) {
 // most one larger prime from KKS_FFT_PRIMES as the last DIF stage.
 struct AxisTables {
   std::vector<float2> tw;
+  std::vector<double2> tw64;  // the same twiddles in double (FP64 step)
   std::vector<int> slot;
 };
 
@@ -239,6 +241,7 @@ static bool build_axis(int n, KksFftAxis& ax, AxisTables& t) {
   ax.P = P;
   int L = n;
   t.tw.clear();
+  t.tw64.clear();
   for (int s = 0; s < ax.nst; ++s) {
     const int r = rad[s], q = L / r;
     ax.r[s] = r;
@@ -252,10 +255,14 @@ static bool build_axis(int n, KksFftAxis& ax, AxisTables& t) {
         for (int mm = 0; mm < r; ++mm) {
           const double th = 2.0 * M_PI * (double)((long long)j * mm % L) / (double)L;
           t.tw.push_back(make_float2((float)cos(th), (float)sin(th)));
+          t.tw64.push_back(make_double2(cos(th), sin(th)));
         }
     L = q;
   }
-  if (t.tw.empty()) t.tw.push_back(make_float2(1.f, 0.f));
+  if (t.tw.empty()) {
+    t.tw.push_back(make_float2(1.f, 0.f));
+    t.tw64.push_back(make_double2(1.0, 0.0));
+  }
   // position of frequency k after the DIF: digits d_s of the position (weights q_s)
   // are the digits of k read with weights r_0 r_1 ... r_{s-1}
   t.slot.assign(n, 0);
@@ -308,21 +315,30 @@ static int fused_rows(const kks_handle* h) {
   return std::max(std::max(kks_fft_row_blocks(h->hc.nx), kks_fft_col_blocks(h->hc.nyh, h->fl.cols)), h->nblocks);
 }
 
+// The fused passes of a mixed cell (kks_fft.cu) or of an FP64 cell
+// (kks_fft64.cu): the same plans and buffers, in single or double precision.
 static int setup_fused(kks_handle* h, const std::vector<double>& kx) {
   KksConst& c = h->hc;
+  const bool f64 = h->precision == KKS_PRECISION_FP64;
   KksFftConst fc;
   memset(&fc, 0, sizeof(fc));
   AxisTables tx, ty;
   if (!build_axis(c.nx, fc.ax, tx) || !build_axis(c.ny, fc.ay, ty)) return KKS_OK;  // not supported: cuFFT
   int optin = 0;
   CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device));
-  if (kks_fft_smem_bytes(c.nx, c.ny, KKS_FFT_COLS) > (size_t)optin) return KKS_OK;
-  fc.cols = KKS_FFT_COLS;
+  fc.cols = f64 ? 1 : KKS_FFT_COLS;
+  const size_t need = f64 ? kks_fft64_smem_bytes(c.nx, c.ny, fc.cols) : kks_fft_smem_bytes(c.nx, c.ny, fc.cols);
+  if (need > (size_t)optin) return KKS_OK;
   fc.wait_polls = KKS_FFT_WAIT_POLLS;
   std::vector<float> kx_slot(c.nx);
-  for (int k = 0; k < c.nx; ++k) kx_slot[tx.slot[k]] = (float)kx[k];
+  std::vector<double> kx_slot64(c.nx);
+  for (int k = 0; k < c.nx; ++k) {
+    kx_slot[tx.slot[k]] = (float)kx[k];
+    kx_slot64[tx.slot[k]] = kx[k];
+  }
   // device tables and buffers in one allocation
-  const size_t fs = (size_t)c.nx * c.nyh * sizeof(float2);
+  const size_t elem = f64 ? sizeof(double2) : sizeof(float2);
+  const size_t fs = (size_t)c.nx * c.nyh * elem;
   auto al = [](size_t b) { return (b + 255) / 256 * 256; };
   const size_t b_twx = al(tx.tw.size() * sizeof(float2)), b_twy = al(ty.tw.size() * sizeof(float2));
   const size_t b_slx = al(tx.slot.size() * sizeof(int)), b_sly = al(ty.slot.size() * sizeof(int));
@@ -331,8 +347,19 @@ static int setup_fused(kks_handle* h, const std::vector<double>& kx) {
   std::vector<float2> ptx(KKS_FFT_PRIME_TABLE_MAX), pty(KKS_FFT_PRIME_TABLE_MAX);
   const int npx = kks_fft_prime_table(fc.ax.P, ptx.data()), npy = kks_fft_prime_table(fc.ay.P, pty.data());
   const size_t b_ptx = al(std::max(npx, 1) * sizeof(float2)), b_pty = al(std::max(npy, 1) * sizeof(float2));
+  // the FP64 step's tables
+  std::vector<double2> ztx(KKS_FFT64_PRIME_TABLE_MAX), zty(KKS_FFT64_PRIME_TABLE_MAX);
+  int nzx = 0, nzy = 0;
+  size_t b_64 = 0;
+  if (f64) {
+    nzx = kks_fft64_prime_table(fc.ax.P, ztx.data());
+    nzy = kks_fft64_prime_table(fc.ay.P, zty.data());
+    b_64 = al(tx.tw64.size() * sizeof(double2)) + al(ty.tw64.size() * sizeof(double2)) +
+           al(kx_slot64.size() * sizeof(double)) + al(std::max(nzx, 1) * sizeof(double2)) +
+           al(std::max(nzy, 1) * sizeof(double2));
+  }
   const size_t b_spec = al(3 * fs) * 2 + al(2 * fs);
-  const size_t total = b_twx + b_twy + b_slx + b_sly + b_kxs + b_ptx + b_pty + b_spec;
+  const size_t total = b_twx + b_twy + b_slx + b_sly + b_kxs + b_ptx + b_pty + b_64 + b_spec;
   CK(cudaMalloc(&h->fft_arena, total));
   char* a = (char*)h->fft_arena;
   cudaError_t put_err = cudaSuccess;
@@ -350,6 +377,18 @@ static int setup_fused(kks_handle* h, const std::vector<double>& kx) {
   fc.kx_slot = (const float*)put(kx_slot.data(), kx_slot.size() * sizeof(float), b_kxs);
   fc.ax.ptw = (const float2*)put(ptx.data(), std::max(npx, 1) * sizeof(float2), b_ptx);
   fc.ay.ptw = (const float2*)put(pty.data(), std::max(npy, 1) * sizeof(float2), b_pty);
+  if (f64) {
+    fc.ax.tw64 = (const double2*)put(tx.tw64.data(), tx.tw64.size() * sizeof(double2),
+                                     al(tx.tw64.size() * sizeof(double2)));
+    fc.ay.tw64 = (const double2*)put(ty.tw64.data(), ty.tw64.size() * sizeof(double2),
+                                     al(ty.tw64.size() * sizeof(double2)));
+    fc.kx_slot64 = (const double*)put(kx_slot64.data(), kx_slot64.size() * sizeof(double),
+                                      al(kx_slot64.size() * sizeof(double)));
+    fc.ax.ptw64 = (const double2*)put(ztx.data(), std::max(nzx, 1) * sizeof(double2),
+                                      al(std::max(nzx, 1) * sizeof(double2)));
+    fc.ay.ptw64 = (const double2*)put(zty.data(), std::max(nzy, 1) * sizeof(double2),
+                                      al(std::max(nzy, 1) * sizeof(double2)));
+  }
   CK(put_err);
   void* RA = a; a += al(3 * fs);
   void* RB = a; a += al(3 * fs);
@@ -377,12 +416,14 @@ static int setup_fused(kks_handle* h, const std::vector<double>& kx) {
   L.cols = fc.cols;
   L.PX = fc.ax.P;
   L.PY = fc.ay.P;
+  L.f64 = f64 ? 1 : 0;
   // bulk copies of whole row pairs need 16-byte multiples for the f32 rows, the
   // tensor maps 16-byte strides (nx even; every pair then has both rows)
   // column runs start at multiples of nx * 8 bytes: bulk copies need nx even
-  L.bulk_cols = c.nx % 2 == 0 ? 1 : 0;
+  // (the FP64 passes move their spectra with plain loads and stores)
+  L.bulk_cols = (!f64 && c.nx % 2 == 0) ? 1 : 0;
   L.bulk_rows = 0;
-  if (c.nx % 2 == 0 && c.ny % 4 == 0 && encode_spectrum_map(&L.map_RA3, RA, c.nx, c.nyh, 3) &&
+  if (!f64 && c.nx % 2 == 0 && c.ny % 4 == 0 && encode_spectrum_map(&L.map_RA3, RA, c.nx, c.nyh, 3) &&
       encode_spectrum_map(&L.map_RB3, RB, c.nx, c.nyh, 3) && encode_spectrum_map(&L.map_RB2, RB, c.nx, c.nyh, 2))
     L.bulk_rows = 1;
   if (kks_fft_set_attributes(L) != 0) return set_error(KKS_ERR_CUDA, "fft kernel attributes");
@@ -581,7 +622,7 @@ static int create_impl(kks_handle* h, const kks_params* prm, int32_t n_steps, co
 
   int rc = make_plans(h);
   if (rc != KKS_OK) return rc;
-  if (h->precision == KKS_PRECISION_MIXED) {
+  if (h->precision != KKS_PRECISION_MIXED_CUFFT) {  // the cuFFT comparison path has no fused passes
     rc = setup_fused(h, kx);
     if (rc != KKS_OK) return rc;
   }
@@ -1000,7 +1041,7 @@ int kks_batch_create(kks_handle* const* cells, int32_t n_cells, int32_t groups, 
   for (int i = 0; i < n_cells; ++i) {
     const kks_handle* h = cells[i];
     if (!h) return set_error(KKS_ERR_ARG, "null cell");
-    if (!h->fused)
+    if (!h->fused || h->fl.f64)
       return set_error(KKS_ERR_ARG, "batched cells must use the fused mixed pipeline (KKS_PRECISION_MIXED, supported sizes)");
     if (h->device != cells[0]->device) return set_error(KKS_ERR_ARG, "cells must share one device");
     if (h->fl.PX != cells[0]->fl.PX || h->fl.PY != cells[0]->fl.PY)
@@ -1186,7 +1227,8 @@ int kks_bounds_report(int device, int32_t* checked, uint64_t* first) {
 
 int kks_set_wait_polls(kks_handle* h, int32_t polls) {
   if (!h) return set_error(KKS_ERR_ARG, "null handle");
-  if (!h->fused_ok || !h->d_fc) return set_error(KKS_ERR_STATE, "the cell has no fused passes (nothing waits)");
+  if (!h->fused_ok || !h->d_fc || h->fl.f64)
+    return set_error(KKS_ERR_STATE, "the cell has no bulk copies in its passes (nothing waits)");
   const int v = polls < 0 ? KKS_FFT_WAIT_POLLS : polls;
   CK(cudaSetDevice(h->device));
   CK(cudaStreamSynchronize(h->stream));
@@ -1547,8 +1589,9 @@ static int apply_shape(kks_handle* h, const kks_launch_shape& s) {
     if (s.cols < 1 || s.cols > KKS_FFT_COLS_MAX) return set_error(KKS_ERR_ARG, "cols out of range (1 .. 4)");
     int optin = 0;
     CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device));
-    if (kks_fft_smem_bytes(h->hc.nx, h->hc.ny, s.cols) > (size_t)optin)
-      return set_error(KKS_ERR_CAPACITY, "column tile does not fit shared memory");
+    const size_t need = h->fl.f64 ? kks_fft64_smem_bytes(h->hc.nx, h->hc.ny, s.cols)
+                                  : kks_fft_smem_bytes(h->hc.nx, h->hc.ny, s.cols);
+    if (need > (size_t)optin) return set_error(KKS_ERR_CAPACITY, "column tile does not fit shared memory");
   }
   CK(cudaSetDevice(h->device));
   CK(cudaStreamSynchronize(h->stream));

@@ -1612,6 +1612,7 @@ int kks_fft_partial_rows(int nx, int ny, int nbx) {
 
 // The large prime of each axis selects the kernel instantiation.
 int kks_fft_set_attributes(const KksFftLaunch& L) {
+  if (L.f64) return kks_fft64_set_attributes(L);
   int rc = -1, rc2 = -1;
 #define KKS_ROWS_ATTR(P) rc = set_row_attrs<P>(L.ny)
 #define KKS_COLS_ATTR(P) rc2 = set_col_attrs<P>(L.nx, L.cols)
@@ -1648,18 +1649,22 @@ int kks_fft_prime_table(int P, float2* out) {
 
 void kks_fft_launch_attempt(const KksFftLaunch& L, int p, cudaStream_t s) {
   const KksFieldPtrs& f = *L.f;
+  if (L.f64) {
+    kks_fft64_launch_passes(L, p, s);
+  } else {
 #define KKS_ROWS(P) launch_rows<P>(L, p, stage, s)
 #define KKS_COLS(P) launch_cols<P>(L, stage, s)
-  int stage = 0;
-  KKS_FFT_DISPATCH(L.PY, KKS_ROWS)
-  KKS_FFT_DISPATCH(L.PX, KKS_COLS)
-  stage = 1;
-  KKS_FFT_DISPATCH(L.PY, KKS_ROWS)
-  KKS_FFT_DISPATCH(L.PX, KKS_COLS)
-  stage = 2;
-  KKS_FFT_DISPATCH(L.PY, KKS_ROWS)
+    int stage = 0;
+    KKS_FFT_DISPATCH(L.PY, KKS_ROWS)
+    KKS_FFT_DISPATCH(L.PX, KKS_COLS)
+    stage = 1;
+    KKS_FFT_DISPATCH(L.PY, KKS_ROWS)
+    KKS_FFT_DISPATCH(L.PX, KKS_COLS)
+    stage = 2;
+    KKS_FFT_DISPATCH(L.PY, KKS_ROWS)
 #undef KKS_ROWS
 #undef KKS_COLS
+  }
   kf_extras<<<L.nbx, kExtrasThreads, 0, s>>>(L.dc, L.par, (const double*)f.eta[1 - p], 3, P5_GRAD2, P5_IFACE,
                                        f.partials);
 }

@@ -29,12 +29,17 @@ struct KksFftAxis {
   const float2* tw;
   const int* slot;
   const float2* ptw;  // prime DFT factors, (cos, sin) pairs (see kks_fft_prime_table); null if P = 0
+  // the FP64 step's tables (kks_fft64.cu): the same twiddles in double, and
+  // its prime factors (kks_fft64_prime_table); null in a mixed cell
+  const double2* tw64;
+  const double2* ptw64;
 };
 
 struct KksFftConst {
   KksFftAxis ax;         // x axis (column passes)
   KksFftAxis ay;         // y axis (row passes)
   const float* kx_slot;  // k_x of the frequency held at each x slot after the DIF
+  const double* kx_slot64;  // the same in double (FP64 step)
   int cols;              // y-frequency columns per column-pass block (1..KKS_FFT_COLS_MAX)
   int wait_polls;        // polls of the first wait for a block's bulk / tensor copies (KKS_FFT_WAIT_POLLS;
                          // kks_set_wait_polls changes it for fault-path tests)
@@ -59,6 +64,7 @@ struct KksFftLaunch {
   int nbx;   // grid of the pointwise extras kernel
   int cols;  // y-frequency columns per column-pass block (the device copy is fc->cols)
   int PX, PY;
+  int f64;        // 1: the FP64 step's passes (kks_fft64.cu; plain loads, no tensor maps)
   int bulk_rows;  // 1: row passes move their spectra with tensor copies and stage their state
                   // rows with bulk copies (needs nx % 2 == 0, ny % 4 == 0 and encoded maps)
   int bulk_cols;  // 1: column passes load their columns with bulk copies (needs nx % 2 == 0)
@@ -89,6 +95,14 @@ int kks_fft_prime_table(int P, float2* out);
 // reset is nonzero. Returns 1 in a bounds-check build, 0 otherwise (*first = 0).
 int kks_fft_bounds_word(unsigned long long* first, int reset);
 void kks_fft_launch_attempt(const KksFftLaunch& L, int parity, cudaStream_t s);
+
+// The FP64 step's passes (kks_fft64.cu). Prime tables: at most
+// KKS_FFT64_PRIME_TABLE_MAX (cos, sin) pairs in double, layout of ZPrime there.
+#define KKS_FFT64_PRIME_TABLE_MAX (7 * 35 * 5)
+size_t kks_fft64_smem_bytes(int nx, int ny, int cols);
+int kks_fft64_set_attributes(const KksFftLaunch& L);
+int kks_fft64_prime_table(int P, double2* out);
+void kks_fft64_launch_passes(const KksFftLaunch& L, int parity, cudaStream_t s);
 
 // ---------------------------------------------------------------------------
 // Batched launches: the cells of an ensemble advance together, every kernel of

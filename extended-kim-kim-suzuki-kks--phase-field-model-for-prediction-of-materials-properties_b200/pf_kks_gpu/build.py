@@ -38,6 +38,7 @@ SOURCES = {
     "kks_fields.cu": [],
     "kks_abi.cu": [],
     "kks_fft.cu": [],
+    "kks_fft64.cu": [],
     "kks_noalloc.cu": [],
     "kks_adjoint.cu": [],
     "kks_init.cu": ["-fmad=false"],
@@ -57,7 +58,7 @@ def cuda_home():
 def _deps(src):
     """Sources plus the headers they include."""
     return [src, os.path.join(CSRC, "kks_internal.cuh"), os.path.join(CSRC, "kks_fft.cuh"),
-            os.path.join(CSRC, "kks_check.cuh"), os.path.join(INCLUDE, "kks.h")]
+            os.path.join(CSRC, "kks_check.cuh"), os.path.join(CSRC, "kks_pointwise.cuh"), os.path.join(INCLUDE, "kks.h")]
 
 
 def _stale(target, deps):

@@ -82,9 +82,11 @@ def test_invalid_shapes_are_rejected():
             with pytest.raises(L.KksError):
                 c.set_launch_shape(*args)
         with pytest.raises(L.KksError):
-            f.set_launch_shape(1, 3, 8)  # no fused passes for FP64
-        f.set_launch_shape(0, 0, 4)
-        assert f.launch_shape()["field_blocks"] == 4
+            f.set_launch_shape(1, 5, 8)  # the FP64 passes take the same column tiles
+        f.set_launch_shape(1, 2, 8)
+        assert f.launch_shape() == {"pipeline": 1, "cols": 2, "field_blocks": 8}
+        f.set_launch_shape(0, 2, 4)
+        assert f.launch_shape()["field_blocks"] == 4 and f.launch_shape()["pipeline"] == 0
     finally:
         c.close()
         f.close()

@@ -71,7 +71,7 @@ def test_wait_polls_needs_fused_passes():
     tables = MaterialTables.from_npz(cfg.material_tables, cfg.c_gamma, cfg.c_eps0)
     cell = solver.Cell(cfg, tables, precision="fp64")
     try:
-        with pytest.raises(L.KksError, match="no fused passes"):
+        with pytest.raises(L.KksError, match="nothing waits"):
             cell.set_wait_polls(0)
     finally:
         cell.close()
