@@ -292,6 +292,32 @@ __global__ void k_finish(const double* __restrict__ partials, int nb, double* __
   out[k] = v;
 }
 
+// The gradient of <lam_out, state_out> with respect to the coefficient row
+// from the finished sums g (one thread; the same expressions as the host
+// version in kks_adj_backward).
+__device__ __host__ inline void dcoef_of(const double* g, const Coef& c, double* d) {
+  for (int k = 0; k < KKS_COEF_COUNT; ++k) d[k] = 0.0;
+  d[KKS_COEF_DT] = c.Ls * g[S_GP] + c.Ds * g[S_GQ];
+  d[KKS_COEF_LS] = c.dt * g[S_GP];
+  d[KKS_COEF_KAPPA2] = g[S_GK];
+  d[KKS_COEF_DS] = c.dt * g[S_GQ];
+  d[KKS_COEF_W] = g[S_W];
+  d[KKS_COEF_A_ALP] = g[S_AA];
+  d[KKS_COEF_B_ALP] = g[S_BA];
+  d[KKS_COEF_C_ALP] = g[S_CA];
+  d[KKS_COEF_A_THET] = g[S_AT];
+  d[KKS_COEF_B_THET] = g[S_BT];
+  d[KKS_COEF_C_THET] = g[S_CT];
+  d[KKS_COEF_EPSX] = g[S_EPSX];
+  d[KKS_COEF_C44] = g[S_C44];
+  d[KKS_COEF_PC_SHIFT] = g[S_PCS];
+  d[KKS_COEF_PC_RATIO] = g[S_PCR];
+}
+
+__global__ void k_dcoef(const double* __restrict__ g, Coef c, double* __restrict__ d) {
+  if (threadIdx.x == 0) dcoef_of(g, c, d);
+}
+
 // i kx A + i ky B (both half spectra), times 1/N
 __global__ void k_spec_div(const double2* __restrict__ A, const double2* __restrict__ B, double2* __restrict__ out,
                            Spec s, const double* kx, const double* ky) {
@@ -323,7 +349,9 @@ struct kks_adj {
   int device = 0;
   int mixed = 0;  // 1: FP32 transforms (kks_adj_set_precision)
   Spec s{};
-  cudaStream_t stream = nullptr;
+  cudaStream_t stream = nullptr;  // the stream the calls run on (own, or bound by kks_adj_set_stream)
+  cudaStream_t own = nullptr;     // the handle's own stream
+  bool bound = false;             // calls run on a caller's stream and return without waiting
   cufftHandle r2c = 0, c2r = 0;
   cufftHandle r2c32 = 0, c2r32 = 0;
   float* fbuf = nullptr;   // FP32 real transform buffer (N)
@@ -444,8 +472,9 @@ int kks_adj_create(int32_t nx, int32_t ny, double C11_0, double C12_0, double C4
   s.c11 = C11_0 / C44_0;
   s.c12 = C12_0 / C44_0;
   auto fail = [&](int rc) { kks_adj_destroy(h); return rc; };
-  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess)
+  if (cudaStreamCreateWithFlags(&h->own, cudaStreamNonBlocking) != cudaSuccess)
     return fail(kks_set_error(KKS_ERR_CUDA, "stream"));
+  h->stream = h->own;
   std::vector<double> kx, ky;
   wave_numbers(nx, kx, nx);
   wave_numbers(ny, ky, s.nyh);
@@ -490,17 +519,16 @@ int kks_adj_forward(kks_adj* h, const double* state_in, const double* coef, doub
   }
   k_phase<<<kBlocks, kT, 0, st>>>(state_in + s.N, eb, state_out + 2 * (size_t)s.N, state_out + 3 * (size_t)s.N, s.N, c);
   ACK(cudaGetLastError());
-  ACK(cudaStreamSynchronize(st));
+  if (!h->bound) ACK(cudaStreamSynchronize(st));
   return KKS_OK;
 }
 
-int kks_adj_backward(kks_adj* h, const double* state_in, const double* state_out, const double* coef,
-                     const double* lam_out, double* lam_in, double* dcoef) {
-  if (!h || !state_in || !state_out || !coef || !lam_out || !lam_in || !dcoef)
-    return kks_set_error(KKS_ERR_ARG, "null argument");
-  ACK(cudaSetDevice(h->device));
+}  // extern "C"
+
+// The backward pass up to the finished sums in h->sums (on h->stream).
+static int backward_sums(kks_adj* h, const double* state_in, const double* state_out, const Coef& c,
+                         const double* lam_out, double* lam_in) {
   const Spec& s = h->s;
-  const Coef c = coef_of(coef);
   cudaStream_t st = h->stream;
   const size_t N = s.N;
   int rc = front(h, state_in, c);  // fields 0 tr, 1 gx, 2 gy, 3 drive, 4 fx, 5 fy; spectra 0-4
@@ -549,25 +577,53 @@ int kks_adj_backward(kks_adj* h, const double* state_in, const double* state_out
                                        lam_x, s.N);
   k_finish<<<1, 32, 0, st>>>(h->partials, kBlocks, h->sums);
   ACK(cudaGetLastError());
-  ACK(cudaMemcpyAsync(h->h_sums, h->sums, kNS * sizeof(double), cudaMemcpyDeviceToHost, st));
-  ACK(cudaStreamSynchronize(st));
-  const double* g = h->h_sums;
-  for (int k = 0; k < KKS_COEF_COUNT; ++k) dcoef[k] = 0.0;
-  dcoef[KKS_COEF_DT] = c.Ls * g[S_GP] + c.Ds * g[S_GQ];
-  dcoef[KKS_COEF_LS] = c.dt * g[S_GP];
-  dcoef[KKS_COEF_KAPPA2] = g[S_GK];
-  dcoef[KKS_COEF_DS] = c.dt * g[S_GQ];
-  dcoef[KKS_COEF_W] = g[S_W];
-  dcoef[KKS_COEF_A_ALP] = g[S_AA];
-  dcoef[KKS_COEF_B_ALP] = g[S_BA];
-  dcoef[KKS_COEF_C_ALP] = g[S_CA];
-  dcoef[KKS_COEF_A_THET] = g[S_AT];
-  dcoef[KKS_COEF_B_THET] = g[S_BT];
-  dcoef[KKS_COEF_C_THET] = g[S_CT];
-  dcoef[KKS_COEF_EPSX] = g[S_EPSX];
-  dcoef[KKS_COEF_C44] = g[S_C44];
-  dcoef[KKS_COEF_PC_SHIFT] = g[S_PCS];
-  dcoef[KKS_COEF_PC_RATIO] = g[S_PCR];
+  return KKS_OK;
+}
+
+extern "C" {
+
+int kks_adj_backward(kks_adj* h, const double* state_in, const double* state_out, const double* coef,
+                     const double* lam_out, double* lam_in, double* dcoef) {
+  if (!h || !state_in || !state_out || !coef || !lam_out || !lam_in || !dcoef)
+    return kks_set_error(KKS_ERR_ARG, "null argument");
+  ACK(cudaSetDevice(h->device));
+  const Coef c = coef_of(coef);
+  int rc = backward_sums(h, state_in, state_out, c, lam_out, lam_in);
+  if (rc != KKS_OK) return rc;
+  ACK(cudaMemcpyAsync(h->h_sums, h->sums, kNS * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  ACK(cudaStreamSynchronize(h->stream));
+  dcoef_of(h->h_sums, c, dcoef);
+  return KKS_OK;
+}
+
+int kks_adj_backward_device(kks_adj* h, const double* state_in, const double* state_out, const double* coef,
+                            const double* lam_out, double* lam_in, double* dcoef_device) {
+  if (!h || !state_in || !state_out || !coef || !lam_out || !lam_in || !dcoef_device)
+    return kks_set_error(KKS_ERR_ARG, "null argument");
+  ACK(cudaSetDevice(h->device));
+  const Coef c = coef_of(coef);
+  int rc = backward_sums(h, state_in, state_out, c, lam_out, lam_in);
+  if (rc != KKS_OK) return rc;
+  k_dcoef<<<1, 32, 0, h->stream>>>(h->sums, c, dcoef_device);
+  ACK(cudaGetLastError());
+  if (!h->bound) ACK(cudaStreamSynchronize(h->stream));
+  return KKS_OK;
+}
+
+int kks_adj_set_stream(kks_adj* h, void* stream) {
+  if (!h) return kks_set_error(KKS_ERR_ARG, "null handle");
+  ACK(cudaSetDevice(h->device));
+  cudaStream_t want = stream ? (cudaStream_t)stream : h->own;
+  if (want == h->stream) {
+    h->bound = stream != nullptr;
+    return KKS_OK;
+  }
+  // work already queued on the old stream comes before anything on the new one
+  ACK(cudaStreamSynchronize(h->stream));
+  h->stream = want;
+  h->bound = stream != nullptr;
+  for (cufftHandle p : {h->r2c, h->c2r, h->r2c32, h->c2r32})
+    if (p && cufftSetStream(p, h->stream) != CUFFT_SUCCESS) return kks_set_error(KKS_ERR_CUFFT, "plan stream");
   return KKS_OK;
 }
 
@@ -608,7 +664,8 @@ int kks_adj_destroy(kks_adj* h) {
   cudaFree(h->partials);
   cudaFree(h->sums);
   if (h->h_sums) cudaFreeHost(h->h_sums);
-  if (h->stream) cudaStreamDestroy(h->stream);
+  if (h->bound && h->stream) cudaStreamSynchronize(h->stream);
+  if (h->own) cudaStreamDestroy(h->own);
   delete h;
   return KKS_OK;
 }

@@ -55,6 +55,7 @@ EXPORTS = (
     "kks_checkpoint", "kks_restore", "kks_timing", "kks_destroy", "kks_last_error", "kks_version",
     "kks_state_sums_noalloc", "kks_run_many", "kks_pipeline",
     "kks_adj_create", "kks_adj_forward", "kks_adj_backward", "kks_adj_destroy", "kks_adj_set_precision",
+    "kks_adj_backward_device", "kks_adj_set_stream",
     "kks_voronoi_edges", "kks_generate_fields", "kks_place_precipitates", "kks_add_nuclei", "kks_count_below",
     "kks_insert_nuclei", "kks_batch_create", "kks_batch_run", "kks_batch_timing", "kks_batch_destroy",
     "kks_get_launch_shape", "kks_set_launch_shape", "kks_autotune", "kks_download_pair",
@@ -166,8 +167,10 @@ def load(path=LIB_PATH):
     lib.kks_adj_backward.argtypes = [vp, vp, vp, dp, vp, vp, dp]
     lib.kks_adj_destroy.argtypes = [vp]
     lib.kks_adj_set_precision.argtypes = [vp, ctypes.c_int]
+    lib.kks_adj_backward_device.argtypes = [vp, vp, vp, dp, vp, vp, vp]
+    lib.kks_adj_set_stream.argtypes = [vp, vp]
     for name in ("kks_adj_create", "kks_adj_forward", "kks_adj_backward", "kks_adj_destroy",
-                 "kks_adj_set_precision"):
+                 "kks_adj_set_precision", "kks_adj_backward_device", "kks_adj_set_stream"):
         getattr(lib, name).restype = ctypes.c_int
     lib.kks_destroy.argtypes = [vp]
     lib.kks_run_many.argtypes = [P(vp), ctypes.c_int32, P(ctypes.c_int32), P(ctypes.c_int32)]

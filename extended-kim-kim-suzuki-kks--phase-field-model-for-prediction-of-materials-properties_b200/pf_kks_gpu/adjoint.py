@@ -158,7 +158,11 @@ class StepAdjoint:
     """The fixed-dt step and its adjoint on one GPU (a ``kks_adj`` handle).
 
     Tensors are float64 CUDA tensors of shape (4, nx, ny) (eta, X, X_al,
-    X_th); coefficient rows are 15 float64 values."""
+    X_th); coefficient rows are 15 float64 values. Every call runs on torch's
+    current CUDA stream (kks_adj_set_stream) and returns once its work is
+    queued: the results are ordered for whatever torch does next on that
+    stream, and nothing waits on the host (a run of steps is launch-bound, not
+    bound by a host round trip per step)."""
 
     def __init__(self, nx, ny, C11_0, C12_0, C44_0, device=0, surf_scale=1.0, precision="fp64"):
         self.lib = L.load()
@@ -169,6 +173,7 @@ class StepAdjoint:
                                         ctypes.byref(h)), "kks_adj_create")
         self.h = h
         self.precision = precision
+        self._stream = None
         if precision != "fp64":
             code = {"mixed": L.KKS_PRECISION_MIXED}[precision]
             L.check(self.lib.kks_adj_set_precision(self.h, code), "kks_adj_set_precision")
@@ -186,7 +191,10 @@ class StepAdjoint:
         for t in tensors:
             if t.dtype != torch.float64 or not t.is_cuda or not t.is_contiguous() or t.numel() != 4 * self.nx * self.ny:
                 raise ValueError("state tensors must be contiguous float64 CUDA tensors of 4 * nx * ny values")
-        torch.cuda.current_stream().synchronize()
+        stream = torch.cuda.current_stream(self.device).cuda_stream
+        if stream != self._stream:
+            L.check(self.lib.kks_adj_set_stream(self.h, ctypes.c_void_p(stream)), "kks_adj_set_stream")
+            self._stream = stream
 
     @staticmethod
     def _row(coef):
@@ -214,6 +222,23 @@ class StepAdjoint:
                                           ctypes.c_void_p(lam_out.data_ptr()), ctypes.c_void_p(lam_in.data_ptr()),
                                           d.ctypes.data_as(ctypes.POINTER(ctypes.c_double))), "kks_adj_backward")
         return d
+
+    def backward_into(self, state_in, state_out, coef, lam_out, lam_in, dcoef):
+        """backward() with the 15 gradient values written into ``dcoef``, a
+        float64 CUDA tensor of KKS_COEF_COUNT values, by the stream."""
+        self._check(state_in, state_out, lam_out, lam_in)
+        torch = _torch()
+        if dcoef.dtype != torch.float64 or not dcoef.is_cuda or not dcoef.is_contiguous() or \
+                dcoef.numel() != L.KKS_COEF_COUNT:
+            raise ValueError("dcoef must be a contiguous float64 CUDA tensor of KKS_COEF_COUNT values")
+        row = self._row(coef)
+        L.check(self.lib.kks_adj_backward_device(self.h, ctypes.c_void_p(state_in.data_ptr()),
+                                                 ctypes.c_void_p(state_out.data_ptr()),
+                                                 row.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                                 ctypes.c_void_p(lam_out.data_ptr()),
+                                                 ctypes.c_void_p(lam_in.data_ptr()),
+                                                 ctypes.c_void_p(dcoef.data_ptr())), "kks_adj_backward_device")
+        return dcoef
 
     def close(self):
         if getattr(self, "h", None):
@@ -293,7 +318,7 @@ def _make_function():
             s0 = ctx.ckpt[0]
             N = s0[0].numel()
             lam = torch.zeros_like(s0) if g_final is None else g_final.detach().contiguous().clone()
-            grad_coef = np.zeros(c.shape, dtype=np.float64)
+            grad_coef = torch.zeros(c.shape, dtype=torch.float64, device=s0.device)
             starts = sorted(ctx.ckpt)
             for seg in reversed(range(len(starts))):
                 a = starts[seg]
@@ -305,16 +330,18 @@ def _make_function():
                     states.append(nxt)
                 for i in reversed(range(a, b)):
                     lam_in = torch.empty_like(lam)
-                    grad_coef[i] = stepper.backward(states[i - a], states[i - a + 1], c[i], lam, lam_in)
+                    stepper.backward_into(states[i - a], states[i - a + 1], c[i], lam, lam_in, grad_coef[i])
                     # history seeds of the step's input state
                     if g_eta is not None:
                         lam_in[0] += g_eta[i] / N
                     if g_xal is not None:
+                        # X_al_mean is the mean over eta < 0.05 (NaN, with no gradient, when no point is)
                         _, _, mask, cnt = _histories(states[i - a])
-                        if int(cnt) > 0:
-                            lam_in[1] += g_xal[i] * mask.to(lam_in.dtype) / cnt
+                        w = torch.where(cnt > 0, g_xal[i] / cnt.clamp(min=1), torch.zeros((), dtype=lam_in.dtype,
+                                                                                          device=lam_in.device))
+                        lam_in[1] += w * mask.to(lam_in.dtype)
                     lam = lam_in
-            gc = torch.tensor(grad_coef, dtype=ctx.coef_dtype).reshape(ctx.coef_shape)
+            gc = grad_coef.to(device="cpu", dtype=ctx.coef_dtype).reshape(ctx.coef_shape)
             return gc, lam, None, None
 
     return FixedDtRun

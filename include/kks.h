@@ -289,7 +289,8 @@ int kks_state_sums_noalloc(const double* eta, const double* X, int32_t nx, int32
  * pf_kks/free_energy.py:74-95). State buffers are device float64 arrays of
  * 4*nx*ny: eta | X | X_al | X_th, each C-order (nx, ny). The stiffness is
  * frozen at C11_0, C12_0, C44_0 (pf_kks/solver.py:152-154). Calls run on the
- * handle's own stream and return after it has finished. */
+ * handle's own stream and return after it has finished, unless the handle is
+ * bound to a caller's stream (kks_adj_set_stream). */
 enum {
   KKS_COEF_DT = 0, KKS_COEF_LS, KKS_COEF_KAPPA2, KKS_COEF_DS, KKS_COEF_W, KKS_COEF_A_ALP, KKS_COEF_B_ALP,
   KKS_COEF_C_ALP, KKS_COEF_A_THET, KKS_COEF_B_THET, KKS_COEF_C_THET, KKS_COEF_EPSX, KKS_COEF_C44,
@@ -305,6 +306,15 @@ int kks_adj_forward(kks_adj* h, const double* state_in, const double* coef, doub
  * with respect to coef (host array). */
 int kks_adj_backward(kks_adj* h, const double* state_in, const double* state_out, const double* coef,
                      const double* lam_out, double* lam_in, double* dcoef);
+/* kks_adj_backward with dcoef[KKS_COEF_COUNT] written to device memory by the
+ * stream, so that a run of backward steps needs no host round trip. */
+int kks_adj_backward_device(kks_adj* h, const double* state_in, const double* state_out, const double* coef,
+                            const double* lam_out, double* lam_in, double* dcoef_device);
+/* Run the handle's calls on the caller's CUDA stream (a cudaStream_t; the
+ * calls then return once their work is queued, ordered after earlier work on
+ * that stream), or, with stream = NULL, on the handle's own stream, returning
+ * after it has finished (the default). Switching waits for queued work. */
+int kks_adj_set_stream(kks_adj* h, void* stream);
 /* Precision of the handle's step and adjoint: KKS_PRECISION_FP64 (default)
  * or KKS_PRECISION_MIXED: every transform in FP32 (cuFFT R2C / C2R on the
  * rounded input, output widened back), all pointwise work, the state and the
