@@ -221,9 +221,17 @@ static uint32_t div_magic(int d) {
   return d <= 1 ? 0u : (uint32_t)((((uint64_t)1 << 32) + (uint64_t)d - 1) / (uint64_t)d);
 }
 
-static bool build_axis(int n, KksFftAxis& ax, AxisTables& t) {
+static bool build_axis(int n, KksFftAxis& ax, AxisTables& t, bool radix8) {
   std::vector<int> rad;
   int m = n;
+  // radix-8 stages first where the sides allow them (fewer passes over shared
+  // memory, barriers and index computations) on axes without a large prime
+  // (their kernels are built without radix 8); the FP64 passes keep radix 4
+  int rest = n;
+  for (int r : {2, 3, 5, 7})
+    while (rest % r == 0) rest /= r;
+  if (radix8 && rest == 1)
+    while (m % 8 == 0) { rad.push_back(8); m /= 8; }
   for (int r : {4, 2, 3, 5, 7})
     while (m % r == 0) { rad.push_back(r); m /= r; }
   int P = 0;
@@ -323,7 +331,7 @@ static int setup_fused(kks_handle* h, const std::vector<double>& kx) {
   KksFftConst fc;
   memset(&fc, 0, sizeof(fc));
   AxisTables tx, ty;
-  if (!build_axis(c.nx, fc.ax, tx) || !build_axis(c.ny, fc.ay, ty)) return KKS_OK;  // not supported: cuFFT
+  if (!build_axis(c.nx, fc.ax, tx, !f64) || !build_axis(c.ny, fc.ay, ty, !f64)) return KKS_OK;  // not supported: cuFFT
   int optin = 0;
   CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device));
   fc.cols = f64 ? 1 : KKS_FFT_COLS;

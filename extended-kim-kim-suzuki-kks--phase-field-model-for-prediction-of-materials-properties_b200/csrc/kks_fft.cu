@@ -174,6 +174,24 @@ __device__ __forceinline__ void dft_small(float2 (&x)[R]) {
     const float2 it3 = DIR < 0 ? make_float2(t3.y, -t3.x) : make_float2(-t3.y, t3.x);
     x[1] = cadd(t1, it3);
     x[3] = csub(t1, it3);
+  } else if constexpr (R == 8) {
+    // two 4-point DFTs of the even and the odd values, combined with
+    // w^k = exp(DIR 2 pi i k / 8): X_k = E_k + w^k O_k, X_{k+4} = E_k - w^k O_k
+    float2 e[4] = {x[0], x[2], x[4], x[6]}, o[4] = {x[1], x[3], x[5], x[7]};
+    dft_small<4, DIR>(e);
+    dft_small<4, DIR>(o);
+    constexpr float h = 0.707106781186547524f;  // sqrt(1/2)
+    const float2 w1o = make_float2(h * (o[1].x - DIR * o[1].y), h * (o[1].y + DIR * o[1].x));
+    const float2 w2o = DIR < 0 ? make_float2(o[2].y, -o[2].x) : make_float2(-o[2].y, o[2].x);
+    const float2 w3o = make_float2(h * (-o[3].x - DIR * o[3].y), h * (-o[3].y + DIR * o[3].x));
+    x[0] = cadd(e[0], o[0]);
+    x[4] = csub(e[0], o[0]);
+    x[1] = cadd(e[1], w1o);
+    x[5] = csub(e[1], w1o);
+    x[2] = cadd(e[2], w2o);
+    x[6] = csub(e[2], w2o);
+    x[3] = cadd(e[3], w3o);
+    x[7] = csub(e[3], w3o);
   } else {
     constexpr int H = (R - 1) / 2;
     float2 s[H], d[H];
@@ -541,6 +559,9 @@ __device__ __forceinline__ void fft_run(int nseq, const KksFftAxis& ax) {
         case 4: bfly_small<4, DIR>(base, q, j, tw); break;
         case 5: bfly_small<5, DIR>(base, q, j, tw); break;
         case 7: bfly_small<7, DIR>(base, q, j, tw); break;
+        case 8:
+          if constexpr (P <= 7) bfly_small<8, DIR>(base, q, j, tw);  // (axes with a large prime: radix <= 7)
+          break;
         default: break;
       }
     }
