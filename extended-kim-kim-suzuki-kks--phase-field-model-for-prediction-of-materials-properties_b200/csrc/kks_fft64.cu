@@ -367,22 +367,68 @@ __device__ __forceinline__ void zsplit_store(const double2* z, const KksFftAxis&
   }
 }
 
-// Inverse of zsplit_store; the y = 0 and Nyquist bins of a real row are real.
-template <int NT>
-__device__ __forceinline__ void zmerge_load(double2* z, const KksFftAxis& ay, const double2* __restrict__ src, int ix0,
-                                            bool has1, int nx, int nyh) {
+// Inverse of zsplit_store for F fields of a spectrum buffer (field f at src +
+// f fs, into z + f ny; the y = 0 and Nyquist bins of a real row are real), the loads of U frequencies of every field issued before any
+// store: each load is a 32-byte row-pair value from its own memory row, so
+// several in flight per thread hide their latency.
+template <int NT, int F>
+__device__ __forceinline__ void zmerge_fields(double2* z, const KksFftAxis& ay, const double2* __restrict__ src,
+                                              size_t fs, int ix0, bool has1, int nx, int nyh) {
+  constexpr int U = 2;
   const int ny = ay.n;
-  for (int k = threadIdx.x; k < nyh; k += NT) {
-    const double2* s = src + (size_t)k * nx + ix0;
-    double2 A = s[0];
-    double2 B = has1 ? s[1] : make_double2(0.0, 0.0);
-    const bool self = k == 0 || 2 * k == ny;
-    if (self) {
-      A.y = 0.0;
-      B.y = 0.0;
+  for (int k0 = threadIdx.x; k0 < nyh; k0 += U * NT) {
+    double2 A[U][F], B[U][F];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int k = k0 + u * NT;
+#pragma unroll
+      for (int f = 0; f < F; ++f) {
+        A[u][f] = make_double2(0.0, 0.0);
+        B[u][f] = make_double2(0.0, 0.0);
+        if (k < nyh) {
+          const double2* sp = src + f * fs + (size_t)k * nx + ix0;
+          A[u][f] = sp[0];
+          if (has1) B[u][f] = sp[1];
+        }
+      }
     }
-    z[__ldg(ay.slot + k)] = make_double2(A.x - B.y, A.y + B.x);
-    if (!self) z[__ldg(ay.slot + (ny - k))] = make_double2(A.x + B.y, B.x - A.y);
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int k = k0 + u * NT;
+      if (k >= nyh) continue;
+      const bool self = k == 0 || 2 * k == ny;
+      const int sk = __ldg(ay.slot + k);
+      const int sm = self ? 0 : __ldg(ay.slot + (ny - k));
+#pragma unroll
+      for (int f = 0; f < F; ++f) {
+        double2 a = A[u][f], b = B[u][f];
+        if (self) {
+          a.y = 0.0;
+          b.y = 0.0;
+        }
+        z[f * ny + sk] = make_double2(a.x - b.y, a.y + b.x);
+        if (!self) z[f * ny + sm] = make_double2(a.x + b.y, b.x - a.y);
+      }
+    }
+  }
+}
+
+// d[0, n) = s[0, n) (global -> shared), four loads in flight per thread.
+template <int NT>
+__device__ __forceinline__ void zcopy_in(double2* d, const double2* __restrict__ s, int n) {
+  constexpr int U = 4;
+  for (int i0 = threadIdx.x; i0 < n; i0 += U * NT) {
+    double2 v[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int i = i0 + u * NT;
+      if (i < n) v[u] = s[i];
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int i = i0 + u * NT;
+      if (i < n) d[i] = v[u];
+    }
   }
 }
 
@@ -458,7 +504,7 @@ __global__ void __launch_bounds__(nt64<PX>(), minb64<PX>())
   const int nv = ncol * nx;
   const int src_field = g == 0 ? 0 : (g == 1 ? 2 : 1);
   const double2* col = RA + src_field * fs + (size_t)ky0 * nx;
-  for (int i = threadIdx.x; i < nv; i += NT) zsm[i] = col[i];
+  zcopy_in<NT>(zsm, col, nv);
   __syncthreads();
   zfft_run<-1, PX>(ncol, ax);
   if (g != 1) {
@@ -532,7 +578,7 @@ __global__ void __launch_bounds__(nt64<PY>(), minb64<PY>())
   const size_t fs = (size_t)nx * nyh;
   const int bx = blockIdx.x, ix0 = 2 * bx;
   const bool has1 = ix0 + 1 < nx;
-  for (int f = 0; f < 3; ++f) zmerge_load<NT>(zsm + f * ny, ay, RB + f * fs, ix0, has1, nx, nyh);
+  zmerge_fields<NT, 3>(zsm, ay, RB, fs, ix0, has1, nx, nyh);
   __syncthreads();
   zfft_run<+1, PY>(3, ay);
   const KksPar q = *par;
@@ -587,7 +633,7 @@ __global__ void __launch_bounds__(nt64<PX>(), minb64<PX>())
   const int ncol = min(cols, nyh - ky0);
   const int nv = ncol * nx;
   const double2* col = RC + (size_t)ky0 * nx;
-  for (int i = threadIdx.x; i < nv; i += NT) zsm[i] = col[i];
+  zcopy_in<NT>(zsm, col, nv);
   __syncthreads();
   zfft_run<-1, PX>(ncol, ax);
   const double inv_N = c->inv_N;
@@ -630,10 +676,8 @@ __global__ void __launch_bounds__(nt64<PX>(), minb64<PX>())
   const int nv = ncol * nx;
   const double2* cx = RC + fs + (size_t)ky0 * nx;
   const double2* cy = RC + 2 * fs + (size_t)ky0 * nx;
-  for (int i = threadIdx.x; i < nv; i += NT) {
-    zsm[i] = cx[i];
-    zsm[nv + i] = cy[i];
-  }
+  zcopy_in<NT>(zsm, cx, nv);
+  zcopy_in<NT>(zsm + nv, cy, nv);
   __syncthreads();
   zfft_run<-1, PX>(2 * ncol, ax);
   const double inv_N = c->inv_N;
@@ -680,8 +724,7 @@ __global__ void __launch_bounds__(nt64<PY>(), minb64<PY>())
   const size_t fs = (size_t)nx * nyh;
   const int bx = blockIdx.x, ix0 = 2 * bx;
   const bool has1 = ix0 + 1 < nx;
-  zmerge_load<NT>(zsm, ay, RD, ix0, has1, nx, nyh);
-  zmerge_load<NT>(zsm + ny, ay, RD + fs, ix0, has1, nx, nyh);
+  zmerge_fields<NT, 2>(zsm, ay, RD, fs, ix0, has1, nx, nyh);
   __syncthreads();
   zfft_run<+1, PY>(2, ay);
   const KksPar q = *par;
