@@ -352,6 +352,13 @@ __device__ __forceinline__ void zreduce_store(double (&v)[NV], double* out) {
 
 __device__ __forceinline__ bool zin_iface(double e) { return e >= 0.1 && e <= 0.9; }
 
+// Ask L2 for `bytes` (a multiple of 16) from a 16-byte aligned global address
+// (one bulk prefetch, no data returned): the state rows a row pass reads
+// after its transforms arrive in L2 while the transforms run.
+__device__ __forceinline__ void zprefetch_l2(const void* p, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
 // Split the transform of (row a + i row b) (digit-reversed) into the half
 // spectra of rows ix0 (a) and ix0+1 (b) of a column-major spectrum field.
 template <int NT>
@@ -578,6 +585,15 @@ __global__ void __launch_bounds__(nt64<PY>(), minb64<PY>())
   const size_t fs = (size_t)nx * nyh;
   const int bx = blockIdx.x, ix0 = 2 * bx;
   const bool has1 = ix0 + 1 < nx;
+  if (threadIdx.x == 0) {  // rows ix0, ix0 + 1 of eta, X_al, X_th for the pointwise phase
+    const size_t i0 = (size_t)ix0 * ny;
+    const uint32_t bytes = (has1 ? 16u : 8u) * (uint32_t)ny;
+    if ((bytes & 15u) == 0) {
+      zprefetch_l2(eta + i0, bytes);
+      zprefetch_l2(Xal + i0, bytes);
+      zprefetch_l2(Xth + i0, bytes);
+    }
+  }
   zmerge_fields<NT, 3>(zsm, ay, RB, fs, ix0, has1, nx, nyh);
   __syncthreads();
   zfft_run<+1, PY>(3, ay);
@@ -724,6 +740,10 @@ __global__ void __launch_bounds__(nt64<PY>(), minb64<PY>())
   const size_t fs = (size_t)nx * nyh;
   const int bx = blockIdx.x, ix0 = 2 * bx;
   const bool has1 = ix0 + 1 < nx;
+  if (threadIdx.x == 0) {  // rows ix0, ix0 + 1 of the old X for the pointwise phase
+    const uint32_t bytes = (has1 ? 16u : 8u) * (uint32_t)ny;
+    if ((bytes & 15u) == 0) zprefetch_l2(X_o + (size_t)ix0 * ny, bytes);
+  }
   zmerge_fields<NT, 2>(zsm, ay, RD, fs, ix0, has1, nx, nyh);
   __syncthreads();
   zfft_run<+1, PY>(2, ay);
