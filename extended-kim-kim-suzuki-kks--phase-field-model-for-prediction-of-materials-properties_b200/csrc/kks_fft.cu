@@ -1686,8 +1686,11 @@ void kks_fft_launch_attempt(const KksFftLaunch& L, int p, cudaStream_t s) {
 #undef KKS_ROWS
 #undef KKS_COLS
   }
-  kf_extras<<<L.nbx, kExtrasThreads, 0, s>>>(L.dc, L.par, (const double*)f.eta[1 - p], 3, P5_GRAD2, P5_IFACE,
-                                       f.partials);
+  // the stencil pass is bound by load latency: give it at least one block per
+  // row pair (the decide kernel reduces that many partial-sum rows anyway)
+  const int ge = std::max(L.nbx, kks_fft_row_blocks(L.nx));
+  kf_extras<<<ge, kExtrasThreads, 0, s>>>(L.dc, L.par, (const double*)f.eta[1 - p], 3, P5_GRAD2, P5_IFACE,
+                                          f.partials);
 }
 
 int kks_fft_col_blocks(int nyh, int cols) { return col_blocks(nyh, cols); }
