@@ -192,6 +192,11 @@ class StepAdjoint:
             if t.dtype != torch.float64 or not t.is_cuda or not t.is_contiguous() or t.numel() != 4 * self.nx * self.ny:
                 raise ValueError("state tensors must be contiguous float64 CUDA tensors of 4 * nx * ny values")
         stream = torch.cuda.current_stream(self.device).cuda_stream
+        if stream == 0:
+            # torch's default is the legacy default stream; NULL would select
+            # the handle's own (non-blocking) stream, so name the legacy one
+            # (cudaStreamLegacy) to stay ordered with torch's work
+            stream = 1
         if stream != self._stream:
             L.check(self.lib.kks_adj_set_stream(self.h, ctypes.c_void_p(stream)), "kks_adj_set_stream")
             self._stream = stream

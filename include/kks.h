@@ -313,7 +313,9 @@ int kks_adj_backward_device(kks_adj* h, const double* state_in, const double* st
 /* Run the handle's calls on the caller's CUDA stream (a cudaStream_t; the
  * calls then return once their work is queued, ordered after earlier work on
  * that stream), or, with stream = NULL, on the handle's own stream, returning
- * after it has finished (the default). Switching waits for queued work. */
+ * after it has finished (the default). The legacy default stream is named
+ * cudaStreamLegacy here, since NULL selects the handle's own stream.
+ * Switching waits for queued work. */
 int kks_adj_set_stream(kks_adj* h, void* stream);
 /* Precision of the handle's step and adjoint: KKS_PRECISION_FP64 (default)
  * or KKS_PRECISION_MIXED: every transform in FP32 (cuFFT R2C / C2R on the
