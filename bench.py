@@ -548,7 +548,7 @@ def main():
     cell.close()
 
     # FP64 step on the same cell, for the mixed-vs-FP64 ratio of the metric
-    fp64 = None
+    fp64 = fp64_cufft = fp64_shape = None
     if args.precision != "fp64" and not args.only_timed:
         c64 = solver.Cell(cfg, tables, precision="fp64", device=local_rank)
         c64.upload(*state)
@@ -561,8 +561,20 @@ def main():
         k64 = max(10, args.steps // 4)
         c64.run(k64)
         m1, _ = c64.timing()
-        c64.close()
         fp64 = k64 / ((m1 - m0) / 1000.0)
+        fp64_shape = c64.launch_shape()
+        c64.close()
+        # the same FP64 step with cuFFT transforms (the plain GPU step before the
+        # fused FP64 passes), the other denominator of the mixed-vs-FP64 ratio
+        c64 = solver.Cell(cfg, tables, precision="fp64", device=local_rank)
+        c64.set_launch_shape(0, fp64_shape["cols"], fp64_shape["field_blocks"])
+        c64.upload(*state)
+        c64.run(args.warmup)
+        m0, _ = c64.timing()
+        c64.run(k64)
+        m1, _ = c64.timing()
+        c64.close()
+        fp64_cufft = k64 / ((m1 - m0) / 1000.0)
 
     # end to end through the C ABI: host fields in, K steps, fields and histories out
     import ctypes
@@ -638,7 +650,10 @@ def main():
                                                          "before the run"}),
         "cell_updates_per_s": value * N,
         "fp64_steps_per_s": fp64,
+        "fp64_launch_shape": fp64_shape,
         "mixed_over_fp64": (value / world / fp64) if fp64 else None,
+        "fp64_cufft_steps_per_s": fp64_cufft,
+        "mixed_over_fp64_cufft": (value / world / fp64_cufft) if fp64_cufft else None,
         "roofline": {
             "bound": "hbm",
             "achieved": achieved,
