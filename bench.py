@@ -339,6 +339,65 @@ def sharded_ensemble_leg(precision, device, steps, warmup, rank, world, barrier,
             "timing": "host wall clock per rank around Ensemble.run, max over ranks"}
 
 
+def profile_armed(args):
+    """Profiling run of armed attempts at 1420^2 that a kernel profiler can
+    reach in few launches. ``save`` advances the ramp1420 cell untimed to step
+    3640 (the adaptive scheme is armed from step 3638) and writes its
+    checkpoint to ``--checkpoint``. ``measure`` runs 3 unarmed attempts of a
+    fresh cell (30 kernels), then restores the checkpoint into a second cell
+    and runs step 3640 (its attempts are all rejected until max_iterations
+    stops the run: every attempt computes the residual pair and restores the
+    step's input), printing both cells' device ms per attempt."""
+    from pf_kks_gpu import solver, workloads
+    from pf_kks_gpu.materials import MaterialTables
+
+    cfg, spec = workloads.ramp1420(n_steps=3700, precision=args.precision)
+    tables = MaterialTables.from_npz(cfg.material_tables, cfg.c_gamma, cfg.c_eps0)
+    shape = [int(v) for v in (args.shape or "1,3,296").split(",")]
+    init = workloads.initial_state(cfg, spec)
+    if args.armed_profile == "save":
+        cell = solver.Cell(cfg, tables, precision=args.precision)
+        try:
+            cell.set_launch_shape(*shape)
+            cell.upload(*init)
+            cell.run(3640)
+            cell.drain()
+            with open(args.checkpoint, "wb") as f:
+                f.write(cell.checkpoint())
+            print(json.dumps({"saved": args.checkpoint, "istep": int(cell.state().istep)}), flush=True)
+        finally:
+            cell.close()
+        return 0
+    out = {}
+    a = solver.Cell(cfg, tables, precision=args.precision)
+    try:
+        a.set_launch_shape(*shape)
+        a.upload(*init)
+        m0, n0 = a.timing()
+        a.run(3)
+        m1, n1 = a.timing()
+        out["unarmed_ms_per_attempt"] = (m1 - m0) / max(n1 - n0, 1)
+    finally:
+        a.close()
+    b = solver.Cell(cfg, tables, precision=args.precision)
+    try:
+        b.set_launch_shape(*shape)
+        with open(args.checkpoint, "rb") as f:
+            b.restore(f.read())
+        s0 = b.state()
+        m0, _ = b.timing()
+        b.run(1)
+        m1, _ = b.timing()
+        s1 = b.state()
+        n = int(s1.attempts - s0.attempts)
+        out.update({"step": int(s0.istep), "armed": bool(s0.flag), "armed_attempts": n,
+                    "armed_ms_per_attempt": (m1 - m0) / max(n, 1), "status": int(s1.status)})
+    finally:
+        b.close()
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def profile_ensemble(args):
     """Profiling run: the 48-cell ensemble as one batch (column tile 4, one
     group), ``--warmup`` then ``--steps`` batch attempts; device time from the
@@ -464,12 +523,18 @@ def main():
     ap.add_argument("--no-armed", action="store_true", help="skip the armed-attempt leg")
     ap.add_argument("--only-timed", action="store_true",
                     help="skip the FP64 comparison and end-to-end cells (profiling runs)")
+    ap.add_argument("--armed-profile", default=None, choices=("save", "measure"),
+                    help="profiling: armed 1420^2 attempts from a checkpoint at step 3640 (save it, then measure)")
+    ap.add_argument("--checkpoint", default=os.path.join(tempfile.gettempdir(), "kks_ramp1420_step3640.bin"),
+                    help="checkpoint file of --armed-profile")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         return run_reference(args)
     if args.only_ensemble:
         return profile_ensemble(args)
+    if args.armed_profile:
+        return profile_armed(args)
 
     rank, world, local_rank = env_rank()
     dist = None

@@ -1154,6 +1154,14 @@ __global__ void __launch_bounds__(pass_threads<PX>(), pass_min_blocks<PX>())
   cols_CD_X_body<PX>(c, par, fc, RC, SA, RD, kys, ctl, bulk, (int)blockIdx.x);
 }
 
+// Bulk prefetch of a contiguous range into L2 (no data returned), issued only
+// where the range starts on a 16-byte boundary and spans whole 16-byte units,
+// as the instruction requires; otherwise the later loads go to memory.
+__device__ __forceinline__ void prefetch_rows_l2(const void* p, uint32_t bytes) {
+  if ((((uintptr_t)p | bytes) & 15u) != 0 || bytes == 0) return;
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
 // pass 5: one row pair of RD -> d_eta, d_X; new state, phase compositions,
 // new free energy and diffusion potential, residual and history sums
 template <int PY>
@@ -1174,6 +1182,22 @@ __device__ __forceinline__ void rows_D_body(const KksConst* __restrict__ c, cons
   const int ix0 = 2 * bx;
   const bool has1 = ix0 + 1 < nx;
   if (!row_block_in_range(c, fc, ix0, bx, kSiteRowsD)) return;
+  if (threadIdx.x == 0 && par->armed_write) {
+    // armed attempts read the pair's rows of mu, G- and the minus state after
+    // the transforms: bring them into L2 while the transforms run
+    const KksPar& qa = *par;
+    const size_t i0 = (size_t)ix0 * ny;
+    const uint32_t rows = has1 ? 2u : 1u;
+    prefetch_rows_l2(mu + i0, rows * 4u * (uint32_t)ny);
+    if (qa.armed_residual) {
+      const float* gm = qa.gm == 0 ? g0 : (qa.gm == 1 ? g1 : g2);
+      prefetch_rows_l2(gm + i0, rows * 4u * (uint32_t)ny);
+      if (!qa.minus_is_state) {
+        prefetch_rows_l2(eta_m + i0, rows * 8u * (uint32_t)ny);
+        prefetch_rows_l2(X_m + i0, rows * 8u * (uint32_t)ny);
+      }
+    }
+  }
   // staging after the two sequences: the pair's two half spectra (tensor
   // load), then rows ix0, ix0+1 of the old eta and X (bulk copies,
   // overlapping the inverse FFT)

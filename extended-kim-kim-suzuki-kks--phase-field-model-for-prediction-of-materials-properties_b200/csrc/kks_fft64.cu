@@ -742,7 +742,20 @@ __global__ void __launch_bounds__(nt64<PY>(), minb64<PY>())
   const bool has1 = ix0 + 1 < nx;
   if (threadIdx.x == 0) {  // rows ix0, ix0 + 1 of the old X for the pointwise phase
     const uint32_t bytes = (has1 ? 16u : 8u) * (uint32_t)ny;
-    if ((bytes & 15u) == 0) zprefetch_l2(X_o + (size_t)ix0 * ny, bytes);
+    const size_t i0 = (size_t)ix0 * ny;
+    if ((bytes & 15u) == 0) {
+      zprefetch_l2(X_o + i0, bytes);
+      // armed attempts also read the pair's rows of mu, G- and the minus state
+      const KksPar& qa = *par;
+      if (qa.armed_write) zprefetch_l2(mu + i0, bytes);
+      if (qa.armed_residual) {
+        zprefetch_l2((qa.gm == 0 ? g0 : (qa.gm == 1 ? g1 : g2)) + i0, bytes);
+        if (!qa.minus_is_state) {
+          zprefetch_l2(eta_m + i0, bytes);
+          zprefetch_l2(X_m + i0, bytes);
+        }
+      }
+    }
   }
   zmerge_fields<NT, 2>(zsm, ay, RD, fs, ix0, has1, nx, nyh);
   __syncthreads();

@@ -34,6 +34,8 @@
 
 #include <math.h>
 
+#include <type_traits>
+
 #include "kks_internal.cuh"
 #include "kks_pointwise.cuh"
 
@@ -447,8 +449,33 @@ __global__ void __launch_bounds__(kThreads)
               double* __restrict__ X_o, typename Tr<MIXED>::R* __restrict__ Xal_o,
               typename Tr<MIXED>::R* __restrict__ Xth_o, double* __restrict__ eta_m, double* __restrict__ X_m) {
   if (!ctl->restore || ctl->status != KKS_STATUS_OK) return;
+  using R = typename Tr<MIXED>::R;
+  using R2 = typename std::conditional<MIXED, float2, double2>::type;
   const int N = c->N;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+  const int stride = gridDim.x * blockDim.x;
+  int start = 0;
+  // two points per access where every array allows it (16-byte double pairs,
+  // 8- or 16-byte pairs of the composition type): a copy of ~80 bytes per
+  // point, bound by HBM, wants the wide accesses and their bytes in flight
+  const uintptr_t a8 = (uintptr_t)eta_i | (uintptr_t)X_i | (uintptr_t)eta_o | (uintptr_t)X_o |
+                       (uintptr_t)eta_m | (uintptr_t)X_m;
+  const uintptr_t ar = (uintptr_t)Xal_i | (uintptr_t)Xth_i | (uintptr_t)Xal_o | (uintptr_t)Xth_o;
+  if ((a8 & 15u) == 0 && (ar & (2 * sizeof(R) - 1)) == 0) {
+    const int N2 = N / 2;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < N2; j += stride) {
+      const double2 eo = ((const double2*)eta_o)[j], xo = ((const double2*)X_o)[j];
+      const double2 ei = ((const double2*)eta_i)[j], xi = ((const double2*)X_i)[j];
+      const R2 ai = ((const R2*)Xal_i)[j], ti = ((const R2*)Xth_i)[j];
+      ((double2*)eta_m)[j] = eo;
+      ((double2*)X_m)[j] = xo;
+      ((double2*)eta_o)[j] = ei;
+      ((double2*)X_o)[j] = xi;
+      ((R2*)Xal_o)[j] = ai;
+      ((R2*)Xth_o)[j] = ti;
+    }
+    start = 2 * N2;
+  }
+  for (int i = start + blockIdx.x * blockDim.x + threadIdx.x; i < N; i += stride) {
     eta_m[i] = eta_o[i];
     X_m[i] = X_o[i];
     eta_o[i] = eta_i[i];
