@@ -1246,6 +1246,16 @@ __device__ __forceinline__ void rows_D_body(const KksConst* __restrict__ c, cons
       if (r == 1 && !has1) continue;
       const size_t i = (size_t)(ix0 + r) * ny + y;
       const int is = r * ny + y;
+      // the residual's inputs first, so that their loads overlap the
+      // phase-composition math (neither buffer is written before its use)
+      float mu_m = 0.0f, g_m = 0.0f;
+      double x_m = 0.0, e_m = 0.0;
+      if (q.armed_residual) {
+        mu_m = mu[i];
+        g_m = gm_buf[i];
+        x_m = X_minus[i];
+        e_m = eta_minus[i];
+      }
       const double xo = bulk ? s_X[is] : X_o[i];
       const double eb = (bulk ? s_eta[is] : eta_o[i]) + (double)(r == 0 ? de.x : de.y);
       const double xb = xo + (double)(r == 0 ? dX.x : dX.y);
@@ -1275,13 +1285,13 @@ __device__ __forceinline__ void rows_D_body(const KksConst* __restrict__ c, cons
         const float gw = e2 - 2.0f * e3 + e2 * e2;
         const float G_b = (1.0f - hh) * fa_s + hh * ft_s + w_s * gw;
         if (q.armed_residual) {
-          const double mum = (double)mu[i];
-          const double dXdt = (xb - X_minus[i]) / dt;
+          const double mum = (double)mu_m;
+          const double dXdt = (xb - x_m) / dt;
           const double mu_mean = ((double)mu_b + mum) / 2;
           const double diffusion = dXdt * mu_mean;
-          const double detadt = (eb - eta_minus[i]) / dt;
+          const double detadt = (eb - e_m) / dt;
           const double allen_cahn = q.inv_Ls * (detadt * detadt);
-          const double temperature = ((double)G_b - (double)gm_buf[i]) / dt;
+          const double temperature = ((double)G_b - (double)g_m) / dt;
           acc[5] += diffusion;
           acc[6] += allen_cahn;
           acc[7] += temperature;
