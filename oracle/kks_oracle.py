@@ -22,6 +22,10 @@ with ``N`` the inverse of the 2x2 acoustic tensor (zero at k = 0), and
 
 The reduction is exact in real arithmetic; it changes round-off only.
 
+``run(update=...)`` can replace the update by an emulation of the mixed CUDA
+step (single-precision transforms; accuracy studies only). The default is the
+reference's update, and every pin below is of that default.
+
 Parity of this oracle is PINNED (tests/test_oracle_golden.py):
 
 * against the map the 2022 reproducible run archived after its first step
@@ -462,8 +466,62 @@ def _nanmean_masked(a, mask):
             return np.mean(a[mask])
 
 
+class FFT32:
+    """Single-precision transforms (complex64 in, complex64 out) for the
+    accuracy studies' emulation of the mixed step; see ``run(update=...)``."""
+
+    def __init__(self):
+        import scipy.fft as sfft
+
+        self._sfft = sfft
+
+    def fft(self, a):
+        return self._sfft.fftn(np.asarray(a).astype(np.complex64), axes=(0, 1, 2))
+
+    def ifft(self, a):
+        return self._sfft.ifftn(np.asarray(a).astype(np.complex64), axes=(0, 1, 2))
+
+
+def _mixed_update(update, eta, X, drive, G_ceta_G_cc, k, k2, ac_mul, ac_den, ch_mul, bk_mul, fft, fft32):
+    """New eta and X of the semi-implicit step (pf_kks/solver.py:249-264) in
+    the mixed CUDA step's increment form, for the accuracy studies. With
+    a_k = ac_den k^2 and b_k = bk_mul k^2:
+
+        d_eta^ = (ac_mul FT(drive) - a_k FT(eta)) / (1 + a_k)
+        d_X^   = (ch_mul FT(flux) - b_k FT(X)) / (1 + b_k),
+        flux   = G_ceta_G_cc grad(eta),  grad(eta) = FT^-1(i k FT(eta)),
+
+    transformed back and added to the FP64 state (algebraically the
+    reference's update). "mixed": every transform and the spectral arithmetic
+    in single precision (drive, flux factor and state rounded to FP32 on
+    input), as the mixed CUDA step. "mixed_ch64": the Cahn-Hilliard chain (the
+    eta gradients, the flux transforms, FT(X) and d_X^) in FP64, only the
+    inverse transform of d_X^ and the Allen-Cahn part in single precision."""
+    f32 = np.float32
+    k0, k1 = k[0].astype(f32), k[1].astype(f32)
+    ak = (ac_den * k2).astype(f32)
+    etak32 = fft32.fft(eta)
+    d_eta = (f32(ac_mul) * fft32.fft(drive.astype(f32)) - ak * etak32) / (1 + ak)
+    eta_b = eta + np.real(fft32.ifft(d_eta)).astype(np.float64)
+    if update == "mixed":
+        bk = (bk_mul * k2).astype(f32)
+        gx = np.real(fft32.ifft(1j * k0 * etak32))
+        gy = np.real(fft32.ifft(1j * k1 * etak32))
+        gc = G_ceta_G_cc.astype(f32)
+        flux_k = 1j * k0 * fft32.fft(gc * gx) + 1j * k1 * fft32.fft(gc * gy)
+        d_X = (f32(ch_mul) * flux_k - bk * fft32.fft(X)) / (1 + bk)
+    else:
+        etak = fft.fft(eta)
+        gx = np.real(fft.ifft(1j * k[0] * etak))
+        gy = np.real(fft.ifft(1j * k[1] * etak))
+        flux_k = 1j * k[0] * fft.fft(G_ceta_G_cc * gx) + 1j * k[1] * fft.fft(G_ceta_G_cc * gy)
+        d_X = (ch_mul * flux_k - bk_mul * k2 * fft.fft(X)) / (1 + bk_mul * k2)
+    X_b = X + np.real(fft32.ifft(d_X)).astype(np.float64)
+    return eta_b, X_b
+
+
 def run(cfg, eta, X, X_al, X_th, tables_path, out_dir=".", write_logs=True, verbose=False, save_maps=True,
-        fft_workers=None, max_steps=None, on_attempt=None, resume=None, snapshot_steps=()):
+        fft_workers=None, max_steps=None, on_attempt=None, resume=None, snapshot_steps=(), update="fp64"):
     """Restatement of ``pf_kks.solver.run`` (pf_kks/solver.py:76-414).
 
     ``tables_path`` is the resolved material-table file (the reference resolves
@@ -482,7 +540,14 @@ def run(cfg, eta, X, X_al, X_th, tables_path, out_dir=".", write_logs=True, verb
     172-173, 353-365). eta, X, X_al, X_th are then the state at ``istep``.
     ``snapshot_steps``: steps at whose start such a dict (plus the four fields
     under ``state``) is recorded in ``Result.snapshots``.
+
+    ``update`` (accuracy studies only): "fp64" is the reference's update;
+    "mixed" emulates the mixed CUDA step's increment form with single-precision
+    transforms, "mixed_ch64" the same with the Cahn-Hilliard chain in FP64
+    (``_mixed_update``). Nothing else changes.
     """
+    if update not in ("fp64", "mixed", "mixed_ch64"):
+        raise ValueError("update must be fp64, mixed or mixed_ch64")
     t_wall = time.time()
     log = RunLog(out_dir, enabled=write_logs)
     maps_dir = os.path.join(out_dir, "saved_maps")
@@ -505,6 +570,7 @@ def run(cfg, eta, X, X_al, X_th, tables_path, out_dir=".", write_logs=True, verb
     if max_steps is not None:
         nstep = min(nstep, max_steps)
     fft = FFT(fft_workers)
+    fft32 = FFT32() if update != "fp64" else None
 
     t_s = 0
     t = 0
@@ -619,19 +685,24 @@ def run(cfg, eta, X, X_al, X_th, tables_path, out_dir=".", write_logs=True, verb
             el_eta_s = el_eta / C44
             el_s = el / (C44)
 
-            # Allen-Cahn (pf_kks/solver.py:249-254)
-            etak = fft.fft(eta)
-            etak_old = etak
-            drive_k = fft.fft(G_eta_s + el_eta_s)
-            etak = (-dtime_s * p["L_s"] * drive_k + etak) / (1 + dtime_s * p["L_s"] * p["kappa2_s"] * k2)
-            eta_b = np.real(fft.ifft(etak))
+            if update == "fp64":
+                # Allen-Cahn (pf_kks/solver.py:249-254)
+                etak = fft.fft(eta)
+                etak_old = etak
+                drive_k = fft.fft(G_eta_s + el_eta_s)
+                etak = (-dtime_s * p["L_s"] * drive_k + etak) / (1 + dtime_s * p["L_s"] * p["kappa2_s"] * k2)
+                eta_b = np.real(fft.ifft(etak))
 
-            # Cahn-Hilliard (pf_kks/solver.py:256-264); the z term is identically zero
-            Xk = fft.fft(X)
-            flux_k = (1j * k[0] * fft.fft(G_ceta_G_cc * np.real(fft.ifft(1j * k[0] * etak_old)))
-                      + 1j * k[1] * fft.fft(G_ceta_G_cc * np.real(fft.ifft(1j * k[1] * etak_old))))
-            Xk = (dtime_s * p["D_s"] * flux_k + Xk) / (1 + dtime_s * k2 * p["D_s"])
-            X_b = np.real(fft.ifft(Xk))
+                # Cahn-Hilliard (pf_kks/solver.py:256-264); the z term is identically zero
+                Xk = fft.fft(X)
+                flux_k = (1j * k[0] * fft.fft(G_ceta_G_cc * np.real(fft.ifft(1j * k[0] * etak_old)))
+                          + 1j * k[1] * fft.fft(G_ceta_G_cc * np.real(fft.ifft(1j * k[1] * etak_old))))
+                Xk = (dtime_s * p["D_s"] * flux_k + Xk) / (1 + dtime_s * k2 * p["D_s"])
+                X_b = np.real(fft.ifft(Xk))
+            else:
+                eta_b, X_b = _mixed_update(update, eta, X, G_eta_s + el_eta_s, G_ceta_G_cc, k, k2,
+                                           -dtime_s * p["L_s"], dtime_s * p["L_s"] * p["kappa2_s"],
+                                           dtime_s * p["D_s"], dtime_s * p["D_s"], fft, fft32)
 
             # Phase compositions from the start-of-step X (pf_kks/solver.py:266-268)
             X_al_b, X_th_b = phase_compositions(X, eta_b, A_alp, B_alp, A_thet, B_thet)
